@@ -1,0 +1,121 @@
+/*
+ * oracle_api.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Shared C interface of the two CPU oracles for the compositional
+ * Peng-Robinson FIM flash:
+ *   - oracle/_ref/libocpref.so : the reference's own MixtureComp compiled from
+ *     its sources (recipe: oracle/Makefile, harness: oracle/ref_harness.cpp);
+ *   - oracle/libflashport.so   : a plain-C restatement of the same algorithm
+ *     (oracle/flash_port.c).
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
+ * either library; the product path never does.
+ *
+ * Layout is the reference Bulk layout (array-of-structures per cell, as in
+ * include/Bulk.hpp:304-357 and the compact dSec_dPri of
+ * src/OCPFluidMethod.cpp:1056-1063, 1122-1187): with numCom = nc + 1 (water
+ * last) and numPhase = 3 (oil, gas, water),
+ *   Ni[n*numCom + i], S[n*3 + j], xij[n*3*numCom + j*numCom + i],
+ *   dSec_dPri[n*(numCom+1)*(numCom+1)*3 + r*(numCom+1) + c].
+ * Units are FIELD: psia, degF on input, ft3/lbmol, lbmol.
+ */
+#ifndef OCP_ORACLE_API_H
+#define OCP_ORACLE_API_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_MAX_NC 16
+
+/* Fluid and solver controls of one PVT region (one MixtureComp instance).
+ * Mirrors ComponentParam (include/ParamReservoir.hpp:87-193) as consumed by
+ * MixtureComp::MixtureComp (src/MixtureComp.cpp:28-165). */
+typedef struct {
+    int32_t nc;            /* hydrocarbon components */
+    int32_t rr_maxit;      /* RR keyword */
+    int32_t ssmsta_maxit;  /* SSMSTA keyword */
+    int32_t nrsta_maxit;   /* NRSTA keyword */
+    int32_t ssmsp_maxit;   /* SSMSP keyword */
+    int32_t nrsp_maxit;    /* NRSP keyword */
+    int32_t use_skip;      /* SkipStaAnaly::ifUseSkip */
+    int32_t pad0;
+    double rr_tol, ssmsta_tol, ssmsta_eyt, nrsta_tol, ssmsp_tol, nrsp_tol;
+    double Tc[ORC_MAX_NC];     /* degR */
+    double Pc[ORC_MAX_NC];     /* psia */
+    double Vc[ORC_MAX_NC];     /* ft3/lbmol (VCRIT) */
+    double MW[ORC_MAX_NC];
+    double Acf[ORC_MAX_NC];
+    double OmegaA[ORC_MAX_NC];
+    double OmegaB[ORC_MAX_NC];
+    double Vshift[ORC_MAX_NC]; /* dimensionless VSHIFT deck value */
+    double BIC[ORC_MAX_NC * ORC_MAX_NC]; /* nc*nc row-major, symmetric */
+    double LBCcoef[5];         /* LBCCOEF deck values (scaled x10 inside) */
+    double pvtw[5];            /* PVTW row: Pref, Bw, Cw, muw, Cvw */
+    double std_rho_w;          /* water density at surface, lb/ft3 */
+} orc_fluid;
+
+/* One batch of FlashFIM calls, one per cell, in Bulk layout. xij_in may alias
+ * xij and S_in may alias S (in-place, as the Bulk arrays are). The skip_*
+ * arrays are the per-bulk SkipStaAnaly cache (src/AcceleratePVT.cpp); they are
+ * read and written when use_skip != 0. Outputs of absent phases are left
+ * untouched, as PassFlashValue does (src/OCPFluidMethod.cpp:1141-1160). */
+typedef struct {
+    int64_t n;
+    /* inputs */
+    const double*  P;      /* [n] psia */
+    const double*  T;      /* [n] degF */
+    const double*  Ni;     /* [n*numCom] lbmol */
+    const double*  S_in;   /* [n*3] */
+    const int32_t* lastNP; /* [n] phase count of the last step, water included */
+    const double*  xij_in; /* [n*3*numCom] */
+    /* skip cache, in/out */
+    int32_t* skip_flag;
+    double*  skip_minEig;
+    double*  skip_P;
+    double*  skip_T;
+    double*  skip_z;       /* [n*nc] */
+    /* outputs */
+    int32_t* phaseNum;     /* [n] */
+    int32_t* phaseExist;   /* [n*3] */
+    double*  S;            /* [n*3] */
+    double*  Nt;           /* [n] */
+    double*  vf;           /* [n] */
+    double*  vfP;          /* [n] */
+    double*  vfi;          /* [n*numCom] */
+    double*  nj;           /* [n*3] */
+    double*  rho;          /* [n*3] */
+    double*  xi;           /* [n*3] */
+    double*  mu;           /* [n*3] */
+    double*  rhoP;         /* [n*3] */
+    double*  xiP;          /* [n*3] */
+    double*  muP;          /* [n*3] */
+    double*  xij;          /* [n*3*numCom] */
+    double*  rhox;         /* [n*3*numCom] */
+    double*  xix;          /* [n*3*numCom] */
+    double*  mux;          /* [n*3*numCom] */
+    double*  dSec_dPri;    /* [n*(numCom+1)*(numCom+1)*3] compact rows */
+    int32_t* bRowSizedSdP; /* [n] */
+    int32_t* pSderExist;   /* [n*3] */
+    int32_t* pVnumCom;     /* [n*3] */
+    double*  ePEC;         /* [n] */
+    int32_t* ftype;        /* [n] */
+    int32_t* NPhc;         /* [n] hydrocarbon phase count */
+    int32_t* iters;        /* [n*5] SSMSTA, NRSTA, SSMSP, NRSP, RR iterations */
+} orc_batch;
+
+/* Runs FlashFIM over the batch with nthreads host threads (each owning its own
+ * flash object). Returns 0 on success; *seconds receives the wall time of the
+ * flash loop alone (construction excluded). */
+int orc_flash_fim_batch(const orc_fluid* fluid, const orc_batch* batch,
+                        int nthreads, double* seconds);
+
+/* Identifies the implementation: "reference" or "port". */
+const char* orc_kind(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OCP_ORACLE_API_H */

@@ -1,0 +1,232 @@
+/*
+ * ref_harness.cpp -- TEST INFRASTRUCTURE ONLY.
+ *
+ * Batch harness around the reference's own MixtureComp (compiled from the
+ * reference sources by oracle/Makefile into oracle/_ref/libocpref.so). For each
+ * cell it makes exactly the calls IsoT_FIM::CalFlash makes
+ * (src/OCPFluidMethod.cpp:1108-1120): MixtureComp::FlashFIM followed by the
+ * copy-out of IsoT_FIM::PassFlashValue (src/OCPFluidMethod.cpp:1122-1187).
+ * Nothing of the reference is copied here; its headers are included and its
+ * objects linked. The access specifiers are opened only to read the
+ * iteration counters, the flash type, the hydrocarbon phase count and the
+ * SkipStaAnaly cache, which the reference keeps private.
+ */
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <thread>
+#include <vector>
+
+#define private public
+#define protected public
+#include "MixtureComp.hpp"
+#include "OptionalFeatures.hpp"
+#include "ParamReservoir.hpp"
+#undef private
+#undef protected
+
+#include "oracle_api.h"
+
+namespace {
+
+std::string num(double v)
+{
+    char buf[64];
+    std::snprintf(buf, sizeof(buf), "%.17g", v);
+    return buf;
+}
+
+std::string num(int v) { return std::to_string(v); }
+
+// Builds the ParamReservoir that MixtureComp(const ParamReservoir&, 0)
+// consumes (src/MixtureComp.cpp:28-165, include/MixtureComp.hpp:155-167).
+void make_param(const orc_fluid& f, ParamReservoir& rs)
+{
+    const int nc          = f.nc;
+    ComponentParam& cp    = rs.comsParam;
+    cp.numCom             = nc;
+    cp.numPhase           = 2;
+    auto set = [nc](Type_A_r<std::vector<OCP_DBL>>& dst, const double* src) {
+        dst.activity = OCP_TRUE;
+        dst.data.assign(1, std::vector<OCP_DBL>(src, src + nc));
+    };
+    cp.Cname.clear();
+    for (int i = 0; i < nc; i++) cp.Cname.push_back("C" + std::to_string(i + 1));
+    set(cp.Tc, f.Tc);
+    set(cp.Pc, f.Pc);
+    set(cp.Vc, f.Vc);
+    set(cp.MW, f.MW);
+    set(cp.Acf, f.Acf);
+    set(cp.OmegaA, f.OmegaA);
+    set(cp.OmegaB, f.OmegaB);
+    set(cp.Vshift, f.Vshift);
+    cp.LBCcoef.assign(f.LBCcoef, f.LBCcoef + 5);
+    // lower triangle, as the BIC keyword gives it (src/MixtureComp.cpp:118-129)
+    std::vector<OCP_DBL> low;
+    for (int i = 1; i < nc; i++)
+        for (int j = 0; j < i; j++) low.push_back(f.BIC[i * nc + j]);
+    cp.BIC.assign(1, low);
+    cp.SSMparamSTA = {num(f.ssmsta_maxit), num(f.ssmsta_tol), num(f.ssmsta_eyt)};
+    cp.NRparamSTA  = {num(f.nrsta_maxit), num(f.nrsta_tol)};
+    cp.SSMparamSP  = {num(f.ssmsp_maxit), num(f.ssmsp_tol)};
+    cp.NRparamSP   = {num(f.nrsp_maxit), num(f.nrsp_tol)};
+    cp.RRparam     = {num(f.rr_maxit), num(f.rr_tol)};
+    cp.miscible    = OCP_FALSE;
+    rs.PVTW_T.data.assign(1, std::vector<std::vector<OCP_DBL>>(5));
+    for (int k = 0; k < 5; k++) rs.PVTW_T.data[0][k] = {f.pvtw[k]};
+    rs.density.activity = OCP_TRUE; // std_RhoW = RHOW_STD, overwritten below
+}
+
+void run_chunk(const orc_fluid& f, const orc_batch& b, int64_t lo, int64_t hi,
+               double* secs)
+{
+    const int nc      = f.nc;
+    const int numCom  = nc + 1;
+    const int np      = 3;
+    const int ncol    = numCom + 1;
+    const int maxLen  = ncol * ncol * np;
+    const int64_t cnt = hi - lo;
+    if (cnt <= 0) {
+        *secs = 0;
+        return;
+    }
+
+    ParamReservoir rs;
+    make_param(f, rs);
+    MixtureComp mc(rs, 0);
+    mc.std_RhoW = f.std_rho_w;
+    OptionalFeatures of;
+    of.skipStaAnaly.SetUseSkip(f.use_skip ? OCP_TRUE : OCP_FALSE);
+    mc.SetupOptionalFeatures(of, static_cast<OCP_USI>(cnt));
+    SkipStaAnaly& sk = of.skipStaAnaly;
+
+    if (f.use_skip) {
+        for (int64_t c = 0; c < cnt; c++) {
+            const int64_t n = lo + c;
+            sk.flag[c]      = b.skip_flag[n] ? OCP_TRUE : OCP_FALSE;
+            sk.minEigen[c]  = b.skip_minEig[n];
+            sk.P[c]         = b.skip_P[n];
+            sk.T[c]         = b.skip_T[n];
+            for (int i = 0; i < nc; i++) sk.zi[c * nc + i] = b.skip_z[n * nc + i];
+        }
+    }
+
+    std::vector<double> Sin(np), xin(np * numCom), Nin(numCom);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int64_t c = 0; c < cnt; c++) {
+        const int64_t n = lo + c;
+        std::copy(b.S_in + n * np, b.S_in + (n + 1) * np, Sin.begin());
+        std::copy(b.xij_in + n * np * numCom, b.xij_in + (n + 1) * np * numCom,
+                  xin.begin());
+        std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, Nin.begin());
+        const OCP_ULL it0[5] = {mc.itersSSMSTA, mc.itersNRSTA, mc.itersSSMSP,
+                                mc.itersNRSP, mc.itersRR};
+
+        mc.FlashFIM(b.P[n], b.T[n], Nin.data(), Sin.data(),
+                    static_cast<USI>(b.lastNP[n]), xin.data(),
+                    static_cast<OCP_USI>(c));
+
+        // copy-out, as IsoT_FIM::PassFlashValue does
+        int pn = 0, len = 0;
+        for (int j = 0; j < np; j++) {
+            b.S[n * np + j]          = mc.GetS(j);
+            const int ex             = mc.GetPhaseExist(j) ? 1 : 0;
+            b.phaseExist[n * np + j] = ex;
+            if (ex) {
+                pn++;
+                b.rho[n * np + j]  = mc.GetRho(j);
+                b.xi[n * np + j]   = mc.GetXi(j);
+                b.mu[n * np + j]   = mc.GetMu(j);
+                b.rhoP[n * np + j] = mc.GetRhoP(j);
+                b.xiP[n * np + j]  = mc.GetXiP(j);
+                b.muP[n * np + j]  = mc.GetMuP(j);
+                b.nj[n * np + j]   = mc.GetNj(j);
+                for (int i = 0; i < numCom; i++) {
+                    const int64_t o = (n * np + j) * numCom + i;
+                    b.xij[o]        = mc.GetXij(j, i);
+                    b.rhox[o]       = mc.GetRhoX(j, i);
+                    b.xix[o]        = mc.GetXiX(j, i);
+                    b.mux[o]        = mc.GetMuX(j, i);
+                }
+            }
+            b.pSderExist[n * np + j] = mc.GetPSderExist(j) ? 1 : 0;
+            b.pVnumCom[n * np + j]   = static_cast<int32_t>(mc.GetPVnumCom(j));
+            if (b.pSderExist[n * np + j]) len++;
+            len += b.pVnumCom[n * np + j];
+        }
+        b.phaseNum[n] = pn;
+        b.Nt[n]       = mc.GetNt();
+        b.vf[n]       = mc.GetVf();
+        b.vfP[n]      = mc.GetVfP();
+        for (int i = 0; i < numCom; i++) b.vfi[n * numCom + i] = mc.GetVfi(i);
+        b.bRowSizedSdP[n]              = len;
+        const std::vector<OCP_DBL>& dd = mc.GetDXsDXp();
+        std::copy(dd.begin(), dd.begin() + len * ncol, b.dSec_dPri + n * maxLen);
+        b.ePEC[n]          = mc.GetErrorPEC();
+        b.ftype[n]         = static_cast<int32_t>(mc.ftype);
+        b.NPhc[n]          = static_cast<int32_t>(mc.NP);
+        b.iters[n * 5 + 0] = static_cast<int32_t>(mc.itersSSMSTA - it0[0]);
+        b.iters[n * 5 + 1] = static_cast<int32_t>(mc.itersNRSTA - it0[1]);
+        b.iters[n * 5 + 2] = static_cast<int32_t>(mc.itersSSMSP - it0[2]);
+        b.iters[n * 5 + 3] = static_cast<int32_t>(mc.itersNRSP - it0[3]);
+        b.iters[n * 5 + 4] = static_cast<int32_t>(mc.itersRR - it0[4]);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    *secs   = std::chrono::duration<double>(t1 - t0).count();
+
+    if (f.use_skip) {
+        for (int64_t c = 0; c < cnt; c++) {
+            const int64_t n  = lo + c;
+            b.skip_flag[n]   = sk.flag[c] ? 1 : 0;
+            b.skip_minEig[n] = sk.minEigen[c];
+            b.skip_P[n]      = sk.P[c];
+            b.skip_T[n]      = sk.T[c];
+            for (int i = 0; i < nc; i++) b.skip_z[n * nc + i] = sk.zi[c * nc + i];
+        }
+    }
+}
+
+} // namespace
+
+extern "C" int orc_flash_fim_batch(const orc_fluid* fluid, const orc_batch* batch,
+                                   int nthreads, double* seconds)
+{
+    if (!fluid || !batch || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
+    if (nthreads < 1) nthreads = 1;
+    const int64_t n = batch->n;
+    if (n <= 0) {
+        if (seconds) *seconds = 0;
+        return 0;
+    }
+    if (nthreads > n) nthreads = static_cast<int>(n);
+
+    // The reference prints from its constructor and from CheckSplit; mute it.
+    std::ios::iostate st = std::cout.rdstate();
+    std::cout.setstate(std::ios::failbit);
+
+    std::vector<double> secs(nthreads, 0.0);
+    std::vector<std::thread> th;
+    auto wall0 = std::chrono::steady_clock::now();
+    for (int t = 0; t < nthreads; t++) {
+        const int64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
+        th.emplace_back(run_chunk, std::cref(*fluid), std::cref(*batch), lo, hi,
+                        &secs[t]);
+    }
+    for (auto& x : th) x.join();
+    auto wall1 = std::chrono::steady_clock::now();
+    std::cout.clear(st);
+    if (seconds) {
+        // wall time of the slowest thread's flash loop
+        *seconds = *std::max_element(secs.begin(), secs.end());
+        (void)wall0;
+        (void)wall1;
+    }
+    return 0;
+}
+
+extern "C" const char* orc_kind(void) { return "reference"; }
