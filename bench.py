@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Flash throughput benchmark: states/s of the compositional PR FIM flash at
+1M cells on B200.
+
+Workload (one "step" = one FIM flash of every cell from a fresh state, i.e.
+MixtureComp::FlashFIM with lastNP = 0 and an empty skip cache, plus the
+PassFlashValue outputs): the 6-component seeded Peng-Robinson fluid, 1,048,576
+states (a 128 x 128 x 64 cell block): 70 % with P ~ U(5, 40) MPa,
+T ~ U(340, 400) K, z ~ Dirichlet(1); 30 % within 5 % of the seeded state's
+saturation pressure. Synthetic, seeded data (the reference publishes no
+dataset).
+
+Output: one JSON line (rank 0). ``value`` is whole-job states/s with inputs
+resident in HBM (device time, CUDA events, max over ranks); ``e2e`` is the
+same metric through the host-buffer C-ABI call (host<->device copies inside
+the timed region); ``roofline`` is the flash kernel against the measured FP64
+FMA throughput (its binding pipe), with the HBM view beside it;
+``cpu_baseline`` is the reference's own MixtureComp (compiled from its
+sources) on a bounded sample on this host's cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--form plain|fast]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "flash states/s at 1M cells: mixed+learned vs plain FP64 GPU, err vs FP64 oracle"
+NCELL = 1 << 20
+SEED = 2025
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="plain", choices=["plain", "fast"])
+    ap.add_argument("--ncell", type=int, default=NCELL)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = max(mx, float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- workload
+def bench_fluid():
+    from opencaeporo_b200.fluid import synthetic_fluid
+    return synthetic_fluid(6, 1234)
+
+
+def gpu_phase_counter(fluid, device, chunk=1 << 18):
+    """Hydrocarbon phase count of (P, T, Ni) batches with the plain GPU flash
+    (used only to place the near-envelope states)."""
+    import torch
+    from opencaeporo_b200.flash import MixtureCompBatch
+    fl = fluid.with_controls(use_skip=False)
+    m = MixtureCompBatch(fl, device)
+    st = m.new_state(chunk)
+
+    def count(P, T, Ni):
+        n = len(P)
+        res = np.empty(n, np.int64)
+        for c0 in range(0, n, chunk):
+            c1 = min(n, c0 + chunk)
+            k = c1 - c0
+            P_ = np.full(chunk, 1000.0)
+            T_ = np.full(chunk, 100.0)
+            N_ = np.tile(Ni[c0:c0 + 1], (chunk, 1))
+            P_[:k], T_[:k], N_[:k] = P[c0:c1], T[c0:c1], Ni[c0:c1]
+            st.load(P_, T_, N_)
+            st.out["phaseNum"].zero_()
+            m.flash_fim(st, diagnostics=False)
+            res[c0:c1] = st.out["phaseNum"][:k].cpu().numpy() - 1
+        return res
+
+    return count, m
+
+
+def make_workload(fluid, n, seed, device):
+    from opencaeporo_b200 import synth
+    count, m = gpu_phase_counter(fluid, device)
+    w = synth.mixed_states(fluid, n, seed, count, near_frac=0.3)
+    m.close()
+    return w
+
+
+# ------------------------------------------------------------ reference arm
+def reference_arm(args):
+    from oracle import oracle as O
+    from opencaeporo_b200 import synth
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    fl = bench_fluid()
+    kind = "reference" if O.available("reference") else "port"
+    cores = os.cpu_count() or 1
+    ns = int(min(args.ncell, max(8192, cores * 4000)))
+
+    def pc(P, T, Ni):
+        return O.flash_fim(kind, fl.with_controls(use_skip=False), P, T, Ni, nthreads=cores)["NPhc"]
+
+    w = synth.mixed_states(fl, ns, SEED, pc, near_frac=0.3)
+    times = []
+    for s in range(args.warmup + args.steps):
+        r = O.flash_fim(kind, fl, w["P"], w["T"], w["Ni"], nthreads=cores)
+        if s >= args.warmup:
+            times.append(r["seconds"])
+    t = float(np.mean(times))
+    v = ns / t
+    line = {"metric": METRIC, "value": v, "unit": "states/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": "FIM flash of fresh cells, 6-component PR fluid, 70 % uniform / "
+                                   "30 % near-envelope states", "cells_per_step": ns,
+                       "full_workload_cells": args.ncell},
+            "cpu_baseline": {"value": v, "unit": "states/s", "cores": cores, "kind": kind,
+                             "sample": f"{ns} states of the 1M-cell workload distribution per step"},
+            "e2e": {"value": v, "unit": "states/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ our arm
+def host_bytes(nc, use_skip):
+    from opencaeporo_b200 import _lib
+    ins = sum(nf * (4 if dt == "u32" else 8) for nf, dt in _lib.in_shapes(nc).values())
+    staged = sum(_lib.out_shapes(nc)[k][0] * 8 for k in
+                 ("rho", "xi", "mu", "rhoP", "xiP", "muP", "xij", "rhox", "xix", "mux", "nj"))
+    sk = sum(nf * (4 if dt == "u32" else 8) for nf, dt in _lib.skip_shapes(nc).values()) if use_skip else 0
+    esz = {"f64": 8, "u32": 4, "i32": 4, "u16": 2, "u8": 1}
+    outs = sum(nf * esz[dt] for nf, dt in _lib.out_shapes(nc).values())
+    return ins + staged + sk, outs + sk
+
+
+def our_arm(args):
+    import torch
+    import torch.distributed as dist
+    from opencaeporo_b200 import _lib, roofline
+    from opencaeporo_b200.flash import MixtureCompBatch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    dev = local
+    fl = bench_fluid()
+    n = args.ncell
+    w = make_workload(fl, n, SEED + rank, dev)
+    nc = fl.nc
+
+    m = MixtureCompBatch(fl, dev)
+    st = m.new_state(n)
+    st.load(w["P"], w["T"], w["Ni"])
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def step(ev=None):
+        flush.zero_()                       # evict L2 (256 MiB > 126 MB) between steps
+        st.skip["flag"].zero_()             # fresh cells: empty skip cache
+        if ev is not None:
+            ev[0].record(stream)
+        m.flash_fim(st, form=args.form, fresh=True)
+        if ev is not None:
+            ev[1].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        t1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms_total = t0.elapsed_time(t1)
+    kern_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    if world > 1:
+        t = torch.tensor([ms_total, kern_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total, kern_ms = float(t[0]), float(t[1])
+    ms_step = ms_total / args.steps
+    value = world * n / (ms_step * 1e-3)
+
+    # roofline of the flash kernel (work model from the device's iteration counters)
+    res = st.to_host()
+    nphc = res["phaseNum"] - 1
+    fl_launch = roofline.flops(nc, res["iters"], nphc)
+    by_launch = roofline.batch_bytes(nc, nphc, fl.controls.use_skip)
+    fp64_peak = _lib.fma_peak_tflops(dev, 64)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    ach_tf = fl_launch / (kern_ms * 1e-3) / 1e12
+    ach_gbs = by_launch / (kern_ms * 1e-3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "flash_plain_nc6_traffic.json")
+    if os.path.exists(tf):
+        try:
+            traffic = json.load(open(tf)).get("bytes_per_launch_1M")
+        except (OSError, ValueError):
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "states/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "FIM flash of fresh cells (lastNP=0, empty skip cache), 6-component PR "
+                               "fluid, 1,048,576 states per GPU (128x128x64): 70 % uniform, 30 % within "
+                               "5 % of the saturation pressure", "form": args.form, "cells_per_gpu": n,
+                   "l2": "flushed between steps (256 MiB write)", "parallelism": f"independent shards x{world}",
+                   "two_phase_share": float(np.mean(nphc == 2)), "near_envelope_share": 0.3},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "fp64", "achieved": ach_tf, "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": ach_tf / fp64_peak, "traffic": traffic,
+                     "peak_source": "FP64 FMA throughput measured in this run (ocpf_measure_fma_peak); "
+                                    "MEASURED_PEAKS.json has no FP64 entry",
+                     "flops_per_launch": fl_launch, "kernel_ms": kern_ms},
+        "roofline_hbm": {"bound": "hbm", "achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": ach_gbs / hbm_peak, "bytes_per_launch": by_launch,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "iters_per_cell": {k: float(v) for k, v in zip(("ssmsta", "nrsta", "ssmsp", "nrsp", "rr"),
+                                                         res["iters"].mean(axis=0))},
+        "status_cells": int(np.count_nonzero(res["status"] & 0xC0)),
+    }
+    line["clocks"] = clk.summary()
+
+    # ------------------------------------------------ e2e through host buffers
+    if not args.no_e2e:
+        hs = m.new_host_state(n, pinned=True)
+        hs["P"].copy_(torch.as_tensor(w["P"]))
+        hs["T"].copy_(torch.as_tensor(w["T"]))
+        hs["Ni"].copy_(torch.as_tensor(np.ascontiguousarray(w["Ni"].T)))
+        times = []
+        for s in range(args.warmup + args.steps):
+            hs["skip"]["flag"].zero_()
+            hs["out"]["phaseNum"].zero_()
+            t_a = time.perf_counter()
+            m.flash_fim_host(hs, form=args.form)
+            t_b = time.perf_counter()
+            if s >= args.warmup:
+                times.append(t_b - t_a)
+        te = float(np.mean(times))
+        if world > 1:
+            t = torch.tensor([te], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t[0])
+        h2d, d2h = host_bytes(nc, fl.controls.use_skip)
+        line["e2e"] = {"value": world * n / te, "unit": "states/s", "h2d_bytes_per_step": h2d * n,
+                       "d2h_bytes_per_step": d2h * n, "ms_per_step": te * 1e3,
+                       "path": "ocpf_flash_fim_host, pinned host SoA buffers"}
+        del hs
+
+    # ------------------------------------------------ CPU baseline (rank 0, N=1)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(fl, w, res)
+
+    m.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(fl, w, gpu_res):
+    from oracle import compare as CMP
+    from oracle import oracle as O
+    kind = "reference" if O.available("reference") else "port"
+    cores = os.cpu_count() or 1
+    ns = int(min(len(w["P"]), max(8192, cores * 4000)))
+    r = O.flash_fim(kind, fl, w["P"][:ns], w["T"][:ns], w["Ni"][:ns], nthreads=cores)
+    sub = {k: (v[:ns] if isinstance(v, np.ndarray) else v) for k, v in gpu_res.items() if k != "skip"}
+    e = CMP.per_cell_errors(sub, r, fl.nc)
+    same = e["same"]
+    worst = np.zeros(ns)
+    for k in CMP.FLOAT_KEYS:
+        worst = np.fmax(worst, np.nan_to_num(e[k], nan=0.0))
+    # cells whose reference compositions are normalised (the reference's split
+    # Newton can leave |n|/nu compositions that do not sum to 1)
+    sx = np.nansum(np.where(r["phaseExist"][:, :2, None].astype(bool), r["xij"][:, :2, :fl.nc], 0.0), axis=2)
+    clean = same & np.all((np.abs(sx - 1) < 1e-10) | (sx == 0), axis=1)
+    return {"value": ns / r["seconds"], "unit": "states/s", "cores": cores, "kind": kind,
+            "sample": f"first {ns} states of the 1M-cell workload, one flash each, {cores} threads",
+            "parity_on_sample": {"phase_count_mismatches": int(np.count_nonzero(~same)),
+                                 "max_rel_err_clean_cells": float(np.max(worst[clean], initial=0.0)),
+                                 "share_cells_le_1e-8": float(np.mean(worst[same] <= 1e-8)),
+                                 "clean_cells": int(clean.sum())}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    our_arm(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,196 @@
+/*
+ * ocp_flash.h -- C ABI of the B200 compositional Peng-Robinson flash.
+ *
+ * One batched call replaces the reference's per-bulk flash loop
+ *   IsoT_FIM::CalFlash (src/OCPFluidMethod.cpp:1108-1120):
+ *     for n: flashCal[PVTNUM[n]]->FlashFIM(P[n], T[n], &Ni[n*nc], &S[n*np],
+ *                                          phaseNum[n], &xij[n*np*nc], n);
+ *            PassFlashValue(bk, n);            (src/OCPFluidMethod.cpp:1122-1187)
+ * with MixtureComp::FlashFIM (src/MixtureComp.cpp:494-573, declared at
+ * include/Mixture.hpp:106-112) evaluated for every cell on the GPU and the
+ * results written straight into the caller's arrays, as PassFlashValue does.
+ *
+ * Conventions
+ *   - nc hydrocarbon components; numCom = nc + 1 (water last); 3 phases
+ *     (0 oil, 1 gas, 2 water), as in MixtureComp (src/MixtureComp.cpp:34-48).
+ *   - FIELD units: psia, degF, ft3/lbmol, lbmol, lb/ft3, cP.
+ *   - Every array pointer is a DEVICE pointer (ocpf_flash_fim_host excepted),
+ *     laid out structure-of-arrays: field index slow, cell index fast, e.g.
+ *     Ni[i*ncell + n], xij[(j*numCom + i)*ncell + n],
+ *     dSec_dPri[(r*(numCom+1) + c)*ncell + n].
+ *   - Outputs of phases that do not exist are left untouched (as
+ *     PassFlashValue leaves them); S, phaseExist, the derivative-shape flags
+ *     and the compact dSec_dPri rows are always written.
+ *   - No call traps or aborts. Numerical trouble is reported per cell in
+ *     `status` (OCPF_CELL_* bits); argument errors return OCPF_EINVAL.
+ *   - Calls are stream-ordered and asynchronous on the given cudaStream_t
+ *     (passed as void*; NULL = legacy default stream). A context may be used
+ *     from one host thread at a time.
+ */
+#ifndef OCP_FLASH_H
+#define OCP_FLASH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OCPF_MAX_NC 16
+#define OCPF_NUM_PHASE 3
+
+/* return codes */
+#define OCPF_OK 0
+#define OCPF_EINVAL 1       /* bad argument */
+#define OCPF_ECUDA 2        /* a CUDA runtime call failed */
+#define OCPF_ENOMEM 3       /* device allocation failed */
+#define OCPF_EUNSUPPORTED 4 /* e.g. no sm_100 device */
+
+/* per-cell status bits (ocpf_fim_out.status) */
+#define OCPF_CELL_SSMSTA_CAP 0x01  /* a stability SSM trial hit maxIt */
+#define OCPF_CELL_NRSTA_FAIL 0x02  /* stability NR not converged */
+#define OCPF_CELL_SSMSP_FAIL 0x04  /* split SSM not converged */
+#define OCPF_CELL_NRSP_FAIL 0x08   /* split NR not converged */
+#define OCPF_CELL_COLLAPSED 0x10   /* split collapsed to one phase (CheckSplit) */
+#define OCPF_CELL_SINGULAR 0x20    /* a dense solve met a zero pivot */
+#define OCPF_CELL_NONFINITE 0x40   /* a non-finite value reached an output */
+#define OCPF_CELL_SPLIT_CAP 0x80   /* split restart loop bound reached */
+
+/* flash forms */
+#define OCPF_FORM_PLAIN 0 /* FP64 drop-in, the reference's algorithm */
+#define OCPF_FORM_FAST 1  /* FP32 successive substitution + FP64 polish */
+
+/* Fluid of one PVT region plus its solver controls: what MixtureComp's
+ * constructor reads from ComponentParam (src/MixtureComp.cpp:28-165,
+ * include/ParamReservoir.hpp:87-193) and the water PVTW row. */
+typedef struct {
+    int32_t nc;
+    int32_t rr_maxit;     /* RR keyword */
+    int32_t ssmsta_maxit; /* SSMSTA keyword */
+    int32_t nrsta_maxit;  /* NRSTA keyword */
+    int32_t ssmsp_maxit;  /* SSMSP keyword */
+    int32_t nrsp_maxit;   /* NRSP keyword */
+    int32_t use_skip;     /* SkipStaAnaly::ifUseSkip (include/AcceleratePVT.hpp:71) */
+    int32_t pad0;
+    double rr_tol, ssmsta_tol, ssmsta_eyt, nrsta_tol, ssmsp_tol, nrsp_tol;
+    double Tc[OCPF_MAX_NC];     /* degR */
+    double Pc[OCPF_MAX_NC];     /* psia */
+    double Vc[OCPF_MAX_NC];     /* ft3/lbmol */
+    double MW[OCPF_MAX_NC];
+    double Acf[OCPF_MAX_NC];
+    double OmegaA[OCPF_MAX_NC];
+    double OmegaB[OCPF_MAX_NC];
+    double Vshift[OCPF_MAX_NC]; /* dimensionless deck VSHIFT */
+    double BIC[OCPF_MAX_NC * OCPF_MAX_NC]; /* nc*nc row-major, symmetric */
+    double LBCcoef[5];          /* deck LBCCOEF (scaled by 10 inside, as the reference does) */
+    double pvtw[5];             /* PVTW row: Pref, Bw, Cw, muw, Cvw */
+    double std_rho_w;           /* lb/ft3 */
+} ocpf_fluid;
+
+/* Inputs of FlashFIM for every cell (device, SoA). xij and S are the
+ * previous step's outputs (the Bulk arrays are passed in place), lastNP the
+ * previous phase count with water included (Bulk::phaseNum). */
+typedef struct {
+    const double*   P;      /* [ncell] psia */
+    const double*   T;      /* [ncell] degF */
+    const double*   Ni;     /* [numCom][ncell] */
+    const double*   S;      /* [3][ncell] */
+    const uint32_t* lastNP; /* [ncell] */
+    const double*   xij;    /* [3*numCom][ncell] */
+} ocpf_fim_in;
+
+/* Per-cell SkipStaAnaly cache (src/AcceleratePVT.cpp:135-233), read and
+ * written in place; may be all-NULL when the fluid's use_skip is 0. */
+typedef struct {
+    uint32_t* flag;   /* [ncell] */
+    double*   minEig; /* [ncell] */
+    double*   P;      /* [ncell] */
+    double*   T;      /* [ncell] degR (the flash's internal temperature) */
+    double*   z;      /* [nc][ncell] */
+} ocpf_skip;
+
+/* Outputs (device, SoA), named as the Bulk arrays PassFlashValue fills.
+ * Pointers marked optional may be NULL. */
+typedef struct {
+    uint32_t* phaseNum;     /* [ncell] phases present, water included */
+    uint32_t* phaseExist;   /* [3][ncell] */
+    double*   S;            /* [3][ncell] */
+    double*   Nt;           /* [ncell] */
+    double*   vf;           /* [ncell] */
+    double*   vfP;          /* [ncell] */
+    double*   vfi;          /* [numCom][ncell] */
+    double*   rho;          /* [3][ncell] */
+    double*   xi;           /* [3][ncell] */
+    double*   mu;           /* [3][ncell] */
+    double*   rhoP;         /* [3][ncell] */
+    double*   xiP;          /* [3][ncell] */
+    double*   muP;          /* [3][ncell] */
+    double*   xij;          /* [3*numCom][ncell] (may alias ocpf_fim_in.xij) */
+    double*   rhox;         /* [3*numCom][ncell] */
+    double*   xix;          /* [3*numCom][ncell] */
+    double*   mux;          /* [3*numCom][ncell] */
+    double*   dSec_dPri;    /* [3*(numCom+1)^2][ncell], first bRowSizedSdP rows written */
+    uint32_t* bRowSizedSdP; /* [ncell] */
+    uint32_t* pSderExist;   /* [3][ncell] */
+    uint32_t* pVnumCom;     /* [3][ncell] */
+    /* optional diagnostics */
+    double*   nj;           /* [3][ncell] phase moles */
+    double*   ePEC;         /* [ncell] MixtureComp::ePEC */
+    uint8_t*  ftype;        /* [ncell] flash type 0/1/2 */
+    int32_t*  iters;        /* [5][ncell] SSMSTA, NRSTA, SSMSP, NRSP, RR iterations */
+    uint16_t* status;       /* [ncell] OCPF_CELL_* bits */
+} ocpf_fim_out;
+
+typedef struct ocpf_ctx ocpf_ctx;
+
+/* Library version string. */
+const char* ocpf_version(void);
+
+/* Human-readable text for a return code. */
+const char* ocpf_status_string(int code);
+
+/* Creates a flash context for one PVT region on the given CUDA device:
+ * the counterpart of constructing MixtureComp(ParamReservoir, i)
+ * (src/MixtureComp.cpp:28-165) and SetupOptionalFeatures
+ * (src/MixtureComp.cpp:5128-5144). Derived constants are computed once here.
+ * Returns OCPF_EINVAL for nc outside [2, OCPF_MAX_NC] or non-positive
+ * critical properties. */
+int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx);
+
+/* Releases a context and every device buffer it owns. */
+int ocpf_destroy(ocpf_ctx* ctx);
+
+/* Batched MixtureComp::FlashFIM + PassFlashValue over ncell cells
+ * (src/MixtureComp.cpp:494-573, src/OCPFluidMethod.cpp:1108-1187), including
+ * the skip-stability decision CalFtypeFIM (src/AcceleratePVT.cpp:96-120) and
+ * CalSkipForNextStep (src/MixtureComp.cpp:5234-5254) on `skip`.
+ * form: OCPF_FORM_PLAIN or OCPF_FORM_FAST. Asynchronous on `stream`;
+ * allocates nothing. */
+int ocpf_flash_fim(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
+                   ocpf_fim_out* out, int form, void* stream);
+
+/* Same call with every array in HOST memory (pinned memory is faster). The
+ * cells are streamed through device staging buffers owned by the context in
+ * chunks, copies overlapping the flash on two streams; returns after the
+ * results are back in host memory. The staging buffers are allocated on the
+ * first call (and grown if a larger chunk is requested) and kept until
+ * ocpf_destroy. */
+int ocpf_flash_fim_host(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
+                        ocpf_fim_out* out, int form);
+
+/* Device time (ms) of the last ocpf_flash_fim's flash kernel, measured with
+ * CUDA events on its stream; waits for that kernel to finish. */
+int ocpf_last_kernel_ms(ocpf_ctx* ctx, float* ms);
+
+/* Measures the device's FMA throughput (TFLOP/s, FMA = 2 flops) in FP64
+ * (bits = 64) or FP32 (bits = 32) with a short register-only kernel: the
+ * compute-roofline denominator for the flash kernels. No reference
+ * counterpart (measurement utility). */
+int ocpf_measure_fma_peak(int device, int bits, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OCP_FLASH_H */

@@ -1,0 +1,168 @@
+"""ctypes declarations of the C ABI in ``include/ocp_flash.h`` and the loader
+of ``opencaeporo_b200/libocpflash.so``.
+
+The library is built in-tree (``python -m opencaeporo_b200.build``). There is
+no fallback: if the library is missing or cannot be loaded, :func:`lib`
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libocpflash.so")
+MAX_NC = 16
+NPH = 3
+
+OCPF_OK, OCPF_EINVAL, OCPF_ECUDA, OCPF_ENOMEM, OCPF_EUNSUPPORTED = 0, 1, 2, 3, 4
+FORM_PLAIN, FORM_FAST = 0, 1
+
+CELL_SSMSTA_CAP = 0x01
+CELL_NRSTA_FAIL = 0x02
+CELL_SSMSP_FAIL = 0x04
+CELL_NRSP_FAIL = 0x08
+CELL_COLLAPSED = 0x10
+CELL_SINGULAR = 0x20
+CELL_NONFINITE = 0x40
+CELL_SPLIT_CAP = 0x80
+
+# Every function the header declares (checked by the CPU test suite).
+EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
+           "ocpf_flash_fim", "ocpf_flash_fim_host", "ocpf_last_kernel_ms",
+           "ocpf_measure_fma_peak")
+
+_vp = C.c_void_p
+
+
+class Fluid(C.Structure):
+    _fields_ = [
+        ("nc", C.c_int32), ("rr_maxit", C.c_int32), ("ssmsta_maxit", C.c_int32),
+        ("nrsta_maxit", C.c_int32), ("ssmsp_maxit", C.c_int32), ("nrsp_maxit", C.c_int32),
+        ("use_skip", C.c_int32), ("pad0", C.c_int32),
+        ("rr_tol", C.c_double), ("ssmsta_tol", C.c_double), ("ssmsta_eyt", C.c_double),
+        ("nrsta_tol", C.c_double), ("ssmsp_tol", C.c_double), ("nrsp_tol", C.c_double),
+        ("Tc", C.c_double * MAX_NC), ("Pc", C.c_double * MAX_NC), ("Vc", C.c_double * MAX_NC),
+        ("MW", C.c_double * MAX_NC), ("Acf", C.c_double * MAX_NC),
+        ("OmegaA", C.c_double * MAX_NC), ("OmegaB", C.c_double * MAX_NC),
+        ("Vshift", C.c_double * MAX_NC), ("BIC", C.c_double * (MAX_NC * MAX_NC)),
+        ("LBCcoef", C.c_double * 5), ("pvtw", C.c_double * 5), ("std_rho_w", C.c_double),
+    ]
+
+
+IN_FIELDS = ("P", "T", "Ni", "S", "lastNP", "xij")
+SKIP_FIELDS = ("flag", "minEig", "P", "T", "z")
+OUT_FIELDS = ("phaseNum", "phaseExist", "S", "Nt", "vf", "vfP", "vfi", "rho", "xi", "mu",
+              "rhoP", "xiP", "muP", "xij", "rhox", "xix", "mux", "dSec_dPri", "bRowSizedSdP",
+              "pSderExist", "pVnumCom", "nj", "ePEC", "ftype", "iters", "status")
+OPTIONAL_OUT = ("nj", "ePEC", "ftype", "iters", "status")
+
+
+class FimIn(C.Structure):
+    _fields_ = [(f, _vp) for f in IN_FIELDS]
+
+
+class Skip(C.Structure):
+    _fields_ = [(f, _vp) for f in SKIP_FIELDS]
+
+
+class FimOut(C.Structure):
+    _fields_ = [(f, _vp) for f in OUT_FIELDS]
+
+
+def out_shapes(nc: int) -> dict:
+    """(number of SoA fields, element type) of every output array."""
+    ncom = nc + 1
+    ncol = ncom + 1
+    return {
+        "phaseNum": (1, "u32"), "phaseExist": (NPH, "u32"), "S": (NPH, "f64"), "Nt": (1, "f64"),
+        "vf": (1, "f64"), "vfP": (1, "f64"), "vfi": (ncom, "f64"), "rho": (NPH, "f64"),
+        "xi": (NPH, "f64"), "mu": (NPH, "f64"), "rhoP": (NPH, "f64"), "xiP": (NPH, "f64"),
+        "muP": (NPH, "f64"), "xij": (NPH * ncom, "f64"), "rhox": (NPH * ncom, "f64"),
+        "xix": (NPH * ncom, "f64"), "mux": (NPH * ncom, "f64"),
+        "dSec_dPri": (NPH * ncol * ncol, "f64"), "bRowSizedSdP": (1, "u32"),
+        "pSderExist": (NPH, "u32"), "pVnumCom": (NPH, "u32"), "nj": (NPH, "f64"),
+        "ePEC": (1, "f64"), "ftype": (1, "u8"), "iters": (5, "i32"), "status": (1, "u16"),
+    }
+
+
+def in_shapes(nc: int) -> dict:
+    ncom = nc + 1
+    return {"P": (1, "f64"), "T": (1, "f64"), "Ni": (ncom, "f64"), "S": (NPH, "f64"),
+            "lastNP": (1, "u32"), "xij": (NPH * ncom, "f64")}
+
+
+def skip_shapes(nc: int) -> dict:
+    return {"flag": (1, "u32"), "minEig": (1, "f64"), "P": (1, "f64"), "T": (1, "f64"),
+            "z": (nc, "f64")}
+
+
+_LIB = None
+
+
+def lib():
+    """Loads libocpflash.so (raises if it is missing: there is no fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing; build it with `python -m opencaeporo_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    L.ocpf_version.restype = C.c_char_p
+    L.ocpf_status_string.restype = C.c_char_p
+    L.ocpf_status_string.argtypes = [C.c_int]
+    L.ocpf_create.argtypes = [C.POINTER(Fluid), C.c_int, C.POINTER(_vp)]
+    L.ocpf_create.restype = C.c_int
+    L.ocpf_destroy.argtypes = [_vp]
+    L.ocpf_destroy.restype = C.c_int
+    L.ocpf_flash_fim.argtypes = [_vp, C.c_int64, C.POINTER(FimIn), C.POINTER(Skip),
+                                 C.POINTER(FimOut), C.c_int, _vp]
+    L.ocpf_flash_fim.restype = C.c_int
+    L.ocpf_flash_fim_host.argtypes = [_vp, C.c_int64, C.POINTER(FimIn), C.POINTER(Skip),
+                                      C.POINTER(FimOut), C.c_int]
+    L.ocpf_flash_fim_host.restype = C.c_int
+    L.ocpf_last_kernel_ms.argtypes = [_vp, C.POINTER(C.c_float)]
+    L.ocpf_last_kernel_ms.restype = C.c_int
+    L.ocpf_measure_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    L.ocpf_measure_fma_peak.restype = C.c_int
+    _LIB = L
+    return L
+
+
+def make_fluid(fl) -> Fluid:
+    """C-ABI fluid block from an :class:`opencaeporo_b200.fluid.Fluid`."""
+    f = Fluid()
+    nc = fl.nc
+    c = fl.controls
+    f.nc = nc
+    f.rr_maxit, f.rr_tol = c.rr_maxit, c.rr_tol
+    f.ssmsta_maxit, f.ssmsta_tol, f.ssmsta_eyt = c.ssmsta_maxit, c.ssmsta_tol, c.ssmsta_eyt
+    f.nrsta_maxit, f.nrsta_tol = c.nrsta_maxit, c.nrsta_tol
+    f.ssmsp_maxit, f.ssmsp_tol = c.ssmsp_maxit, c.ssmsp_tol
+    f.nrsp_maxit, f.nrsp_tol = c.nrsp_maxit, c.nrsp_tol
+    f.use_skip = 1 if c.use_skip else 0
+    for name in ("Tc", "Pc", "Vc", "MW", "Acf", "OmegaA", "OmegaB", "Vshift"):
+        arr = getattr(f, name)
+        for i, v in enumerate(getattr(fl, name)):
+            arr[i] = float(v)
+    for i in range(nc):
+        for k in range(nc):
+            f.BIC[i * nc + k] = float(fl.BIC[i, k])
+    for k in range(5):
+        f.LBCcoef[k] = float(fl.LBCcoef[k])
+        f.pvtw[k] = float(fl.pvtw[k])
+    f.std_rho_w = float(fl.std_rho_w)
+    return f
+
+
+def check(rc: int, what: str):
+    if rc != OCPF_OK:
+        msg = lib().ocpf_status_string(rc).decode()
+        raise RuntimeError(f"{what} failed: {msg} ({rc})")
+
+
+def fma_peak_tflops(device: int = 0, bits: int = 64) -> float:
+    """Measured FMA throughput of the device (TFLOP/s)."""
+    v = C.c_double(0)
+    check(lib().ocpf_measure_fma_peak(int(device), int(bits), C.byref(v)), "ocpf_measure_fma_peak")
+    return float(v.value)

@@ -1,0 +1,449 @@
+// flash_api.cu -- the C ABI of include/ocp_flash.h: context set-up (the
+// derived per-fluid constants of MixtureComp's constructor), the batched
+// FlashFIM launch on device buffers, and the pipelined host-buffer variant.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "flash_common.cuh"
+
+namespace ocpf {
+
+// Per-NC launchers, one translation unit each (flash_plain_ncN.cu).
+#define OCPF_DECL_PLAIN(N)                                                                        \
+    cudaError_t launch_plain_nc##N(const FluidConst& F, int64_t count, int64_t stride,            \
+                                   const ocpf_fim_in& in, const ocpf_skip& sk,                     \
+                                   const ocpf_fim_out& out, unsigned blocks, int bs, cudaStream_t st);
+OCPF_DECL_PLAIN(3)
+OCPF_DECL_PLAIN(6)
+OCPF_DECL_PLAIN(9)
+OCPF_DECL_PLAIN(12)
+
+using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const ocpf_fim_in&,
+                                      const ocpf_skip&, const ocpf_fim_out&, unsigned, int,
+                                      cudaStream_t);
+
+static PlainLauncher plain_kernel(int nc)
+{
+    switch (nc) {
+        case 3: return launch_plain_nc3;
+        case 6: return launch_plain_nc6;
+        case 9: return launch_plain_nc9;
+        case 12: return launch_plain_nc12;
+        default: return nullptr;
+    }
+}
+
+// ------------------------------------------------------- constant block
+
+bool make_fluid_const(const ocpf_fluid& in, FluidConst& f)
+{
+    const int nc = in.nc;
+    if (nc < 2 || nc > MAXNC) return false;
+    std::memset(&f, 0, sizeof(f));
+    f.nc           = nc;
+    f.use_skip     = in.use_skip ? 1 : 0;
+    f.rr_maxit     = in.rr_maxit;
+    f.ssmsta_maxit = in.ssmsta_maxit;
+    f.nrsta_maxit  = in.nrsta_maxit;
+    f.ssmsp_maxit  = in.ssmsp_maxit;
+    f.nrsp_maxit   = in.nrsp_maxit;
+    f.rr_tol       = in.rr_tol;
+    f.ssmsta_tol2  = in.ssmsta_tol * in.ssmsta_tol;  // src/MixtureComp.cpp:143
+    f.ssmsta_eyt   = in.ssmsta_eyt;
+    f.nrsta_tol    = in.nrsta_tol;
+    f.ssmsp_tol2   = in.ssmsp_tol * in.ssmsp_tol;
+    f.nrsp_tol     = in.nrsp_tol;
+    if (in.rr_maxit < 0 || in.ssmsta_maxit < 0 || in.nrsta_maxit < 0 || in.ssmsp_maxit < 0 ||
+        in.nrsp_maxit < 0)
+        return false;
+    for (int i = 0; i < nc; i++) {
+        if (!(in.Tc[i] > 0) || !(in.Pc[i] > 0) || !(in.Vc[i] > 0) || !(in.MW[i] > 0)) return false;
+        f.Tc[i]     = in.Tc[i];
+        f.Pc[i]     = in.Pc[i];
+        f.Vc[i]     = in.Vc[i];
+        f.Vcvis[i]  = in.Vc[i];  // no VCRITVIS/ZCRITVIS: Vcvis = Vc (src/MixtureComp.cpp:98-106)
+        f.MW[i]     = in.MW[i];
+        f.Acf[i]    = in.Acf[i];
+        f.OmegaA[i] = in.OmegaA[i];
+        f.OmegaB[i] = in.OmegaB[i];
+        // VSHIFT scaling, src/MixtureComp.cpp:89-93
+        f.Vshift[i] = in.Vshift[i] * (GAS_CONSTANT * in.OmegaB[i] * in.Tc[i] / in.Pc[i]);
+        // PR m(omega), src/MixtureComp.cpp:923-929
+        const double acf = in.Acf[i];
+        f.mwi[i] = (acf <= 0.49) ? 0.37464 + 1.54226 * acf - 0.26992 * std::pow(acf, 2)
+                                 : 0.379642 + 1.48503 * acf - 0.164423 * std::pow(acf, 2) +
+                                       0.016667 * std::pow(acf, 3);
+        f.sqrtMW[i]  = std::sqrt(in.MW[i]);
+        f.muAux1I[i] = 5.4402 * std::pow(in.Tc[i], 1.0 / 6) / std::pow(in.Pc[i], 2.0 / 3);
+        f.lbc1[i]    = 5.4402 * std::pow(in.Tc[i], 1.0 / 6);
+        f.lbc2[i]    = std::pow(in.Pc[i], 2.0 / 3);
+        for (int k = 0; k < nc; k++) {
+            if (in.BIC[i * nc + k] != in.BIC[k * nc + i]) return false;
+            f.omb[i * MAXNC + k] = 1 - in.BIC[i * nc + k];
+        }
+    }
+    for (int k = 0; k < 5; k++) {
+        f.L[k]    = in.LBCcoef[k] * 10;  // src/MixtureComp.cpp:108-111
+        f.pvtw[k] = in.pvtw[k];
+    }
+    f.std_rho_w = in.std_rho_w;
+    return true;
+}
+
+}  // namespace ocpf
+
+using namespace ocpf;
+
+struct ocpf_ctx {
+    int         device;
+    FluidConst  fc;
+    cudaEvent_t ev0, ev1;
+    bool        timed;
+    // host-path staging (device) buffers, grown on demand
+    int64_t     stage_cap;
+    void*       stage;
+    cudaStream_t hs[2];
+};
+
+static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
+
+extern "C" const char* ocpf_version(void) { return kVersion; }
+
+extern "C" const char* ocpf_status_string(int code)
+{
+    switch (code) {
+        case OCPF_OK: return "ok";
+        case OCPF_EINVAL: return "invalid argument";
+        case OCPF_ECUDA: return "CUDA runtime error";
+        case OCPF_ENOMEM: return "device allocation failed";
+        case OCPF_EUNSUPPORTED: return "unsupported";
+        default: return "unknown";
+    }
+}
+
+extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
+{
+    if (!fluid || !ctx) return OCPF_EINVAL;
+    *ctx = nullptr;
+    FluidConst fc;
+    if (!make_fluid_const(*fluid, fc)) return OCPF_EINVAL;
+    if (!plain_kernel(fc.nc)) return OCPF_EUNSUPPORTED;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return OCPF_ECUDA;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return OCPF_ECUDA;
+    if (prop.major != 10) return OCPF_EUNSUPPORTED;  // built for sm_100a only
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (cudaSetDevice(device) != cudaSuccess) return OCPF_ECUDA;
+    ocpf_ctx* c = new (std::nothrow) ocpf_ctx();
+    if (!c) return OCPF_ENOMEM;
+    c->device    = device;
+    c->fc        = fc;
+    c->timed     = false;
+    c->stage_cap = 0;
+    c->stage     = nullptr;
+    c->hs[0] = c->hs[1] = nullptr;
+    if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        cudaSetDevice(prev);
+        return OCPF_ECUDA;
+    }
+    cudaSetDevice(prev);
+    *ctx = c;
+    return OCPF_OK;
+}
+
+extern "C" int ocpf_destroy(ocpf_ctx* c)
+{
+    if (!c) return OCPF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(c->device);
+    cudaEventDestroy(c->ev0);
+    cudaEventDestroy(c->ev1);
+    if (c->stage) cudaFree(c->stage);
+    for (auto& s : c->hs)
+        if (s) cudaStreamDestroy(s);
+    cudaSetDevice(prev);
+    delete c;
+    return OCPF_OK;
+}
+
+static bool fim_args_ok(const ocpf_ctx* c, const ocpf_fim_in* in, const ocpf_skip* sk,
+                        const ocpf_fim_out* o)
+{
+    if (!in || !o) return false;
+    if (!in->P || !in->T || !in->Ni || !in->S || !in->lastNP || !in->xij) return false;
+    if (!o->phaseNum || !o->phaseExist || !o->S || !o->Nt || !o->vf || !o->vfP || !o->vfi ||
+        !o->rho || !o->xi || !o->mu || !o->rhoP || !o->xiP || !o->muP || !o->xij || !o->rhox ||
+        !o->xix || !o->mux || !o->dSec_dPri || !o->bRowSizedSdP || !o->pSderExist || !o->pVnumCom)
+        return false;
+    if (c->fc.use_skip && (!sk || !sk->flag || !sk->minEig || !sk->P || !sk->T || !sk->z)) return false;
+    return true;
+}
+
+static int launch_plain(ocpf_ctx* c, int64_t count, int64_t stride, const ocpf_fim_in& in,
+                        const ocpf_skip& sk, const ocpf_fim_out& out, cudaStream_t st, bool timed)
+{
+    if (count == 0) return OCPF_OK;
+    PlainLauncher k = plain_kernel(c->fc.nc);
+    if (!k) return OCPF_EUNSUPPORTED;
+    const int     bs     = 128;
+    const int64_t blocks = (count + bs - 1) / bs;
+    if (blocks > 0x7fffffffLL) return OCPF_EINVAL;
+    if (timed) cudaEventRecord(c->ev0, st);
+    const cudaError_t e = k(c->fc, count, stride, in, sk, out, (unsigned)blocks, bs, st);
+    if (timed) cudaEventRecord(c->ev1, st);
+    return e == cudaSuccess ? OCPF_OK : OCPF_ECUDA;
+}
+
+extern "C" int ocpf_flash_fim(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* sk,
+                              ocpf_fim_out* out, int form, void* stream)
+{
+    if (!c || ncell < 0) return OCPF_EINVAL;
+    if (ncell == 0) return OCPF_OK;
+    if (!fim_args_ok(c, in, sk, out)) return OCPF_EINVAL;
+    if (form != OCPF_FORM_PLAIN && form != OCPF_FORM_FAST) return OCPF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    ocpf_skip s{};
+    if (sk) s = *sk;
+    const int rc = launch_plain(c, ncell, ncell, *in, s, *out, (cudaStream_t)stream, true);
+    c->timed     = (rc == OCPF_OK && ncell > 0);
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+extern "C" int ocpf_last_kernel_ms(ocpf_ctx* c, float* ms)
+{
+    if (!c || !ms) return OCPF_EINVAL;
+    if (!c->timed) {
+        *ms = 0;
+        return OCPF_OK;
+    }
+    if (cudaEventSynchronize(c->ev1) != cudaSuccess) return OCPF_ECUDA;
+    return cudaEventElapsedTime(ms, c->ev0, c->ev1) == cudaSuccess ? OCPF_OK : OCPF_ECUDA;
+}
+
+// ------------------------------------------------------------ host path
+
+namespace {
+
+// Field counts of each SoA array group, per cell.
+struct Layout {
+    int nc, ncom, ncol;
+    // doubles per cell
+    int in_d() const { return 2 + ncom + NPH + NPH * ncom; }             // P, T, Ni, S, xij
+    int sk_d() const { return 3 + nc; }                                  // minEig, P, T, z
+    int out_d() const
+    {
+        return NPH + 3 + ncom + 6 * NPH + 4 * NPH * ncom + NPH * ncol * ncol + NPH + 1;  // + nj, ePEC
+    }
+    int u32() const { return 1 + 1 + NPH + 1 + NPH + NPH + 1 + 5; }   // lastNP, phaseNum, phaseExist,
+                                                                     // bRow, pSder, pVnum, skflag, iters
+    int u16() const { return 1; }
+    int u8() const { return 1; }
+    size_t bytes_per_cell() const
+    {
+        return (size_t)(in_d() + sk_d() + out_d()) * 8 + (size_t)u32() * 4 + u16() * 2 + u8();
+    }
+};
+
+// Bytes of one staging buffer, rounded up to 256 so that the second buffer
+// (and every array carved from it) stays aligned.
+inline size_t stage_stride(size_t per_cell, int64_t cap) { return ((per_cell * (size_t)cap + 255) / 256) * 256; }
+
+// Carves per-chunk device views out of one staging block (stride = cap).
+struct Views {
+    ocpf_fim_in  in;
+    ocpf_skip    sk;
+    ocpf_fim_out out;
+};
+
+Views carve(void* base, int64_t cap, const Layout& L, const ocpf_skip* hsk, const ocpf_fim_out* ho)
+{
+    Views   v{};
+    char*   p   = (char*)base;
+    auto    D   = [&](int nf) { double* r = (double*)p; p += (size_t)nf * cap * 8; return r; };
+    auto    U32 = [&](int nf) { uint32_t* r = (uint32_t*)p; p += (size_t)nf * cap * 4; return r; };
+    v.in.P          = D(1);
+    v.in.T          = D(1);
+    v.in.Ni         = D(L.ncom);
+    v.in.S          = D(NPH);
+    v.in.xij        = D(NPH * L.ncom);
+    v.sk.minEig     = D(1);
+    v.sk.P          = D(1);
+    v.sk.T          = D(1);
+    v.sk.z          = D(L.nc);
+    v.out.S         = D(NPH);
+    v.out.Nt        = D(1);
+    v.out.vf        = D(1);
+    v.out.vfP       = D(1);
+    v.out.vfi       = D(L.ncom);
+    v.out.rho       = D(NPH);
+    v.out.xi        = D(NPH);
+    v.out.mu        = D(NPH);
+    v.out.rhoP      = D(NPH);
+    v.out.xiP       = D(NPH);
+    v.out.muP       = D(NPH);
+    v.out.xij       = D(NPH * L.ncom);
+    v.out.rhox      = D(NPH * L.ncom);
+    v.out.xix       = D(NPH * L.ncom);
+    v.out.mux       = D(NPH * L.ncom);
+    v.out.dSec_dPri = D(NPH * L.ncol * L.ncol);
+    v.out.nj        = D(NPH);
+    v.out.ePEC      = D(1);
+    v.in.lastNP     = U32(1);
+    v.out.phaseNum  = U32(1);
+    v.out.phaseExist = U32(NPH);
+    v.out.bRowSizedSdP = U32(1);
+    v.out.pSderExist = U32(NPH);
+    v.out.pVnumCom  = U32(NPH);
+    v.sk.flag       = U32(1);
+    v.out.iters     = (int32_t*)U32(5);
+    v.out.status    = (uint16_t*)p;
+    p += (size_t)cap * 2;
+    v.out.ftype = (uint8_t*)p;
+    p += (size_t)cap;
+    if (!hsk) v.sk = ocpf_skip{};
+    if (!ho->nj) v.out.nj = nullptr;
+    if (!ho->ePEC) v.out.ePEC = nullptr;
+    if (!ho->iters) v.out.iters = nullptr;
+    if (!ho->status) v.out.status = nullptr;
+    if (!ho->ftype) v.out.ftype = nullptr;
+    return v;
+}
+
+// Copies nf fields of `esz`-byte elements for cells [c0, c0+cnt) between a
+// host SoA array (stride ncell) and a staging array (stride cap).
+inline cudaError_t copy_fields(void* dst, const void* src, int nf, size_t esz, int64_t c0,
+                               int64_t cnt, int64_t ncell, int64_t cap, bool h2d, cudaStream_t st)
+{
+    if (!dst || !src || cnt == 0) return cudaSuccess;
+    if (h2d)
+        return cudaMemcpy2DAsync(dst, cap * esz, (const char*)src + c0 * esz, ncell * esz, cnt * esz,
+                                 nf, cudaMemcpyHostToDevice, st);
+    return cudaMemcpy2DAsync((char*)dst + c0 * esz, ncell * esz, src, cap * esz, cnt * esz, nf,
+                             cudaMemcpyDeviceToHost, st);
+}
+
+}  // namespace
+
+extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* sk,
+                                   ocpf_fim_out* out, int form)
+{
+    if (!c || ncell < 0) return OCPF_EINVAL;
+    if (ncell == 0) return OCPF_OK;
+    if (!fim_args_ok(c, in, sk, out)) return OCPF_EINVAL;
+    if (form != OCPF_FORM_PLAIN && form != OCPF_FORM_FAST) return OCPF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    int rc = OCPF_OK;
+    Layout L{c->fc.nc, c->fc.nc + 1, c->fc.nc + 2};
+    const int64_t chunk = std::min<int64_t>(ncell, 131072);
+    const size_t  per   = L.bytes_per_cell();
+    if (c->stage_cap < chunk) {
+        if (c->stage) cudaFree(c->stage);
+        c->stage     = nullptr;
+        c->stage_cap = 0;
+        if (cudaMalloc(&c->stage, 2 * stage_stride(per, chunk)) != cudaSuccess) {
+            if (prev != c->device) cudaSetDevice(prev);
+            return OCPF_ENOMEM;
+        }
+        c->stage_cap = chunk;
+    }
+    for (auto& s : c->hs)
+        if (!s) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    const int64_t cap = c->stage_cap;
+    Views         V[2];
+    for (int b = 0; b < 2; b++) V[b] = carve((char*)c->stage + b * stage_stride(per, cap), cap, L, sk, out);
+    const bool use_sk = c->fc.use_skip != 0;
+    int        bidx   = 0;
+    for (int64_t c0 = 0; c0 < ncell && rc == OCPF_OK; c0 += cap, bidx ^= 1) {
+        const int64_t cnt = std::min<int64_t>(cap, ncell - c0);
+        cudaStream_t  st  = c->hs[bidx];
+        const Views&  v   = V[bidx];
+        cudaError_t   e   = cudaSuccess;
+        auto H = [&](void* d, const void* s, int nf, size_t esz) {
+            if (e == cudaSuccess) e = copy_fields(d, s, nf, esz, c0, cnt, ncell, cap, true, st);
+        };
+        auto D = [&](void* h, const void* d, int nf, size_t esz) {
+            if (e == cudaSuccess && h && d) e = copy_fields(h, d, nf, esz, c0, cnt, ncell, cap, false, st);
+        };
+        H((void*)v.in.P, in->P, 1, 8);
+        H((void*)v.in.T, in->T, 1, 8);
+        H((void*)v.in.Ni, in->Ni, L.ncom, 8);
+        H((void*)v.in.S, in->S, NPH, 8);
+        H((void*)v.in.xij, in->xij, NPH * L.ncom, 8);
+        H((void*)v.in.lastNP, in->lastNP, 1, 4);
+        // outputs of absent phases are left untouched: stage the caller's values
+        H(v.out.rho, out->rho, NPH, 8);
+        H(v.out.xi, out->xi, NPH, 8);
+        H(v.out.mu, out->mu, NPH, 8);
+        H(v.out.rhoP, out->rhoP, NPH, 8);
+        H(v.out.xiP, out->xiP, NPH, 8);
+        H(v.out.muP, out->muP, NPH, 8);
+        H(v.out.xij, out->xij, NPH * L.ncom, 8);
+        H(v.out.rhox, out->rhox, NPH * L.ncom, 8);
+        H(v.out.xix, out->xix, NPH * L.ncom, 8);
+        H(v.out.mux, out->mux, NPH * L.ncom, 8);
+        if (out->nj) H(v.out.nj, out->nj, NPH, 8);
+        if (use_sk) {
+            H(v.sk.flag, sk->flag, 1, 4);
+            H(v.sk.minEig, sk->minEig, 1, 8);
+            H(v.sk.P, sk->P, 1, 8);
+            H(v.sk.T, sk->T, 1, 8);
+            H(v.sk.z, sk->z, L.nc, 8);
+        }
+        if (e != cudaSuccess) {
+            rc = OCPF_ECUDA;
+            break;
+        }
+        rc = launch_plain(c, cnt, cap, v.in, v.sk, v.out, st, false);
+        if (rc != OCPF_OK) break;
+        D(out->phaseNum, v.out.phaseNum, 1, 4);
+        D(out->phaseExist, v.out.phaseExist, NPH, 4);
+        D(out->S, v.out.S, NPH, 8);
+        D(out->Nt, v.out.Nt, 1, 8);
+        D(out->vf, v.out.vf, 1, 8);
+        D(out->vfP, v.out.vfP, 1, 8);
+        D(out->vfi, v.out.vfi, L.ncom, 8);
+        D(out->rho, v.out.rho, NPH, 8);
+        D(out->xi, v.out.xi, NPH, 8);
+        D(out->mu, v.out.mu, NPH, 8);
+        D(out->rhoP, v.out.rhoP, NPH, 8);
+        D(out->xiP, v.out.xiP, NPH, 8);
+        D(out->muP, v.out.muP, NPH, 8);
+        D(out->xij, v.out.xij, NPH * L.ncom, 8);
+        D(out->rhox, v.out.rhox, NPH * L.ncom, 8);
+        D(out->xix, v.out.xix, NPH * L.ncom, 8);
+        D(out->mux, v.out.mux, NPH * L.ncom, 8);
+        D(out->dSec_dPri, v.out.dSec_dPri, NPH * L.ncol * L.ncol, 8);
+        D(out->bRowSizedSdP, v.out.bRowSizedSdP, 1, 4);
+        D(out->pSderExist, v.out.pSderExist, NPH, 4);
+        D(out->pVnumCom, v.out.pVnumCom, NPH, 4);
+        D(out->nj, v.out.nj, NPH, 8);
+        D(out->ePEC, v.out.ePEC, 1, 8);
+        D(out->ftype, v.out.ftype, 1, 1);
+        D(out->iters, v.out.iters, 5, 4);
+        D(out->status, v.out.status, 1, 2);
+        if (use_sk) {
+            D(sk->flag, v.sk.flag, 1, 4);
+            D(sk->minEig, v.sk.minEig, 1, 8);
+            D(sk->P, v.sk.P, 1, 8);
+            D(sk->T, v.sk.T, 1, 8);
+            D(sk->z, v.sk.z, L.nc, 8);
+        }
+        if (e != cudaSuccess) rc = OCPF_ECUDA;
+    }
+    for (auto& s : c->hs)
+        if (cudaStreamSynchronize(s) != cudaSuccess) rc = OCPF_ECUDA;
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}

@@ -1,0 +1,747 @@
+// flash_cell.cuh -- one cell's FIM flash in FP64 on one thread, with a
+// compile-time component count NC so every per-component array lives in
+// registers. This is the plain (drop-in) form: it evaluates the reference's
+// algorithm and formulas (src/MixtureComp.cpp) step by step; the cited line
+// ranges say which reference function each method follows.
+#pragma once
+
+#include "flash_math.cuh"
+
+namespace ocpf {
+
+template <int NC>
+struct CellFlash {
+    static constexpr int NUMCOM = NC + 1;
+    static constexpr int NCOL   = NC + 2;  // dXsdXp columns: P, N_1..N_nc, N_w
+
+    const FluidConst& F;
+    // cell state
+    double P, T, Nh;
+    double Ni[NUMCOM];
+    double zi[NC];
+    double Ai[NC], Bi[NC], sA[NC];  // sA = sqrt(Ai)
+    int    NP, lNP, ftype;
+    bool   flagSkip;
+    double nu[2];
+    double x[2][NC];
+    double phi[2][NC], fug[2][NC];
+    double Aj[2], Bj[2], Zj[2];
+    double Kw0[NC], Ks[NC], lKs[NC];
+    double Yt;
+    double n[2][NC];
+    // convergence bookkeeping (include/MixtureComp.hpp:28-92)
+    bool   ssmsta_conflag, nrsta_conflag, ssmsp_conflag, nrsp_conflag;
+    double ssmsta_realTol, nrsta_realTol, ssmsp_realTol, nrsp_realTol;
+    int    it_ssmsta, it_nrsta, it_ssmsp, it_nrsp, it_rr;
+    uint16_t status;
+    double ePEC;
+
+    __device__ __forceinline__ explicit CellFlash(const FluidConst& f) : F(f) {}
+
+    __device__ __forceinline__ double omb(int i, int k) const { return F.omb[i * MAXNC + k]; }
+
+    // CalAiBi, src/MixtureComp.cpp:916-937 (m(omega) precomputed per fluid)
+    __device__ __forceinline__ void cal_ai_bi()
+    {
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            const double Pri = P / F.Pc[i];
+            const double Tri = T / F.Tc[i];
+            Ai[i]            = F.OmegaA[i] * Pri / (Tri * Tri) * sq(1 + F.mwi[i] * (1 - sqrt(Tri)));
+            Bi[i]            = F.OmegaB[i] * Pri / Tri;
+            sA[i]            = sqrt(Ai[i]);
+        }
+    }
+
+    // Mixture parameters and the per-component sums t_i = sum_k a_ik x_k with
+    // a_ik = (1 - k_ik) sqrt(A_i A_k) (CalAjBj, src/MixtureComp.cpp:939-969;
+    // the inner sums of CalFugPhi, :1004-1008).
+    __device__ __forceinline__ void mix_ab(const double* xj, double* t, double& aj, double& bj) const
+    {
+        double w[NC];
+#pragma unroll
+        for (int k = 0; k < NC; k++) w[k] = sA[k] * xj[k];
+        aj = 0;
+        bj = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            double s = 0;
+#pragma unroll
+            for (int k = 0; k < NC; k++) s += omb(i, k) * w[k];
+            t[i] = sA[i] * s;
+            aj += xj[i] * t[i];
+            bj += Bi[i] * xj[i];
+        }
+    }
+
+    // CalFugPhi (src/MixtureComp.cpp:993-1101): ln phi, phi and fugacity of
+    // composition xj; phiT may be null. Returns the mixture a, b, Z.
+    __device__ __forceinline__ void fug_phi(const double* xj, double* phiT, double* fugT, double& aj,
+                                            double& bj, double& zj) const
+    {
+        double t[NC];
+        mix_ab(xj, t, aj, bj);
+        zj               = sol_eos(aj, bj);
+        const double L1  = log(zj - bj);
+        const double L2  = log((zj + D1 * bj) / (zj + D2 * bj));
+        const double ib  = 1.0 / bj;
+        const double ia  = 1.0 / aj;
+        const double cf  = aj / D1MD2 * ib;
+        const double zm1 = zj - 1;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            const double bi = Bi[i] * ib;
+            const double ph = exp(bi * zm1 - L1 - cf * (2 * t[i] * ia - bi) * L2);
+            if (phiT) phiT[i] = ph;
+            fugT[i] = ph * xj[i] * P;
+        }
+    }
+
+    // CalFugPhiAll, src/MixtureComp.cpp:1103-1145
+    __device__ __forceinline__ void fug_phi_all()
+    {
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            if (j < NP) fug_phi(x[j], phi[j], fug[j], Aj[j], Bj[j], Zj[j]);
+        }
+    }
+
+    // CalKwilson, src/MixtureComp.cpp:1269-1277 (Kw[1..3] are formed from
+    // Kw[0] where they are used).
+    __device__ __forceinline__ void cal_kwilson()
+    {
+#pragma unroll
+        for (int i = 0; i < NC; i++)
+            Kw0[i] = (F.Pc[i] / P) * exp(5.373 * (1 + F.Acf[i]) * (1 - F.Tc[i] / T));
+    }
+    __device__ __forceinline__ double kw(int k, int i) const
+    {
+        const double k0 = Kw0[i];
+        if (k == 0) return k0;
+        if (k == 1) return 1 / k0;
+        if (k == 2) return pow(k0, 1.0 / 3);
+        return pow(1 / k0, 1.0 / 3);
+    }
+
+    // ---------------- stability ------------------------------------------
+
+    // StableNR with CalFugXSTA / AssembleJmatSTA / SYSSolve('U'),
+    // src/MixtureComp.cpp:1590-1741. The reference hands the row-major
+    // Jacobian to dsysv('U'), which reads its lower triangle as the upper
+    // triangle of a symmetric matrix; the same symmetric matrix is solved here.
+    __device__ bool stable_nr(const double* fugId, double* Y, double* fugSta, double& Asta,
+                              double& Bsta, double& Zsta)
+    {
+        double res[NC];
+#pragma unroll
+        for (int i = 0; i < NC; i++) res[i] = log(fugId[i] / (fugSta[i] * Yt));
+        double Se = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) Se += res[i] * res[i];
+        Se       = sqrt(Se);
+        int iter = 0;
+        while (Se > F.nrsta_tol) {
+            // CalFugXSTA, src/MixtureComp.cpp:1638-1714
+            double       M[NC][NC];
+            {
+                const double aj = Asta, bj = Bsta, zj = Zsta;
+                double       Ax[NC], Zx[NC];
+                double       t[NC];
+                {
+                    double w[NC];
+#pragma unroll
+                    for (int k = 0; k < NC; k++) w[k] = sA[k] * Y[k];
+#pragma unroll
+                    for (int i = 0; i < NC; i++) {
+                        double s = 0;
+#pragma unroll
+                        for (int k = 0; k < NC; k++) s += omb(i, k) * w[k];
+                        t[i] = sA[i] * s;
+                    }
+                }
+                const DzCoef dz(aj, bj, zj);
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    Ax[i] = 2 * t[i];
+                    Zx[i] = dz(Ax[i], Bi[i]);
+                }
+                const double zmb  = zj - bj;
+                const double G    = (zj + D1 * bj) / (zj + D2 * bj);
+                const double lnG  = log(G);
+                const double ib   = 1.0 / bj;
+                const double zd2  = zj + D2 * bj;
+                const double gfac = D1MD2 / zd2 / zd2;
+                double       fx[NC][NC];
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    const double E = -aj / (D1MD2 * bj) * (Ax[i] / aj - Bi[i] * ib);
+#pragma unroll
+                    for (int k = 0; k < NC; k++) {
+                        const double a_ik = omb(i, k) * sA[i] * sA[k];
+                        // 1/C * Cxk with C = Y_i P / (z - b)
+                        const double cterm = (zmb * dlt(i, k) - Y[i] * (Zx[k] - Bi[k])) / (Y[i] * zmb);
+                        const double Dxk   = Bi[i] * ib * (Zx[k] - Bi[k] * (zj - 1) * ib);
+                        double       Exk   = (2 * (aj * ib * Bi[k] * Bi[i] + bj * a_ik) - Ax[i] * Bi[k] -
+                                      Ax[k] * Bi[i]) *
+                                     (ib * ib);
+                        Exk /= -D1MD2;
+                        const double Gxk = gfac * (zj * Bi[k] - Zx[k] * bj);
+                        fx[i][k]         = cterm + Dxk + Exk * lnG + E / G * Gxk;
+                    }
+                }
+                // AssembleJmatSTA: J[i][j] = (fx[i][j] - sum_k Y_k fx[i][k] + 1) / Yt;
+                // symmetric matrix from J's lower triangle.
+                const double iYt = 1.0 / Yt;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    double s = 0;
+#pragma unroll
+                    for (int k = 0; k < NC; k++) s += Y[k] * fx[i][k];
+#pragma unroll
+                    for (int j = 0; j <= i; j++) {
+                        M[i][j] = (fx[i][j] - s + 1) * iYt;
+                        M[j][i] = M[i][j];
+                    }
+                }
+            }
+            double B[NC][1];
+#pragma unroll
+            for (int i = 0; i < NC; i++) B[i][0] = res[i];
+            if (gauss_solve<NC, 1>(M, B)) {
+#pragma unroll
+                for (int i = 0; i < NC; i++) res[i] = B[i][0];
+            } else {
+                status |= ST_SINGULAR;  // dsysv leaves the right-hand side unchanged
+            }
+            double ys = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                Y[i] = Y[i] * Yt + res[i];
+                ys += Y[i];
+            }
+            Yt             = ys;
+            const double r = 1 / Yt;
+#pragma unroll
+            for (int i = 0; i < NC; i++) Y[i] *= r;
+            fug_phi(Y, nullptr, fugSta, Asta, Bsta, Zsta);
+            Se = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                res[i] = log(fugId[i] / (fugSta[i] * Yt));
+                Se += res[i] * res[i];
+            }
+            Se = sqrt(Se);
+            iter++;
+            if (iter > F.nrsta_maxit) {
+                it_nrsta += iter;
+                status |= ST_NRSTA_FAIL;
+                nrsta_conflag = false;
+                nrsta_realTol = Se;
+                return false;
+            }
+        }
+        it_nrsta += iter;
+        nrsta_conflag = true;
+        nrsta_realTol = Se;
+        return true;
+    }
+
+    // StableSSM (strict, four Wilson trials), src/MixtureComp.cpp:1492-1588.
+    // Tests phase 0 (the only phase when PhaseStable runs on this path).
+    __device__ bool stable_ssm()
+    {
+        double phiId[NC], fugId[NC], di[NC];
+        double aj0, bj0, zj0;
+        fug_phi(x[0], phiId, fugId, aj0, bj0, zj0);
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            phi[0][i] = phiId[i];
+            fug[0][i] = fugId[i];
+            di[i]     = phiId[i] * x[0][i];
+        }
+        double Se = 0;
+        for (int k = 0; k < 4; k++) {
+            double Y[NC], phiSta[NC], fugSta[NC], Asta, Bsta, Zsta;
+            Yt = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                Y[i] = x[0][i] / kw(k, i);
+                Yt += Y[i];
+            }
+            double r = 1 / Yt;
+#pragma unroll
+            for (int i = 0; i < NC; i++) Y[i] *= r;
+            fug_phi(Y, phiSta, fugSta, Asta, Bsta, Zsta);
+            Se = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) Se += sq(log(fugSta[i] / fugId[i] * Yt));
+            int iter = 0;
+            while (Se > F.ssmsta_tol2) {
+                Yt = 0;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    Y[i] = di[i] / phiSta[i];
+                    Yt += Y[i];
+                }
+                r = 1 / Yt;
+#pragma unroll
+                for (int i = 0; i < NC; i++) Y[i] *= r;
+                fug_phi(Y, phiSta, fugSta, Asta, Bsta, Zsta);
+                Se = 0;
+#pragma unroll
+                for (int i = 0; i < NC; i++) Se += sq(log(fugSta[i] / fugId[i] * Yt));
+                iter++;
+                if (iter > F.ssmsta_maxit) {
+                    status |= ST_SSMSTA_CAP;
+                    break;
+                }
+            }
+            it_ssmsta += iter;
+            const bool flag = stable_nr(fugId, Y, fugSta, Asta, Bsta, Zsta);
+            if (flag && Yt > 1 + F.ssmsta_eyt) {
+                ssmsta_conflag = true;
+                ssmsta_realTol = sqrt(Se);
+                return false;
+            }
+        }
+        ssmsta_realTol = sqrt(Se);
+        return true;
+    }
+
+    // StableSSM01 (relaxed, two Wilson trials with trivial-solution exit),
+    // src/MixtureComp.cpp:1392-1490
+    __device__ bool stable_ssm01()
+    {
+        double fugId[NC];
+        {
+            double aj0, bj0, zj0;
+            fug_phi(x[0], phi[0], fugId, aj0, bj0, zj0);
+#pragma unroll
+            for (int i = 0; i < NC; i++) fug[0][i] = fugId[i];
+        }
+        double Se = 0, Sk = 0;
+        for (int k = 0; k < 2; k++) {
+            double ks[NC], Y[NC], di[NC], fugSta[NC];
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                ks[i] = kw(k, i);
+                di[i] = 0;
+            }
+            int  iter = 0;
+            bool flag = false;
+            while (true) {
+                Yt = 0;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    Y[i] = x[0][i] * ks[i];
+                    Yt += Y[i];
+                }
+                const double r = 1 / Yt;
+#pragma unroll
+                for (int i = 0; i < NC; i++) Y[i] *= r;
+                if (iter > 0) {
+                    double dY = 0;
+#pragma unroll
+                    for (int i = 0; i < NC; i++) dY += sq(Y[i] - di[i]);
+                    if (dY < 1e-6) {  // dYtol, include/MixtureComp.hpp:34
+                        flag = true;
+                        break;
+                    }
+                }
+                double a_, b_, z_;
+                fug_phi(Y, nullptr, fugSta, a_, b_, z_);
+                Se = 0;
+                Sk = 0;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    di[i] = fugId[i] / (fugSta[i] * Yt);
+                    ks[i] *= di[i];
+                    Se += sq(di[i] - 1);
+                    Sk += sq(log(ks[i]));
+                }
+                iter++;
+                if (Se < F.ssmsta_tol2) {
+                    flag = true;
+                    break;
+                }
+                if (Sk < 1e-4) {  // Ktol, include/MixtureComp.hpp:33
+                    flag = true;
+                    break;
+                }
+                if (iter > F.ssmsta_maxit) {
+                    status |= ST_SSMSTA_CAP;
+                    break;
+                }
+#pragma unroll
+                for (int i = 0; i < NC; i++) di[i] = Y[i];
+            }
+            it_ssmsta += iter;
+            if (flag && Yt > 1 - 0.1 && Sk > 1) flagSkip = false;
+            if (flag && Yt > 1 + F.ssmsta_eyt) {
+                ssmsta_conflag = true;
+                ssmsta_realTol = sqrt(Se);
+                return false;
+            }
+        }
+        ssmsta_realTol = sqrt(Se);
+        return true;
+    }
+
+    // PhaseStable, src/MixtureComp.cpp:1355-1390 (NP = 1 on this path)
+    __device__ bool phase_stable()
+    {
+        ssmsta_conflag = false;
+        nrsta_conflag  = false;
+        bool flag;
+        int  tmpNP = NP;
+        if (lNP == 0) {
+            flag = stable_ssm();
+        } else {
+            flag = stable_ssm01();
+            if (!flag) tmpNP++;
+            if (tmpNP != lNP) {
+                flag     = stable_ssm();
+                flagSkip = false;
+            }
+        }
+        return flag;
+    }
+
+    // ---------------- phase split ----------------------------------------
+
+    // RachfordRice2, src/MixtureComp.cpp:1907-1959
+    __device__ void rachford_rice2()
+    {
+        double Kmin = Ks[0], Kmax = Ks[0];
+#pragma unroll
+        for (int i = 1; i < NC; i++) {
+            if (Ks[i] < Kmin) Kmin = Ks[i];
+            if (Ks[i] > Kmax) Kmax = Ks[i];
+        }
+        const double numin = 1 / (1 - Kmax);
+        const double numax = 1 / (1 - Kmin);
+        double       v     = 0.5 * (numin + numax);
+        int          iter  = 0;
+        while (true) {
+            double rj = 0, J = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                const double km1 = Ks[i] - 1;
+                const double tmp = 1 + v * km1;
+                rj += zi[i] * km1 / tmp;
+                J -= zi[i] * km1 * km1 / (tmp * tmp);
+            }
+            if (fabs(rj) < F.rr_tol || iter > F.rr_maxit) break;
+            const double dnuj  = -rj / J;
+            const double tmpnu = v + dnuj;
+            if (tmpnu < numax && tmpnu > numin)
+                v = tmpnu;
+            else if (dnuj > 0)
+                v = (v + numax) / 2;
+            else
+                v = (v + numin) / 2;
+            iter++;
+        }
+        it_rr += iter;
+        nu[0] = v;
+        nu[1] = 1 - v;
+    }
+
+    // SplitSSM2 with UpdateXRR, src/MixtureComp.cpp:1847-1903, 2030-2043
+    __device__ void split_ssm2(bool restart)
+    {
+        ssmsp_conflag = true;
+        double Se     = 1;
+        double Stol   = F.ssmsp_tol2;
+        int    maxIt  = F.ssmsp_maxit;
+        if (!restart) {
+#pragma unroll
+            for (int i = 0; i < NC; i++) Ks[i] = (lNP == 2) ? lKs[i] : Kw0[i];
+        } else {
+            Stol *= 1e-1;
+            maxIt *= 2;
+        }
+        if (Yt < 1.1) {
+            Stol *= 1e-1;
+            maxIt *= 2;
+        }
+        int iter = 0;
+        while (Se > Stol) {
+            rachford_rice2();
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                const double tmp = 1 + nu[0] * (Ks[i] - 1);
+                x[1][i]          = zi[i] / tmp;
+                x[0][i]          = Ks[i] * x[1][i];
+            }
+            fug_phi_all();
+            Se = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                Se += sq(fug[1][i] / fug[0][i] - 1);
+                Ks[i] = phi[1][i] / phi[0][i];
+            }
+            iter++;
+            if (iter > maxIt) {
+                ssmsp_conflag = false;
+                break;
+            }
+        }
+        ssmsp_realTol = sqrt(Se);
+        it_ssmsp += iter;
+    }
+
+    // Sum over the two phases of d ln f_ij / d n_kj (CalFugNAll,
+    // src/MixtureComp.cpp:2168-2250, Znflag true) for phase j into S and,
+    // if R is non-null, phase 1's matrix alone into R; also returns Zn.
+    __device__ __forceinline__ void fugn_phase(int j, double (&S)[NC][NC], bool accumulate,
+                                               double (*R)[NC], double* Znj) const
+    {
+        const double  aj = Aj[j], bj = Bj[j], zj = Zj[j], nuj = nu[j];
+        const double* xj = x[j];
+        double        t[NC], An[NC], Bn[NC];
+        {
+            double w[NC];
+#pragma unroll
+            for (int k = 0; k < NC; k++) w[k] = sA[k] * xj[k];
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                double s = 0;
+#pragma unroll
+                for (int k = 0; k < NC; k++) s += omb(i, k) * w[k];
+                t[i] = sA[i] * s;
+            }
+        }
+        const DzCoef dz(aj, bj, zj);
+        const double inu = 1.0 / nuj;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            An[i]  = 2 * inu * (t[i] - aj);
+            Bn[i]  = inu * (Bi[i] - bj);
+            Znj[i] = dz(An[i], Bn[i]);
+        }
+        const double zmb  = zj - bj;
+        const double G    = (zj + D1 * bj) / (zj + D2 * bj);
+        const double lnG  = log(G);
+        const double ib   = 1.0 / bj;
+        const double zd2  = zj + D2 * bj;
+        const double gfac = D1MD2 / (zd2 * zd2);
+        const double efac = -1 / D1MD2 * (ib * ib);
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            const double E   = -aj / (D1MD2 * bj) * (2 * t[i] / aj - Bi[i] * ib);
+            const double iC  = zmb / (xj[i] * P);
+#pragma unroll
+            for (int k = 0; k <= i; k++) {
+                const double a_ik = omb(i, k) * sA[i] * sA[k];
+                const double Cnk  = P / zmb / zmb * (zmb * inu * (dlt(i, k) - xj[i]) - xj[i] * (Znj[k] - Bn[k]));
+                const double Dnk  = Bi[i] * ib * (Znj[k] - (Bi[k] - bj) * (zj - 1) * inu * ib);
+                const double Gnk  = gfac * (Bn[k] * zj - Znj[k] * bj);
+                double       Enk  = efac * (2 * (bj * a_ik * inu + Bn[k] * (Bi[i] * aj * ib - t[i])) -
+                                   An[k] * Bi[i] - aj * Bi[i] * inu);
+                Enk -= E * inu;
+                const double v = iC * Cnk + Dnk + Enk * lnG + E / G * Gnk;
+                if (accumulate) {
+                    S[i][k] += v;
+                    if (k != i) S[k][i] += v;
+                } else {
+                    S[i][k] = v;
+                    S[k][i] = v;
+                }
+                if (R) {
+                    R[i][k] = v;
+                    R[k][i] = v;
+                }
+            }
+        }
+    }
+
+    // SplitNR with CalResSP / AssembleJmatSP / CalStepNRsp (NP = 2),
+    // src/MixtureComp.cpp:2057-2166, 2265-2319
+    __device__ void split_nr()
+    {
+        nrsp_conflag = false;
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int i = 0; i < NC; i++) n[j][i] = nu[j] * x[j][i];
+        double res[NC];
+        double eNR = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            res[i] = log(fug[1][i] / fug[0][i]);
+            eNR += res[i] * res[i];
+        }
+        eNR               = sqrt(eNR);
+        const double eNR0 = eNR;
+        int          iter = 0;
+        while (eNR > F.nrsp_tol) {
+            double ln0[NC], ln1[NC];
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                ln0[i] = n[0][i];
+                ln1[i] = n[1][i];
+            }
+            double J[NC][NC];
+            double Zn_[NC];
+            fugn_phase(0, J, false, nullptr, Zn_);
+            fugn_phase(1, J, true, nullptr, Zn_);
+            double B[NC][1];
+#pragma unroll
+            for (int i = 0; i < NC; i++) B[i][0] = res[i];
+            if (gauss_solve<NC, 1>(J, B)) {
+#pragma unroll
+                for (int i = 0; i < NC; i++) res[i] = B[i][0];
+            } else {
+                status |= ST_SINGULAR;
+            }
+            double alpha = 1;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                const double tmp = n[0][i] + alpha * res[i];
+                if (tmp < 0) alpha *= 0.9 * fabs(n[0][i] / res[i]);
+            }
+            double s0 = 0, s1 = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                n[0][i] += alpha * res[i];
+                n[1][i] = zi[i] + -1 * n[0][i];
+                s0 += n[0][i];
+                s1 += n[1][i];
+            }
+            nu[0] = s0;
+            nu[1] = s1;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                x[0][i] = fabs(n[0][i] / nu[0]);
+                x[1][i] = fabs(n[1][i] / nu[1]);
+            }
+            fug_phi_all();
+            eNR = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                res[i] = log(fug[1][i] / fug[0][i]);
+                eNR += res[i] * res[i];
+            }
+            eNR = sqrt(eNR);
+            iter++;
+            if (eNR > eNR0 || iter > F.nrsp_maxit) break;
+            double e0 = 0, e1 = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                e0 += sq(ln0[i] + -1 * n[0][i]);
+                e1 += sq(ln1[i] + -1 * n[1][i]);
+            }
+            const double en = sqrt(e0) + sqrt(e1);
+            if (en / (2 * NC) < 1e-8) {
+                nrsp_conflag = true;
+                break;
+            }
+        }
+        nrsp_realTol = eNR;
+        if (eNR < F.nrsp_tol) nrsp_conflag = true;
+        it_nrsp += iter;
+    }
+
+    // CheckSplit, src/MixtureComp.cpp:1784-1836 (its Gibbs-energy evaluation
+    // only feeds a diagnostic print and is not repeated here)
+    __device__ bool check_split()
+    {
+        if (NP == 2) {
+            double       eX    = 0;
+            const double nuMax = (nu[0] < nu[1]) ? nu[1] : nu[0];
+#pragma unroll
+            for (int i = 0; i < NC; i++) eX += (x[0][i] - x[1][i]) * (x[0][i] - x[1][i]);
+            if (nuMax < 1 && nrsp_conflag && isfinite(eX)) {
+                // accept
+            } else if (!isfinite(eX) || 1 - nuMax < 1e-3) {
+                NP = 1;
+#pragma unroll
+                for (int i = 0; i < NC; i++) x[0][i] = zi[i];
+                nu[0] = 1;
+                double t[NC];
+                mix_ab(x[0], t, Aj[0], Bj[0]);
+                Zj[0]          = sol_eos(Aj[0], Bj[0]);
+                ssmsta_conflag = false;
+                nrsta_conflag  = false;
+                status |= ST_COLLAPSED;
+                return false;
+            }
+        }
+        return true;
+    }
+
+    // PhaseSplit, src/MixtureComp.cpp:1743-1782
+    __device__ void phase_split()
+    {
+        ssmsp_conflag = false;
+        nrsp_conflag  = false;
+        split_ssm2(false);
+        split_nr();
+        int guard = 0;
+        while (!nrsp_conflag) {
+            if (++guard > SPLIT_RESTART_CAP) {
+                status |= ST_SPLIT_CAP;
+                break;
+            }
+            split_ssm2(true);
+            split_nr();
+            if (!check_split()) break;
+            if (ssmsp_conflag) break;
+        }
+        check_split();
+        if (!ssmsp_conflag) status |= ST_SSMSP_FAIL;
+        if (!nrsp_conflag) status |= ST_NRSP_FAIL;
+    }
+
+    // PhaseEquilibrium, src/MixtureComp.cpp:1279-1353 (NPmax = 2)
+    __device__ void phase_equilibrium()
+    {
+        if (ftype == 0) {
+            flagSkip = true;
+            NP       = 1;
+            nu[0]    = 1;
+#pragma unroll
+            for (int i = 0; i < NC; i++) x[0][i] = zi[i];
+            cal_ai_bi();
+            {
+                double t[NC];
+                mix_ab(x[0], t, Aj[0], Bj[0]);
+            }
+            Zj[0] = sol_eos(Aj[0], Bj[0]);
+            cal_kwilson();
+            if (!phase_stable()) {
+                NP++;
+                phase_split();
+            }
+            if (NP > 1) flagSkip = false;
+            if (NP == 1)
+                ePEC = nrsta_conflag ? nrsta_realTol : (ssmsta_conflag ? ssmsta_realTol : 1e8);
+            else
+                ePEC = nrsp_conflag ? nrsp_realTol : (ssmsp_conflag ? ssmsp_realTol : 1e8);
+        } else if (ftype == 1) {
+            flagSkip = true;
+            NP       = 1;
+            nu[0]    = 1;
+#pragma unroll
+            for (int i = 0; i < NC; i++) x[0][i] = zi[i];
+            cal_ai_bi();
+            {
+                double t[NC];
+                mix_ab(x[0], t, Aj[0], Bj[0]);
+            }
+            Zj[0] = sol_eos(Aj[0], Bj[0]);
+            ePEC  = 0.0;
+        } else {
+            flagSkip = false;
+            NP       = 2;
+            Yt       = 1.01;
+            cal_ai_bi();
+            cal_kwilson();
+            phase_split();
+            ePEC = nrsp_conflag ? nrsp_realTol : (ssmsp_conflag ? ssmsp_realTol : 1e8);
+        }
+    }
+};
+
+}  // namespace ocpf

@@ -1,0 +1,68 @@
+// flash_common.cuh -- constants, the per-fluid constant block and small
+// helpers shared by the flash kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "ocp_flash.h"
+
+namespace ocpf {
+
+constexpr int MAXNC = OCPF_MAX_NC;
+constexpr int NPH   = OCPF_NUM_PHASE;  // oil, gas, water
+
+// include/OCPConst.hpp:37-69 and include/MixtureComp.hpp:350-351
+constexpr double GAS_CONSTANT = 10.73159;
+constexpr double PI_TRUNC     = 3.141592653;  // truncated, as the reference uses it
+constexpr double CONV1        = 5.61458;
+constexpr double CONV5        = 459.67;
+constexpr double D1           = 2.41421356237;
+constexpr double D2           = -0.41421356237;
+constexpr double D1PD2        = D1 + D2;
+constexpr double D1MD2        = D1 - D2;
+constexpr double D1TD2        = D1 * D2;
+
+// Everything a flash of one fluid reads that does not depend on the cell.
+// Passed by value as a __grid_constant__ kernel parameter, so that with a
+// compile-time component count every access is a constant-bank operand.
+// Fixed row stride MAXNC keeps those offsets compile-time constants.
+struct FluidConst {
+    int32_t nc;
+    int32_t use_skip;
+    int32_t rr_maxit, ssmsta_maxit, nrsta_maxit, ssmsp_maxit, nrsp_maxit, pad;
+    double  rr_tol, ssmsta_tol2, ssmsta_eyt, nrsta_tol, ssmsp_tol2, nrsp_tol;
+    double  Tc[MAXNC], Pc[MAXNC], Vc[MAXNC], Vcvis[MAXNC], MW[MAXNC], Acf[MAXNC];
+    double  OmegaA[MAXNC], OmegaB[MAXNC], Vshift[MAXNC];
+    double  mwi[MAXNC];          // PR m(omega), src/MixtureComp.cpp:923-929
+    double  sqrtMW[MAXNC];       // sqrtMWi, src/MixtureComp.cpp:2323-2324
+    double  muAux1I[MAXNC];      // src/MixtureComp.cpp:2330-2333
+    double  lbc1[MAXNC];         // 5.4402 Tc^(1/6)
+    double  lbc2[MAXNC];         // Pc^(2/3)
+    double  omb[MAXNC * MAXNC];  // 1 - BIC, row stride MAXNC
+    double  L[5];                // LBC coefficients x 10
+    double  pvtw[5];
+    double  std_rho_w;
+};
+
+// per-cell status bits mirror OCPF_CELL_*
+constexpr uint16_t ST_SSMSTA_CAP = OCPF_CELL_SSMSTA_CAP;
+constexpr uint16_t ST_NRSTA_FAIL = OCPF_CELL_NRSTA_FAIL;
+constexpr uint16_t ST_SSMSP_FAIL = OCPF_CELL_SSMSP_FAIL;
+constexpr uint16_t ST_NRSP_FAIL  = OCPF_CELL_NRSP_FAIL;
+constexpr uint16_t ST_COLLAPSED  = OCPF_CELL_COLLAPSED;
+constexpr uint16_t ST_SINGULAR   = OCPF_CELL_SINGULAR;
+constexpr uint16_t ST_NONFINITE  = OCPF_CELL_NONFINITE;
+constexpr uint16_t ST_SPLIT_CAP  = OCPF_CELL_SPLIT_CAP;
+
+// Bound on PhaseSplit's restart loop (src/MixtureComp.cpp:1752-1757 has none).
+constexpr int SPLIT_RESTART_CAP = 1000;
+
+__device__ __forceinline__ double sq(double v) { return v * v; }
+__device__ __forceinline__ double dlt(int i, int k) { return i == k ? 1.0 : 0.0; }
+
+// Host-side derivation of the constant block from the C-ABI fluid; returns
+// false on invalid input.
+bool make_fluid_const(const ocpf_fluid& in, FluidConst& out);
+
+}  // namespace ocpf

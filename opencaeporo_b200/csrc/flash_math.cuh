@@ -1,0 +1,203 @@
+// flash_math.cuh -- per-thread FP64 building blocks of the flash: the
+// Peng-Robinson cubic with its root choice, dZ derivatives, and small dense
+// solves and eigenvalues held in registers.
+#pragma once
+
+#include "flash_common.cuh"
+
+namespace ocpf {
+
+// Newton polish of one cubic root, keeping the best iterate
+// (NTcubicroot, src/MixtureComp.cpp:5078-5102).
+__device__ __forceinline__ double nt_polish(double root, double a, double b, double c)
+{
+    double e       = root * (root * (root + a) + b) + c;
+    double optroot = root;
+    double opte    = fabs(e);
+    int    iter    = 0;
+    while (fabs(e) > 1e-8) {
+        const double df = root * (3 * root + 2 * a) + b;
+        root            = root - e / df;
+        iter++;
+        if (iter > 10) break;
+        e = root * (root * (root + a) + b) + c;
+        if (fabs(e) <= opte) {
+            opte    = fabs(e);
+            optroot = root;
+        }
+    }
+    return optroot;
+}
+
+__device__ __forceinline__ double signD(double d) { return d > 0 ? 1.0 : (d < 0 ? -1.0 : 0.0); }
+
+// Z factor of the PR cubic for mixture parameters (aj, bj): Cardano /
+// trigonometric roots with the reference's truncated pi, Newton polish, and
+// for three roots the Gibbs-energy choice between the smallest and largest
+// (SolEoS + CubicRoot, src/MixtureComp.cpp:889-914, 4999-5056).
+__device__ __forceinline__ double sol_eos(double aj, double bj)
+{
+    const double a  = (D1PD2 - 1) * bj - 1;
+    const double b  = (aj + D1TD2 * bj * bj - D1PD2 * bj * (bj + 1));
+    const double c  = -(aj * bj + D1TD2 * bj * bj * (bj + 1));
+    const double Q  = (a * a - 3 * b) / 9;
+    const double R  = (2 * a * a * a - 9 * a * b + 27 * c) / 54;
+    const double Q3 = Q * Q * Q;
+    const double M  = R * R - Q3;
+    if (M <= 0) {
+        const double theta = acos(R / sqrt(Q3));
+        const double s2    = -2 * sqrt(Q);
+        const double a3    = a / 3;
+        double       z0    = nt_polish(s2 * cos(theta / 3) - a3, a, b, c);
+        double       z1    = nt_polish(s2 * cos((theta + 2 * PI_TRUNC) / 3) - a3, a, b, c);
+        double       z2    = nt_polish(s2 * cos((theta - 2 * PI_TRUNC) / 3) - a3, a, b, c);
+        const double zmin  = fmin(z0, fmin(z1, z2));
+        const double zmax  = fmax(z0, fmax(z1, z2));
+        const double dG    = (zmax - zmin) + log((zmin - bj) / (zmax - bj)) -
+                          aj / (bj * (D2 - D1)) *
+                              log((zmin + D1 * bj) * (zmax + D2 * bj) /
+                                  ((zmin + D2 * bj) * (zmax + D1 * bj)));
+        return dG > 0 ? zmin : zmax;
+    } else {
+        const double sM = sqrt(M);
+        const double t1 = -R + sM;
+        const double t2 = R + sM;
+        const double S  = signD(t1) * cbrt(fabs(t1));
+        const double T  = -signD(t2) * cbrt(fabs(t2));
+        return nt_polish(S + T - a / 3, a, b, c);
+    }
+}
+
+// dZ for a perturbation (dA, dB) of the mixture parameters: the implicit
+// derivative of the PR cubic used by CalFugXSTA, CalFugNAll, CalFugPAll,
+// CalVfiVfp_full02 and CalXiPNX_partial (e.g. src/MixtureComp.cpp:1664-1670).
+struct DzCoef {
+    double num_b, inv_den, bmz;
+    __device__ __forceinline__ DzCoef(double aj, double bj, double zj)
+    {
+        bmz   = bj - zj;
+        num_b = (aj + D1TD2 * (3 * bj * bj + 2 * bj)) +
+                (D1PD2 * (2 * bj + 1) - 2 * D1TD2 * bj) * zj - (D1PD2 - 1) * zj * zj;
+        inv_den = 1.0 / (3 * zj * zj + 2 * ((D1PD2 - 1) * bj - 1) * zj +
+                         (aj + D1TD2 * bj * bj - D1PD2 * bj * (bj + 1)));
+    }
+    __device__ __forceinline__ double operator()(double dA, double dB) const
+    {
+        return (bmz * dA + num_b * dB) * inv_den;
+    }
+};
+
+// Solves A X = B (A: N x N, B: N x M, both row-major in registers) by
+// Gaussian elimination with partial pivoting, the same pivot rule as LAPACK
+// dgetf2 (first largest magnitude). Row swaps are predicated so every index
+// stays a compile-time constant. Returns false on an exactly zero pivot;
+// A and B are then partially reduced and the caller restores B.
+template <int N, int M>
+__device__ __forceinline__ bool gauss_solve(double (&A)[N][N], double (&B)[N][M])
+{
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < N; j++) {
+        int    p  = j;
+        double mx = fabs(A[j][j]);
+#pragma unroll
+        for (int i = j + 1; i < N; i++) {
+            const double v = fabs(A[i][j]);
+            if (v > mx) {
+                mx = v;
+                p  = i;
+            }
+        }
+#pragma unroll
+        for (int i = j + 1; i < N; i++) {
+            const bool sw = (p == i);
+#pragma unroll
+            for (int c = j; c < N; c++) {
+                const double t = A[j][c];
+                A[j][c]        = sw ? A[i][c] : A[j][c];
+                A[i][c]        = sw ? t : A[i][c];
+            }
+#pragma unroll
+            for (int c = 0; c < M; c++) {
+                const double t = B[j][c];
+                B[j][c]        = sw ? B[i][c] : B[j][c];
+                B[i][c]        = sw ? t : B[i][c];
+            }
+        }
+        if (A[j][j] == 0.0) ok = false;
+        const double r = 1.0 / A[j][j];
+#pragma unroll
+        for (int i = j + 1; i < N; i++) {
+            const double l = A[i][j] * r;
+#pragma unroll
+            for (int c = j + 1; c < N; c++) A[i][c] -= l * A[j][c];
+#pragma unroll
+            for (int c = 0; c < M; c++) B[i][c] -= l * B[j][c];
+        }
+    }
+#pragma unroll
+    for (int j = N - 1; j >= 0; j--) {
+#pragma unroll
+        for (int c = 0; c < M; c++) {
+            double s = B[j][c];
+#pragma unroll
+            for (int k = j + 1; k < N; k++) s -= A[j][k] * B[k][c];
+            B[j][c] = s / A[j][j];
+        }
+    }
+    return ok;
+}
+
+// Smallest eigenvalue of a symmetric matrix given in single precision (what
+// CalEigenSY / ssyevd returns first, src/DenseMat.cpp:14-26): cyclic Jacobi in
+// FP64 on the single-precision entries, rounded to single precision.
+template <int N>
+__device__ __forceinline__ float min_eig_sym(float (&Af)[N][N])
+{
+    double a[N][N];
+#pragma unroll
+    for (int i = 0; i < N; i++)
+#pragma unroll
+        for (int j = 0; j < N; j++) a[i][j] = (double)Af[i][j];
+    for (int sweep = 0; sweep < 30; sweep++) {
+        double off = 0, dia = 0;
+#pragma unroll
+        for (int p = 0; p < N; p++) {
+            dia += a[p][p] * a[p][p];
+#pragma unroll
+            for (int q = p + 1; q < N; q++) off += a[p][q] * a[p][q];
+        }
+        if (off <= 1e-36 * dia) break;
+#pragma unroll
+        for (int p = 0; p < N - 1; p++) {
+#pragma unroll
+            for (int q = p + 1; q < N; q++) {
+                const double apq = a[p][q];
+                if (apq != 0.0) {
+                    const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+                    const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                    const double c = rsqrt(t * t + 1.0);
+                    const double s = t * c;
+#pragma unroll
+                    for (int k = 0; k < N; k++) {
+                        const double akp = a[k][p], akq = a[k][q];
+                        a[k][p] = c * akp - s * akq;
+                        a[k][q] = s * akp + c * akq;
+                    }
+#pragma unroll
+                    for (int k = 0; k < N; k++) {
+                        const double apk = a[p][k], aqk = a[q][k];
+                        a[p][k] = c * apk - s * aqk;
+                        a[q][k] = s * apk + c * aqk;
+                    }
+                }
+            }
+        }
+    }
+    double m = a[0][0];
+#pragma unroll
+    for (int i = 1; i < N; i++) m = fmin(m, a[i][i]);
+    return (float)m;
+}
+
+}  // namespace ocpf

@@ -1,0 +1,28 @@
+// flash_plain_nc12.cu -- the plain FP64 FIM flash kernel for 12 hydrocarbon
+// components (one translation unit per component count keeps builds parallel).
+#include "flash_fim.cuh"
+
+namespace ocpf {
+
+// One thread per cell, 128 cells per block: the hardware block scheduler
+// balances the very uneven per-cell iteration counts across the SMs.
+__global__ void __launch_bounds__(128) k_flash_fim_plain_nc12(const __grid_constant__ FluidConst F,
+                                                             int64_t count, int64_t stride,
+                                                             const ocpf_fim_in in, const ocpf_skip sk,
+                                                             const ocpf_fim_out out)
+{
+    const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (n >= count) return;
+    FimCell<12> c(F);
+    c.run(n, stride, in, sk, out);
+}
+
+cudaError_t launch_plain_nc12(const FluidConst& F, int64_t count, int64_t stride, const ocpf_fim_in& in,
+                              const ocpf_skip& sk, const ocpf_fim_out& out, unsigned blocks, int bs,
+                              cudaStream_t st)
+{
+    k_flash_fim_plain_nc12<<<blocks, bs, 0, st>>>(F, count, stride, in, sk, out);
+    return cudaGetLastError();
+}
+
+}  // namespace ocpf

@@ -1,0 +1,193 @@
+"""Batched compositional PR flash on the GPU: the host-side mirror of the
+reference's ``MixtureComp`` interface for the FIM path.
+
+The reference calls, for every bulk cell ``n`` (``src/OCPFluidMethod.cpp:1108-1187``)::
+
+    flashCal[PVTNUM[n]]->FlashFIM(P[n], T[n], &Ni[n*nc], &S[n*np], phaseNum[n], &xij[n*np*nc], n)
+    PassFlashValue(bk, n)
+
+:class:`MixtureCompBatch` does the same for all cells in one call of the C ABI
+(``include/ocp_flash.h``) on device-resident structure-of-arrays state:
+``S``, ``phaseNum`` and ``xij`` are read as the previous step's values and
+overwritten in place, exactly as the Bulk arrays are. PyTorch only supplies
+device memory and streams; the flash itself is the CUDA library, which must
+be present (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import FORM_FAST, FORM_PLAIN, NPH, check, lib, make_fluid
+
+_TORCH_DT = {"f64": "float64", "u32": "int32", "i32": "int32", "u16": "int16", "u8": "uint8"}
+_NP_DT = {"f64": np.float64, "u32": np.uint32, "i32": np.int32, "u16": np.uint16, "u8": np.uint8}
+
+FORMS = {"plain": FORM_PLAIN, "fast": FORM_FAST}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+@dataclass
+class CellState:
+    """Device-resident cell arrays of one PVT region (SoA: ``[field, cell]``).
+
+    ``P``, ``T`` and ``Ni`` are the flash inputs. ``out`` holds every output
+    named as in ``Bulk``; ``out['S']``, ``out['phaseNum']`` and ``out['xij']``
+    double as the warm-start inputs of the next call. ``skip`` is the
+    SkipStaAnaly cache."""
+
+    ncell: int
+    nc: int
+    P: object
+    T: object
+    Ni: object
+    out: dict = field(default_factory=dict)
+    skip: dict = field(default_factory=dict)
+
+    def load(self, P, T, Ni):
+        """Copies new P [n], T [n] and Ni [n, numCom] (host arrays, cell-major)
+        into the device inputs."""
+        torch = _torch()
+        self.P.copy_(torch.as_tensor(np.ascontiguousarray(P, dtype=np.float64)))
+        self.T.copy_(torch.as_tensor(np.ascontiguousarray(T, dtype=np.float64)))
+        self.Ni.copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(Ni, dtype=np.float64).T)))
+
+    def to_host(self) -> dict:
+        """Outputs as numpy arrays in the cell-major layout of the oracle
+        (``[cell, ...]``)."""
+        ncom = self.nc + 1
+        res = {}
+        for k, t in self.out.items():
+            a = t.cpu().numpy()
+            if a.ndim == 2:
+                a = a.T.copy()
+            res[k] = a
+        for k in ("phaseNum", "phaseExist", "bRowSizedSdP", "pSderExist", "pVnumCom"):
+            res[k] = res[k].astype(np.int64)
+        res["iters"] = res["iters"].astype(np.int64)
+        res["status"] = res["status"].astype(np.uint16)
+        for k in ("xij", "rhox", "xix", "mux"):
+            res[k] = res[k].reshape(self.ncell, NPH, ncom)
+        res["skip"] = {k: (v.cpu().numpy().T.copy() if v.ndim == 2 else v.cpu().numpy())
+                       for k, v in self.skip.items()}
+        return res
+
+
+class MixtureCompBatch:
+    """One PVT region's flash on one GPU (``MixtureComp`` + ``SkipStaAnaly``)."""
+
+    def __init__(self, fluid, device: int = 0):
+        self.fluid = fluid
+        self.nc = fluid.nc
+        self.device = device
+        self._f = make_fluid(fluid)
+        h = C.c_void_p()
+        check(lib().ocpf_create(C.byref(self._f), int(device), C.byref(h)), "ocpf_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ocpf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ----------------------------------------------------------- device path
+    def new_state(self, ncell: int) -> CellState:
+        """Zero-initialised device state for ``ncell`` fresh cells (phaseNum 0:
+        the first flash runs the strict stability test)."""
+        torch = _torch()
+        dev = torch.device("cuda", self.device)
+        mk = lambda nf, dt: torch.zeros((nf, ncell) if nf > 1 else (ncell,),
+                                        dtype=getattr(torch, _TORCH_DT[dt]), device=dev)
+        st = CellState(ncell, self.nc, mk(1, "f64"), mk(1, "f64"), mk(self.nc + 1, "f64"))
+        for k, (nf, dt) in _lib.out_shapes(self.nc).items():
+            st.out[k] = mk(nf, dt)
+        for k, (nf, dt) in _lib.skip_shapes(self.nc).items():
+            st.skip[k] = mk(nf, dt)
+        return st
+
+    def _structs(self, st: CellState, optional=True, fresh=False):
+        o = st.out
+        if fresh:
+            # warm-start inputs of a fresh cell (lastNP = 0), kept apart from
+            # the outputs so that repeated calls do identical work
+            if st.__dict__.get("_fresh") is None:
+                torch = _torch()
+                dev = st.P.device
+                st.__dict__["_fresh"] = (
+                    torch.zeros((NPH, st.ncell), dtype=torch.float64, device=dev),
+                    torch.zeros(st.ncell, dtype=torch.int32, device=dev),
+                    torch.zeros((NPH * (st.nc + 1), st.ncell), dtype=torch.float64, device=dev))
+            S0, NP0, X0 = st.__dict__["_fresh"]
+            fin = _lib.FimIn(st.P.data_ptr(), st.T.data_ptr(), st.Ni.data_ptr(), S0.data_ptr(),
+                             NP0.data_ptr(), X0.data_ptr())
+        else:
+            fin = _lib.FimIn(st.P.data_ptr(), st.T.data_ptr(), st.Ni.data_ptr(), o["S"].data_ptr(),
+                             o["phaseNum"].data_ptr(), o["xij"].data_ptr())
+        sk = _lib.Skip(*[st.skip[k].data_ptr() for k in _lib.SKIP_FIELDS])
+        vals = []
+        for k in _lib.OUT_FIELDS:
+            vals.append(o[k].data_ptr() if (optional or k not in _lib.OPTIONAL_OUT) else None)
+        return fin, sk, _lib.FimOut(*vals)
+
+    def flash_fim(self, st: CellState, form: str = "plain", stream=None, diagnostics: bool = True,
+                  fresh: bool = False):
+        """Batched FlashFIM + PassFlashValue on device state (asynchronous on
+        ``stream``, default: torch's current stream). With ``fresh`` every
+        cell is flashed as a new bulk (lastNP = 0) instead of warm-starting
+        from the previous outputs."""
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        fin, sk, fo = self._structs(st, optional=diagnostics, fresh=fresh)
+        rc = lib().ocpf_flash_fim(self._h, st.ncell, C.byref(fin), C.byref(sk), C.byref(fo),
+                                  FORMS[form], C.c_void_p(stream.cuda_stream))
+        check(rc, "ocpf_flash_fim")
+
+    def last_kernel_ms(self) -> float:
+        ms = C.c_float(0)
+        check(lib().ocpf_last_kernel_ms(self._h, C.byref(ms)), "ocpf_last_kernel_ms")
+        return float(ms.value)
+
+    # ------------------------------------------------------------- host path
+    def new_host_state(self, ncell: int, pinned: bool = True) -> dict:
+        """Host SoA buffers for :meth:`flash_fim_host` (pinned if requested)."""
+        torch = _torch()
+
+        def mk(nf, dt):
+            shape = (nf, ncell) if nf > 1 else (ncell,)
+            t = torch.zeros(shape, dtype=getattr(torch, _TORCH_DT[dt]), pin_memory=pinned)
+            return t
+        hs = {"P": mk(1, "f64"), "T": mk(1, "f64"), "Ni": mk(self.nc + 1, "f64"), "out": {}, "skip": {}}
+        for k, (nf, dt) in _lib.out_shapes(self.nc).items():
+            hs["out"][k] = mk(nf, dt)
+        for k, (nf, dt) in _lib.skip_shapes(self.nc).items():
+            hs["skip"][k] = mk(nf, dt)
+        return hs
+
+    def flash_fim_host(self, hs: dict, form: str = "plain", diagnostics: bool = True):
+        """Same flash with every array in host memory (``new_host_state``);
+        the library streams the cells through its device staging buffers and
+        returns when the results are back on the host."""
+        o = hs["out"]
+        ncell = hs["P"].shape[0]
+        fin = _lib.FimIn(hs["P"].data_ptr(), hs["T"].data_ptr(), hs["Ni"].data_ptr(),
+                         o["S"].data_ptr(), o["phaseNum"].data_ptr(), o["xij"].data_ptr())
+        sk = _lib.Skip(*[hs["skip"][k].data_ptr() for k in _lib.SKIP_FIELDS])
+        fo = _lib.FimOut(*[(o[k].data_ptr() if (diagnostics or k not in _lib.OPTIONAL_OUT) else None)
+                           for k in _lib.OUT_FIELDS])
+        rc = lib().ocpf_flash_fim_host(self._h, ncell, C.byref(fin), C.byref(sk), C.byref(fo),
+                                       FORMS[form])
+        check(rc, "ocpf_flash_fim_host")

@@ -1,0 +1,49 @@
+"""Shared test set-up: the ``gpu`` marker, import paths and the golden-fixture
+loader."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+GOLDEN_CASES = ("spe5", "uniform_nc6", "warm_nc6", "uniform_nc3", "uniform_nc9", "uniform_nc12",
+                "near_nc6")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+def load_golden(name):
+    """Returns (fluid, inputs, reference outputs, fragile mask) of a fixture;
+    the reference's per-field self-noise is in out['noise']."""
+    from opencaeporo_b200.fluid import Controls, Fluid
+
+    d = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    c = d["controls"]
+    ctl = Controls(rr_maxit=int(c[0]), rr_tol=c[1], ssmsta_maxit=int(c[2]), ssmsta_tol=c[3],
+                   ssmsta_eyt=c[4], nrsta_maxit=int(c[5]), nrsta_tol=c[6], ssmsp_maxit=int(c[7]),
+                   ssmsp_tol=c[8], nrsp_maxit=int(c[9]), nrsp_tol=c[10], use_skip=bool(c[11]))
+    nc = len(d["fluid_Tc"])
+    fl = Fluid(nc=nc, Tc=d["fluid_Tc"], Pc=d["fluid_Pc"], Vc=d["fluid_Vc"], MW=d["fluid_MW"],
+               Acf=d["fluid_Acf"], BIC=d["fluid_BIC"], OmegaA=d["fluid_OmegaA"],
+               OmegaB=d["fluid_OmegaB"], Vshift=d["fluid_Vshift"], LBCcoef=d["fluid_LBCcoef"],
+               pvtw=d["fluid_pvtw"], std_rho_w=float(d["fluid_std_rho_w"]), controls=ctl,
+               name=str(d["fluid_name"]))
+    inp = {"P": d["in_P"], "T": d["in_T"], "Ni": d["in_Ni"], "S": d["in_S"],
+           "lastNP": d["in_lastNP"].astype(np.int32), "xij": d["in_xij"],
+           "skip": {k: d[f"skipin_{k}"] for k in ("flag", "minEig", "P", "T", "z")}}
+    out = {k[4:]: d[k] for k in d.files if k.startswith("out_")}
+    out["skip"] = {k: d[f"skipout_{k}"] for k in ("flag", "minEig", "P", "T", "z")}
+    out["noise"] = {k[6:]: d[k].astype(np.float64) for k in d.files if k.startswith("noise_")}
+    return fl, inp, out, d["fragile"]
+
+
+@pytest.fixture(scope="session")
+def golden():
+    return load_golden

@@ -1,0 +1,165 @@
+"""Generates the golden flash fixtures in tests/golden/ from the reference's
+own MixtureComp, compiled from the reference sources into
+oracle/_ref/libocpref.so (``make -C oracle ref``).
+
+Every fixture stores the fluid, the solver controls, the seeded inputs (with
+the warm-start state where the case has one) and the reference's outputs in
+the cell-major Bulk layout, plus a ``fragile`` mask: cells whose reference
+phase count changes when the inputs are perturbed by a few units in the last
+place (P, T and each Ni scaled by 1 +- 2^-50). Such cells sit on a knife
+edge of an iteration cap or a stability threshold; any implementation whose
+rounding differs from the reference's may legitimately land on either side.
+
+    python tests/golden/make_golden.py            # writes tests/golden/*.npz
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from opencaeporo_b200.fluid import Fluid, spe5_fluid, synthetic_fluid  # noqa: E402
+from opencaeporo_b200 import synth  # noqa: E402
+
+OUT_KEYS = ("phaseNum", "phaseExist", "S", "Nt", "vf", "vfP", "vfi", "nj", "rho", "xi", "mu",
+            "rhoP", "xiP", "muP", "xij", "rhox", "xix", "mux", "dSec_dPri", "bRowSizedSdP",
+            "pSderExist", "pVnumCom", "ePEC", "ftype", "NPhc", "iters")
+
+
+def fluid_arrays(fl: Fluid) -> dict:
+    c = fl.controls
+    d = {f"fluid_{k}": getattr(fl, k) for k in ("Tc", "Pc", "Vc", "MW", "Acf", "OmegaA", "OmegaB",
+                                                "Vshift", "BIC", "LBCcoef", "pvtw")}
+    d["fluid_std_rho_w"] = np.float64(fl.std_rho_w)
+    d["controls"] = np.array([c.rr_maxit, c.rr_tol, c.ssmsta_maxit, c.ssmsta_tol, c.ssmsta_eyt,
+                              c.nrsta_maxit, c.nrsta_tol, c.ssmsp_maxit, c.ssmsp_tol, c.nrsp_maxit,
+                              c.nrsp_tol, float(c.use_skip)])
+    d["fluid_name"] = np.array(fl.name)
+    return d
+
+
+def fragile_mask(fl, inp, base, nthreads=8):
+    """(fragile mask, per-field self-noise) of the reference on these cells."""
+    from oracle import compare as CMP
+    base_np = base["phaseNum"]
+    n = len(inp["P"])
+    frag = np.zeros(n, bool)
+    noise = {k: np.zeros(n) for k in CMP.FLOAT_KEYS}
+    eps = 2.0 ** -50
+    rng = np.random.default_rng(7)
+    for trial in range(6):
+        P, T, Ni = inp["P"].copy(), inp["T"].copy(), inp["Ni"].copy()
+        s = 1 if trial % 2 == 0 else -1
+        if trial < 2:
+            P *= 1 + s * eps
+        elif trial < 4:
+            T = T + s * eps * np.maximum(np.abs(T), 1.0)
+        else:
+            Ni = Ni * (1 + eps * rng.choice([-1.0, 1.0], size=Ni.shape))
+        skip = {k: v.copy() for k, v in inp["skip"].items()} if "skip" in inp else None
+        r = O.flash_fim("reference", fl, P, T, Ni, S=inp.get("S"), lastNP=inp.get("lastNP"),
+                        xij=inp.get("xij"), skip=skip, nthreads=nthreads)
+        frag |= r["phaseNum"] != base_np
+        e = CMP.per_cell_errors(r, base, fl.nc)
+        for k in CMP.FLOAT_KEYS:
+            noise[k] = np.fmax(noise[k], np.nan_to_num(e[k], nan=0.0))
+    return frag, noise
+
+
+def run_case(name, fl, inp, keep=None, note=""):
+    skip_in = {k: v.copy() for k, v in inp["skip"].items()} if "skip" in inp else O.new_skip(len(inp["P"]), fl.nc)
+    skip_run = {k: v.copy() for k, v in skip_in.items()}
+    r = O.flash_fim("reference", fl, inp["P"], inp["T"], inp["Ni"], S=inp.get("S"),
+                    lastNP=inp.get("lastNP"), xij=inp.get("xij"), skip=skip_run, nthreads=8)
+    inp2 = dict(inp)
+    inp2["skip"] = skip_in
+    frag, noise = fragile_mask(fl, inp2, r)
+    n = len(inp["P"])
+    sel = np.arange(n) if keep is None else np.asarray(keep)
+    d = fluid_arrays(fl)
+    d["note"] = np.array(note)
+    d["index"] = sel
+    d["in_P"], d["in_T"], d["in_Ni"] = inp["P"][sel], inp["T"][sel], inp["Ni"][sel]
+    d["in_S"] = (inp["S"] if "S" in inp else np.zeros((n, 3)))[sel]
+    d["in_lastNP"] = (inp["lastNP"] if "lastNP" in inp else np.zeros(n, np.int32))[sel]
+    d["in_xij"] = (inp["xij"] if "xij" in inp else np.zeros((n, 3, fl.nc + 1)))[sel]
+    for k, v in skip_in.items():
+        d[f"skipin_{k}"] = v[sel]
+    for k, v in skip_run.items():
+        d[f"skipout_{k}"] = v[sel]
+    for k in OUT_KEYS:
+        d[f"out_{k}"] = r[k][sel]
+    d["fragile"] = frag[sel]
+    for k, v in noise.items():
+        d[f"noise_{k}"] = v[sel].astype(np.float32)
+    path = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(path, **d)
+    two = np.mean(r["NPhc"][sel] == 2)
+    ft = np.bincount(r["ftype"][sel], minlength=3)
+    nz = max(float(np.max(v[sel])) for v in noise.values())
+    print(f"{name}: n={len(sel)} two-phase={two:.3f} ftype={ft.tolist()} fragile={frag[sel].sum()} "
+          f"max self-noise={nz:.1e} "
+          f"size={os.path.getsize(path) / 1e6:.2f} MB")
+    return r
+
+
+def main():
+    if not O.available("reference"):
+        raise SystemExit("oracle/_ref/libocpref.so missing: run `make -C oracle ref` first")
+
+    # 1) SPE5 fluid (examples/spe5/EGOIL.in) at 160 degF, the deck's initial composition
+    fl = spe5_fluid()
+    inp = {"P": np.array([1000.0, 2000.0, 3000.0, 4000.0]), "T": np.full(4, 160.0),
+           "Ni": np.tile([500.0, 30, 70, 200, 150, 50, 100], (4, 1))}
+    run_case("spe5", fl, inp, note="SPE5 fluid, fresh cells")
+
+    # 2) 6-component synthetic fluid, uniform states (P 5-40 MPa, T 340-400 K,
+    #    z ~ Dirichlet(1)); keep every two-phase cell of the first 1536 and
+    #    single-phase cells up to 512 in total
+    fl = synthetic_fluid(6, 1234)
+    inp = synth.uniform_states(fl, 4096, 1234)
+    r = O.flash_fim("reference", fl, inp["P"], inp["T"], inp["Ni"], nthreads=8)
+    two = np.nonzero(r["NPhc"][:1536] == 2)[0]
+    one = np.nonzero(r["NPhc"][:1536] == 1)[0][: max(512 - len(two), 0)]
+    keep = np.sort(np.concatenate([two, one]))[:512]
+    run_case("uniform_nc6", fl, inp, keep=keep, note="synthetic nc=6 seed 1234, uniform_states seed 1234")
+
+    # 3) warm start: a second FIM step from the first step's state, with P and
+    #    Ni perturbed (some cells inside the skip ranges -> ftype 1, two-phase
+    #    cells -> ftype 2, the rest -> ftype 0 with the relaxed stability test)
+    n = 512
+    inp = synth.uniform_states(fl, n, 99)
+    skip = O.new_skip(n, fl.nc)
+    a = O.flash_fim("reference", fl, inp["P"], inp["T"], inp["Ni"], skip=skip, nthreads=8)
+    rng = np.random.default_rng(5)
+    scale = np.where(rng.uniform(size=n) < 0.5, 1e-4, 3e-2)
+    inp2 = {"P": inp["P"] * (1 + scale * rng.uniform(-1, 1, n)), "T": inp["T"].copy(),
+            "Ni": inp["Ni"] * (1 + scale[:, None] * rng.uniform(-1, 1, inp["Ni"].shape)),
+            "S": a["S"], "lastNP": a["phaseNum"], "xij": np.nan_to_num(a["xij"], nan=0.0),
+            "skip": skip}
+    run_case("warm_nc6", fl, inp2, note="second FIM step: warm start, skip cache, perturbed P and Ni")
+
+    # 4) config-3-style fluids: P 2-60 MPa, T 300-450 K, z ~ Dirichlet(0.5)
+    for nc, seed in ((3, 31), (9, 91), (12, 121)):
+        fl = synthetic_fluid(nc, seed)
+        inp = synth.uniform_states(fl, 256, seed, p_mpa=(2.0, 60.0), t_k=(300.0, 450.0), alpha=0.5)
+        run_case(f"uniform_nc{nc}", fl, inp, note=f"synthetic nc={nc} seed {seed}, Dirichlet(0.5)")
+
+    # 5) near the phase envelope (P within 5 % of the saturation pressure)
+    fl = synthetic_fluid(6, 1234)
+
+    def pc(P, T, Ni):
+        return O.flash_fim("reference", fl, P, T, Ni, nthreads=8)["NPhc"]
+
+    inp = synth.near_envelope_states(fl, 256, 2024, pc)
+    run_case("near_nc6", fl, inp, note="synthetic nc=6, P = Psat * U(0.95, 1.05)")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,169 @@
+"""GPU parity tests: the CUDA flash through the C ABI against the reference's
+golden fixtures and against the plain-C oracle on larger seeded sets.
+
+Bar (oracle/compare.py): identical phase counts except on knife-edge cells
+(where the reference itself flips under 1-ulp input perturbations), and per
+output <= 1e-8 relative error, or <= 10x the reference's own 1-ulp
+sensitivity in the cells where the reference is ill-conditioned."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, load_golden
+from oracle import compare as CMP
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    return torch
+
+
+def _run_gpu(fl, inp, form="plain"):
+    from opencaeporo_b200.flash import MixtureCompBatch
+    torch = _torch()
+    m = MixtureCompBatch(fl)
+    n = len(inp["P"])
+    st = m.new_state(n)
+    st.load(inp["P"], inp["T"], inp["Ni"])
+    o = st.out
+    o["S"].copy_(torch.as_tensor(np.ascontiguousarray(inp["S"].T)))
+    o["phaseNum"].copy_(torch.as_tensor(inp["lastNP"].astype(np.int32)))
+    ncom = fl.nc + 1
+    o["xij"].copy_(torch.as_tensor(np.ascontiguousarray(inp["xij"].reshape(n, 3 * ncom).T)))
+    sk = inp["skip"]
+    st.skip["flag"].copy_(torch.as_tensor(sk["flag"].astype(np.int32)))
+    for k in ("minEig", "P", "T"):
+        st.skip[k].copy_(torch.as_tensor(np.asarray(sk[k], dtype=np.float64)))
+    st.skip["z"].copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(sk["z"]).T)))
+    m.flash_fim(st, form=form)
+    torch.cuda.synchronize()
+    res = st.to_host()
+    m.close()
+    return res
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_plain_matches_reference_goldens(case):
+    fl, inp, ref, fragile = load_golden(case)
+    got = _run_gpu(fl, inp)
+    chk = CMP.check(got, ref, fl.nc, noise=ref["noise"], fragile=fragile)
+    assert chk["ok"], f"{case}: {CMP.check_summary(chk)}"
+    res = CMP.compare(got, ref, fl.nc)
+    for k in ("phaseExist", "bRowSizedSdP", "pSderExist", "pVnumCom"):
+        assert res[k + "_mismatch"] == 0, f"{case}: {k}"
+    same = got["phaseNum"] == ref["phaseNum"]
+    assert np.array_equal(got["ftype"][same], ref["ftype"][same])
+    # iteration totals follow the reference's (noise-sensitive, so loosely)
+    a = got["iters"].sum(axis=0).astype(float)
+    b = ref["iters"].sum(axis=0).astype(float)
+    assert np.all(np.abs(a - b) <= 0.10 * np.maximum(b, 1) + 10), (a, b)
+
+
+def test_plain_skip_cache_matches_reference():
+    fl, inp, ref, fragile = load_golden("warm_nc6")
+    got = _run_gpu(fl, inp)
+    ok = (got["phaseNum"] == ref["phaseNum"]) & ~fragile
+    sg, sr = got["skip"], ref["skip"]
+    assert np.array_equal(sg["flag"][ok].astype(int), sr["flag"][ok].astype(int))
+    f = sr["flag"].astype(bool) & ok
+    np.testing.assert_allclose(sg["P"][f], sr["P"][f], rtol=0)
+    np.testing.assert_allclose(sg["T"][f], sr["T"][f], rtol=0)
+    np.testing.assert_allclose(sg["z"][f], sr["z"][f], rtol=1e-15)
+    np.testing.assert_allclose(sg["minEig"][f], sr["minEig"][f], rtol=2e-5, atol=2e-6)
+
+
+def test_host_path_equals_device_path():
+    """ocpf_flash_fim_host (host buffers, chunked copies on two streams) gives
+    bit-identical results to the device-buffer call."""
+    from opencaeporo_b200.flash import MixtureCompBatch
+    torch = _torch()
+    fl, inp, ref, _ = load_golden("warm_nc6")
+    dev = _run_gpu(fl, inp)
+    m = MixtureCompBatch(fl)
+    n = len(inp["P"])
+    hs = m.new_host_state(n)
+    hs["P"].copy_(torch.as_tensor(inp["P"]))
+    hs["T"].copy_(torch.as_tensor(inp["T"]))
+    hs["Ni"].copy_(torch.as_tensor(np.ascontiguousarray(inp["Ni"].T)))
+    o = hs["out"]
+    o["S"].copy_(torch.as_tensor(np.ascontiguousarray(inp["S"].T)))
+    o["phaseNum"].copy_(torch.as_tensor(inp["lastNP"].astype(np.int32)))
+    o["xij"].copy_(torch.as_tensor(np.ascontiguousarray(inp["xij"].reshape(n, -1).T)))
+    sk = inp["skip"]
+    hs["skip"]["flag"].copy_(torch.as_tensor(sk["flag"].astype(np.int32)))
+    for k in ("minEig", "P", "T"):
+        hs["skip"][k].copy_(torch.as_tensor(np.asarray(sk[k], dtype=np.float64)))
+    hs["skip"]["z"].copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(sk["z"]).T)))
+    m.flash_fim_host(hs)
+    for k in ("phaseNum", "S", "vfi", "xij", "mux", "dSec_dPri", "status", "iters"):
+        a = o[k].numpy()
+        a = a.T if a.ndim == 2 else a
+        b = dev[k].reshape(a.shape) if k in ("xij", "mux") else dev[k]
+        np.testing.assert_array_equal(np.nan_to_num(a.reshape(b.shape).astype(np.float64)),
+                                      np.nan_to_num(b.astype(np.float64)), err_msg=k)
+    m.close()
+
+
+def _port_noise(fl, inp, base, runs=4):
+    """The port's own 1-ulp sensitivity (per cell and field) and knife-edge mask."""
+    n = len(inp["P"])
+    noise = {k: np.zeros(n) for k in CMP.FLOAT_KEYS}
+    frag = np.zeros(n, bool)
+    eps = 2.0 ** -50
+    for t in range(runs):
+        s = 1 if t % 2 == 0 else -1
+        P = inp["P"] * (1 + s * eps) if t < 2 else inp["P"]
+        Ni = inp["Ni"] * (1 + s * eps) if t >= 2 else inp["Ni"]
+        r = O.flash_fim("port", fl, P, inp["T"], Ni, nthreads=0)
+        frag |= r["phaseNum"] != base["phaseNum"]
+        e = CMP.per_cell_errors(r, base, fl.nc)
+        for k in CMP.FLOAT_KEYS:
+            noise[k] = np.fmax(noise[k], np.nan_to_num(e[k], nan=0.0))
+    return noise, frag
+
+
+@pytest.mark.parametrize("nc,seed", [(6, 1234), (12, 7)])
+def test_plain_matches_port_4096(nc, seed):
+    """4096 seeded states (the 6-component workload distribution; and a
+    12-component fluid) against the plain-C oracle."""
+    from opencaeporo_b200.fluid import synthetic_fluid
+    from opencaeporo_b200 import synth
+    fl = synthetic_fluid(nc, seed)
+    inp = synth.uniform_states(fl, 4096, seed)
+    port = O.flash_fim("port", fl, inp["P"], inp["T"], inp["Ni"], nthreads=0)
+    noise, frag = _port_noise(fl, inp, port)
+    full = dict(inp, S=np.zeros((4096, 3)), lastNP=np.zeros(4096, np.int32),
+                xij=np.zeros((4096, 3, nc + 1)), skip=O.new_skip(4096, nc))
+    got = _run_gpu(fl, full)
+    chk = CMP.check(got, port, nc, noise=noise, fragile=frag)
+    assert chk["ok"], CMP.check_summary(chk)
+    assert len(chk["np_mismatch_all"]) <= 4
+
+
+def test_degenerate_inputs_do_not_hang_or_fault():
+    """NaN pressure, zero and negative moles, a single cell: the kernel
+    returns with every loop bounded and flags non-finite results."""
+    fl = load_golden("spe5")[0]
+    n = 4
+    inp = {"P": np.array([np.nan, 2000.0, 3000.0, 1e-3]), "T": np.full(n, 160.0),
+           "Ni": np.array([[500.0, 30, 70, 200, 150, 50, 100]] * n),
+           "S": np.zeros((n, 3)), "lastNP": np.zeros(n, np.int32),
+           "xij": np.zeros((n, 3, 7)), "skip": O.new_skip(n, 6)}
+    inp["Ni"][1, :6] = 0.0
+    inp["Ni"][2, 0] = -5.0
+    got = _run_gpu(fl, inp)
+    assert got["status"][0] & 0x40  # non-finite flagged
+    assert set(got["phaseNum"].tolist()) <= {2, 3}
+
+
+def test_zero_cells_is_a_noop():
+    from opencaeporo_b200.flash import MixtureCompBatch
+    _torch()
+    m = MixtureCompBatch(load_golden("spe5")[0])
+    st = m.new_state(0)
+    m.flash_fim(st)
+    m.close()

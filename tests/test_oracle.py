@@ -1,0 +1,100 @@
+"""CPU tests of the oracles: the plain-C restatement (oracle/flash_port.c) and,
+when it can be built here, the compiled reference (oracle/_ref) against the
+golden fixtures that the reference produced."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, load_golden
+from oracle import compare as CMP
+from oracle import oracle as O
+
+REF_SRC = "/root/reference/src/MixtureComp.cpp"
+
+
+def _run(kind, fl, inp):
+    skip = {k: np.array(v, copy=True) for k, v in inp["skip"].items()}
+    return O.flash_fim(kind, fl, inp["P"], inp["T"], inp["Ni"], S=inp["S"], lastNP=inp["lastNP"],
+                       xij=inp["xij"], skip=skip, nthreads=4)
+
+
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_port_matches_reference_goldens(case):
+    """The port reproduces the reference's outputs: identical phase counts
+    (except knife-edge cells) and <= 1e-8 relative error on every output, or
+    10x the reference's own 1-ulp sensitivity where that is larger."""
+    fl, inp, ref, fragile = load_golden(case)
+    got = _run("port", fl, inp)
+    chk = CMP.check(got, ref, fl.nc, noise=ref["noise"], fragile=fragile)
+    assert chk["ok"], f"{case}: {CMP.check_summary(chk)}"
+    res = CMP.compare(got, ref, fl.nc)
+    for k in ("phaseExist", "bRowSizedSdP", "pSderExist", "pVnumCom"):
+        assert res[k + "_mismatch"] == 0, f"{case}: {k}"
+
+
+@pytest.mark.parametrize("case", ["warm_nc6"])
+def test_port_skip_cache_and_flash_type(case):
+    """Warm-started step: the flash type (0 full / 1 skip / 2 two-phase warm)
+    and the SkipStaAnaly cache written back agree with the reference."""
+    fl, inp, ref, fragile = load_golden(case)
+    got = _run("port", fl, inp)
+    ok = ~fragile
+    assert np.array_equal(got["ftype"][ok], ref["ftype"][ok])
+    assert set(np.unique(ref["ftype"])) == {0, 1, 2}
+    sk_g, sk_r = got["skip"], ref["skip"]
+    assert np.array_equal(sk_g["flag"][ok], sk_r["flag"][ok])
+    np.testing.assert_allclose(sk_g["P"][ok], sk_r["P"][ok], rtol=0, atol=0)
+    np.testing.assert_allclose(sk_g["z"][ok], sk_r["z"][ok], rtol=1e-15)
+    # single-precision minimum eigenvalue (ssyevd in the reference)
+    f = sk_r["flag"].astype(bool) & ok
+    np.testing.assert_allclose(sk_g["minEig"][f], sk_r["minEig"][f], rtol=2e-5, atol=2e-6)
+
+
+def test_port_iteration_counts_close():
+    """Stability and split iteration counts of the port track the reference's
+    (they are noise-sensitive at tol^2 = 1e-24, so only the totals are held
+    to a few percent)."""
+    fl, inp, ref, fragile = load_golden("uniform_nc6")
+    got = _run("port", fl, inp)
+    a = got["iters"].sum(axis=0).astype(float)
+    b = ref["iters"].sum(axis=0).astype(float)
+    assert np.all(np.abs(a - b) <= 0.05 * np.maximum(b, 1) + 5), (a, b)
+
+
+def test_port_spe5_bitwise():
+    """On the SPE5 deck fluid the restatement is bit-for-bit the reference."""
+    fl, inp, ref, _ = load_golden("spe5")
+    got = _run("port", fl, inp)
+    assert np.array_equal(got["phaseNum"], ref["phaseNum"])
+    ex = ref["phaseExist"].astype(bool)
+    for k in ("S", "Nt", "vf"):
+        np.testing.assert_allclose(got[k], ref[k], rtol=1e-15, atol=0)
+    for k in ("rho", "xi", "mu"):
+        np.testing.assert_allclose(got[k][ex], ref[k][ex], rtol=1e-15, atol=0)
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SRC), reason="reference sources not present")
+def test_reference_reproduces_goldens():
+    """The compiled reference, rebuilt here, still produces the committed
+    fixtures (guards the fixtures and the harness)."""
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", os.path.join(os.path.dirname(O.__file__)), "ref"])
+    for case in GOLDEN_CASES:
+        fl, inp, ref, _ = load_golden(case)
+        got = _run("reference", fl, inp)
+        res = CMP.compare(got, ref, fl.nc)
+        assert len(res["np_mismatch"]) == 0, case
+        assert CMP.max_rel(res) == 0.0, f"{case}: {CMP.summary(res)}"
+
+
+def test_compare_flags_planted_error():
+    """The comparison catches a planted error in oracle output."""
+    fl, inp, ref, _ = load_golden("spe5")
+    bad = {k: (np.array(v, copy=True) if isinstance(v, np.ndarray) else v) for k, v in ref.items()}
+    bad["xi"][0, 0] *= 1 + 1e-6
+    res = CMP.compare(bad, ref, fl.nc)
+    assert res["xi"] > 5e-7
+    bad["phaseNum"][1] = 2
+    res = CMP.compare(bad, ref, fl.nc)
+    assert list(res["np_mismatch"]) == [1]
