@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--ncell", type=int, default=NCELL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload-cache", default=None,
+                    help="npz file: load the workload from it if present, else generate and save it")
     return ap.parse_args()
 
 
@@ -215,7 +217,14 @@ def our_arm(args):
     dev = local
     fl = bench_fluid()
     n = args.ncell
-    w = make_workload(fl, n, SEED + rank, dev)
+    cache = args.workload_cache
+    if cache and world == 1 and os.path.exists(cache):
+        d = np.load(cache)
+        w = {"P": d["P"][:n], "T": d["T"][:n], "Ni": d["Ni"][:n]}
+    else:
+        w = make_workload(fl, n, SEED + rank, dev)
+        if cache and world == 1:
+            np.savez(cache, P=w["P"], T=w["T"], Ni=w["Ni"])
     nc = fl.nc
 
     m = MixtureCompBatch(fl, dev)
@@ -344,6 +353,14 @@ def our_arm(args):
 
 
 def cpu_baseline(fl, w, gpu_res):
+    """The reference's own MixtureComp on the first cells of the workload
+    with every host thread, and, as a checker, the GPU outputs' error
+    against it on those cells. Cells are split by how well the reference
+    itself determines them: single-phase cells and two-phase cells whose
+    split converged (the reference's ePEC <= 1e-9) are well determined; the
+    rest stopped on an iteration cap or a small-step exit with a residual
+    above 1e-9, and the reference's own outputs move by up to O(1) under
+    1-ulp input perturbations there."""
     from oracle import compare as CMP
     from oracle import oracle as O
     kind = "reference" if O.available("reference") else "port"
@@ -356,16 +373,18 @@ def cpu_baseline(fl, w, gpu_res):
     worst = np.zeros(ns)
     for k in CMP.FLOAT_KEYS:
         worst = np.fmax(worst, np.nan_to_num(e[k], nan=0.0))
-    # cells whose reference compositions are normalised (the reference's split
-    # Newton can leave |n|/nu compositions that do not sum to 1)
-    sx = np.nansum(np.where(r["phaseExist"][:, :2, None].astype(bool), r["xij"][:, :2, :fl.nc], 0.0), axis=2)
-    clean = same & np.all((np.abs(sx - 1) < 1e-10) | (sx == 0), axis=1)
+    det = same & ((r["NPhc"] == 1) | (r["ePEC"] <= 1e-9))
+    ill = same & ~det
     return {"value": ns / r["seconds"], "unit": "states/s", "cores": cores, "kind": kind,
             "sample": f"first {ns} states of the 1M-cell workload, one flash each, {cores} threads",
-            "parity_on_sample": {"phase_count_mismatches": int(np.count_nonzero(~same)),
-                                 "max_rel_err_clean_cells": float(np.max(worst[clean], initial=0.0)),
-                                 "share_cells_le_1e-8": float(np.mean(worst[same] <= 1e-8)),
-                                 "clean_cells": int(clean.sum())}}
+            "parity_on_sample": {
+                "cells": ns, "phase_count_mismatches": int(np.count_nonzero(~same)),
+                "well_determined_cells": int(det.sum()),
+                "max_rel_err_well_determined": float(np.max(worst[det], initial=0.0)),
+                "share_well_determined_le_1e-8": float(np.mean(worst[det] <= 1e-8)) if det.any() else None,
+                "ill_determined_cells": int(ill.sum()),
+                "metric": "max over outputs of |gpu-ref|/max(|ref|, 1e-12 field scale); dSec_dPri "
+                          "entries against max(|ref|, 1e-4 column scale)"}}
 
 
 def main():
