@@ -56,10 +56,14 @@ extern "C" {
 #define OCPF_CELL_SINGULAR 0x20    /* a dense solve met a zero pivot */
 #define OCPF_CELL_NONFINITE 0x40   /* a non-finite value reached an output */
 #define OCPF_CELL_SPLIT_CAP 0x80   /* split restart loop bound reached */
+#define OCPF_CELL_GUARD 0x100      /* internal control-flow bound reached (a bug if ever set) */
 
-/* flash forms */
-#define OCPF_FORM_PLAIN 0 /* FP64 drop-in, the reference's algorithm */
-#define OCPF_FORM_FAST 1  /* FP32 successive substitution + FP64 polish */
+/* flash forms (all return the same outputs) */
+#define OCPF_FORM_PLAIN 0   /* one thread per cell, FP64: the reference's algorithm as written */
+#define OCPF_FORM_BATCHED 1 /* same FP64 arithmetic, persistent lane-refilling equilibrium
+                               kernel + separate finalize kernel */
+#define OCPF_FORM_MIXED 2   /* batched, successive substitution in FP32, FP64 Newton polish */
+#define OCPF_FORM_FAST 3    /* mixed + learned initialiser where a model is loaded */
 
 /* Fluid of one PVT region plus its solver controls: what MixtureComp's
  * constructor reads from ComponentParam (src/MixtureComp.cpp:28-165,
@@ -165,10 +169,19 @@ int ocpf_destroy(ocpf_ctx* ctx);
  * (src/MixtureComp.cpp:494-573, src/OCPFluidMethod.cpp:1108-1187), including
  * the skip-stability decision CalFtypeFIM (src/AcceleratePVT.cpp:96-120) and
  * CalSkipForNextStep (src/MixtureComp.cpp:5234-5254) on `skip`.
- * form: OCPF_FORM_PLAIN or OCPF_FORM_FAST. Asynchronous on `stream`;
- * allocates nothing. */
+ * form: one of OCPF_FORM_*. Asynchronous on `stream`. The plain form
+ * allocates nothing; the batched forms use the context's scratch (see
+ * ocpf_reserve). */
 int ocpf_flash_fim(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
                    ocpf_fim_out* out, int form, void* stream);
+
+/* Pre-allocates the context's device scratch (per-cell equilibrium buffer
+ * and work queue, about 0.3 KB per cell) for batches of up to ncell cells,
+ * so that later calls of the batched forms allocate nothing (e.g. before
+ * capturing them in a CUDA graph). Without it the scratch grows on the
+ * first call that needs more. No reference counterpart (the reference keeps
+ * its scratch inside each MixtureComp object). */
+int ocpf_reserve(ocpf_ctx* ctx, int64_t ncell);
 
 /* Same call with every array in HOST memory (pinned memory is faster). The
  * cells are streamed through device staging buffers owned by the context in

@@ -16,7 +16,7 @@ MAX_NC = 16
 NPH = 3
 
 OCPF_OK, OCPF_EINVAL, OCPF_ECUDA, OCPF_ENOMEM, OCPF_EUNSUPPORTED = 0, 1, 2, 3, 4
-FORM_PLAIN, FORM_FAST = 0, 1
+FORM_PLAIN, FORM_BATCHED, FORM_MIXED, FORM_FAST = 0, 1, 2, 3
 
 CELL_SSMSTA_CAP = 0x01
 CELL_NRSTA_FAIL = 0x02
@@ -26,11 +26,12 @@ CELL_COLLAPSED = 0x10
 CELL_SINGULAR = 0x20
 CELL_NONFINITE = 0x40
 CELL_SPLIT_CAP = 0x80
+CELL_GUARD = 0x100
 
 # Every function the header declares (checked by the CPU test suite).
 EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_flash_fim", "ocpf_flash_fim_host", "ocpf_last_kernel_ms",
-           "ocpf_measure_fma_peak")
+           "ocpf_measure_fma_peak", "ocpf_reserve")
 
 _vp = C.c_void_p
 
@@ -125,6 +126,8 @@ def lib():
     L.ocpf_last_kernel_ms.restype = C.c_int
     L.ocpf_measure_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.ocpf_measure_fma_peak.restype = C.c_int
+    L.ocpf_reserve.argtypes = [_vp, C.c_int64]
+    L.ocpf_reserve.restype = C.c_int
     _LIB = L
     return L
 

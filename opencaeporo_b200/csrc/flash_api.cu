@@ -7,7 +7,7 @@
 #include <cstring>
 #include <new>
 
-#include "flash_common.cuh"
+#include "flash_batched.cuh"
 
 namespace ocpf {
 
@@ -24,6 +24,32 @@ OCPF_DECL_PLAIN(12)
 using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const ocpf_fim_in&,
                                       const ocpf_skip&, const ocpf_fim_out&, unsigned, int,
                                       cudaStream_t);
+
+// Batched-form launchers (flash_batched_ncN.cu).
+#define OCPF_DECL_BATCHED(N)                                                                       \
+    cudaError_t launch_batched_nc##N(const FluidConst& F, int64_t count, int64_t stride,           \
+                                     const ocpf_fim_in& in, const ocpf_skip& sk,                    \
+                                     const ocpf_fim_out& out, const EqBuf& eb,                      \
+                                     unsigned long long* queue, int eq_blocks, cudaStream_t st);
+OCPF_DECL_BATCHED(3)
+OCPF_DECL_BATCHED(6)
+OCPF_DECL_BATCHED(9)
+OCPF_DECL_BATCHED(12)
+
+using BatchedLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const ocpf_fim_in&,
+                                        const ocpf_skip&, const ocpf_fim_out&, const EqBuf&,
+                                        unsigned long long*, int, cudaStream_t);
+
+static BatchedLauncher batched_kernel(int nc)
+{
+    switch (nc) {
+        case 3: return launch_batched_nc3;
+        case 6: return launch_batched_nc6;
+        case 9: return launch_batched_nc9;
+        case 12: return launch_batched_nc12;
+        default: return nullptr;
+    }
+}
 
 static PlainLauncher plain_kernel(int nc)
 {
@@ -106,6 +132,10 @@ struct ocpf_ctx {
     int64_t     stage_cap;
     void*       stage;
     cudaStream_t hs[2];
+    // batched-form scratch: per-cell equilibrium buffer and work queue
+    int64_t     eq_cap;
+    void*       eq;
+    unsigned long long* queue;
 };
 
 static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
@@ -147,6 +177,9 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->stage_cap = 0;
     c->stage     = nullptr;
     c->hs[0] = c->hs[1] = nullptr;
+    c->eq_cap    = 0;
+    c->eq        = nullptr;
+    c->queue     = nullptr;
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         cudaSetDevice(prev);
@@ -166,6 +199,8 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
     if (c->stage) cudaFree(c->stage);
+    if (c->eq) cudaFree(c->eq);
+    if (c->queue) cudaFree(c->queue);
     for (auto& s : c->hs)
         if (s) cudaStreamDestroy(s);
     cudaSetDevice(prev);
@@ -186,18 +221,71 @@ static bool fim_args_ok(const ocpf_ctx* c, const ocpf_fim_in* in, const ocpf_ski
     return true;
 }
 
-static int launch_plain(ocpf_ctx* c, int64_t count, int64_t stride, const ocpf_fim_in& in,
-                        const ocpf_skip& sk, const ocpf_fim_out& out, cudaStream_t st, bool timed)
+static int ensure_scratch(ocpf_ctx* c, int64_t ncell)
+{
+    if (!c->queue && cudaMalloc(&c->queue, 256) != cudaSuccess) return OCPF_ENOMEM;
+    if (c->eq_cap >= ncell) return OCPF_OK;
+    if (c->eq) {
+        cudaDeviceSynchronize();  // the old scratch may still be in use by queued work
+        cudaFree(c->eq);
+    }
+    c->eq     = nullptr;
+    c->eq_cap = 0;
+    if (cudaMalloc(&c->eq, eqbuf_bytes_per_cell(c->fc.nc) * (size_t)ncell + 1024) != cudaSuccess)
+        return OCPF_ENOMEM;
+    c->eq_cap = ncell;
+    return OCPF_OK;
+}
+
+// View of part `part` of the scratch, each part holding `cap` cells (the
+// host path runs two chunks concurrently, one per part and stream).
+static EqBuf eqbuf_view(const ocpf_ctx* c, int part, int64_t cap)
+{
+    EqBuf e;
+    char* base = (char*)c->eq + (size_t)part * (((eqbuf_bytes_per_cell(c->fc.nc) * (size_t)cap) + 255) / 256 * 256);
+    e.cap      = cap;
+    e.d        = (double*)base;
+    e.iters    = (int32_t*)(e.d + (size_t)eq_dbl(c->fc.nc) * cap);
+    e.meta     = (uint32_t*)(e.iters + 5 * (size_t)cap);
+    return e;
+}
+
+static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, const ocpf_fim_in& in,
+                       const ocpf_skip& sk, const ocpf_fim_out& out, cudaStream_t st, bool timed,
+                       int part = -1)
 {
     if (count == 0) return OCPF_OK;
-    PlainLauncher k = plain_kernel(c->fc.nc);
-    if (!k) return OCPF_EUNSUPPORTED;
-    const int     bs     = 128;
-    const int64_t blocks = (count + bs - 1) / bs;
-    if (blocks > 0x7fffffffLL) return OCPF_EINVAL;
-    if (timed) cudaEventRecord(c->ev0, st);
-    const cudaError_t e = k(c->fc, count, stride, in, sk, out, (unsigned)blocks, bs, st);
-    if (timed) cudaEventRecord(c->ev1, st);
+    cudaError_t e;
+    if (form == OCPF_FORM_PLAIN) {
+        PlainLauncher k = plain_kernel(c->fc.nc);
+        if (!k) return OCPF_EUNSUPPORTED;
+        const int     bs     = 128;
+        const int64_t blocks = (count + bs - 1) / bs;
+        if (blocks > 0x7fffffffLL) return OCPF_EINVAL;
+        if (timed) cudaEventRecord(c->ev0, st);
+        e = k(c->fc, count, stride, in, sk, out, (unsigned)blocks, bs, st);
+        if (timed) cudaEventRecord(c->ev1, st);
+    } else {
+        BatchedLauncher k = batched_kernel(c->fc.nc);
+        if (!k) return OCPF_EUNSUPPORTED;
+        EqBuf               eb;
+        unsigned long long* q;
+        if (part < 0) {
+            if (c->eq_cap < count) {
+                const int rc = ensure_scratch(c, count);
+                if (rc != OCPF_OK) return rc;
+            }
+            eb = eqbuf_view(c, 0, c->eq_cap);
+            q  = c->queue;
+        } else {
+            // host path: scratch already sized for two parts of `stride` cells
+            eb = eqbuf_view(c, part, stride);
+            q  = c->queue + part;
+        }
+        if (timed) cudaEventRecord(c->ev0, st);
+        e = k(c->fc, count, stride, in, sk, out, eb, q, 0, st);
+        if (timed) cudaEventRecord(c->ev1, st);
+    }
     return e == cudaSuccess ? OCPF_OK : OCPF_ECUDA;
 }
 
@@ -207,13 +295,13 @@ extern "C" int ocpf_flash_fim(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in* in,
     if (!c || ncell < 0) return OCPF_EINVAL;
     if (ncell == 0) return OCPF_OK;
     if (!fim_args_ok(c, in, sk, out)) return OCPF_EINVAL;
-    if (form != OCPF_FORM_PLAIN && form != OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != c->device) cudaSetDevice(c->device);
     ocpf_skip s{};
     if (sk) s = *sk;
-    const int rc = launch_plain(c, ncell, ncell, *in, s, *out, (cudaStream_t)stream, true);
+    const int rc = launch_form(c, form, ncell, ncell, *in, s, *out, (cudaStream_t)stream, true);
     c->timed     = (rc == OCPF_OK && ncell > 0);
     if (prev != c->device) cudaSetDevice(prev);
     return rc;
@@ -340,7 +428,7 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
     if (!c || ncell < 0) return OCPF_EINVAL;
     if (ncell == 0) return OCPF_OK;
     if (!fim_args_ok(c, in, sk, out)) return OCPF_EINVAL;
-    if (form != OCPF_FORM_PLAIN && form != OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != c->device) cudaSetDevice(c->device);
@@ -361,6 +449,15 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
     for (auto& s : c->hs)
         if (!s) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     const int64_t cap = c->stage_cap;
+    if (form != OCPF_FORM_PLAIN) {
+        // two parts of cap cells each, rounded to 256 bytes per part
+        const int64_t need = 2 * (cap + 256);
+        const int     r2   = ensure_scratch(c, need);
+        if (r2 != OCPF_OK) {
+            if (prev != c->device) cudaSetDevice(prev);
+            return r2;
+        }
+    }
     Views         V[2];
     for (int b = 0; b < 2; b++) V[b] = carve((char*)c->stage + b * stage_stride(per, cap), cap, L, sk, out);
     const bool use_sk = c->fc.use_skip != 0;
@@ -405,7 +502,7 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
             rc = OCPF_ECUDA;
             break;
         }
-        rc = launch_plain(c, cnt, cap, v.in, v.sk, v.out, st, false);
+        rc = launch_form(c, form, cnt, cap, v.in, v.sk, v.out, st, false, bidx);
         if (rc != OCPF_OK) break;
         D(out->phaseNum, v.out.phaseNum, 1, 4);
         D(out->phaseExist, v.out.phaseExist, NPH, 4);
@@ -444,6 +541,17 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
     }
     for (auto& s : c->hs)
         if (cudaStreamSynchronize(s) != cudaSuccess) rc = OCPF_ECUDA;
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+extern "C" int ocpf_reserve(ocpf_ctx* c, int64_t ncell)
+{
+    if (!c || ncell < 0) return OCPF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    const int rc = ensure_scratch(c, ncell);
     if (prev != c->device) cudaSetDevice(prev);
     return rc;
 }

@@ -125,10 +125,100 @@ struct CellFlash {
 
     // ---------------- stability ------------------------------------------
 
-    // StableNR with CalFugXSTA / AssembleJmatSTA / SYSSolve('U'),
-    // src/MixtureComp.cpp:1590-1741. The reference hands the row-major
-    // Jacobian to dsysv('U'), which reads its lower triangle as the upper
-    // triangle of a symmetric matrix; the same symmetric matrix is solved here.
+    // One Newton update of the stability test (the body of StableNR,
+    // src/MixtureComp.cpp:1600-1620): CalFugXSTA (:1638-1714) and
+    // AssembleJmatSTA (:1716-1741) at the trial composition Y (normalised,
+    // with mixture Asta, Bsta, Zsta), then SYSSolve('U'). The reference hands
+    // the row-major Jacobian to dsysv('U'), which reads its lower triangle as
+    // the upper triangle of a symmetric matrix; the same symmetric matrix is
+    // solved here. On return res holds the step and Y, Yt the new trial.
+    __device__ void sta_nr_update(double* Y, double& Yt_, double* res, double Asta, double Bsta,
+                                  double Zsta)
+    {
+        double M[NC][NC];
+        {
+            const double aj = Asta, bj = Bsta, zj = Zsta;
+            double       Ax[NC], Zx[NC];
+            double       t[NC];
+            {
+                double w[NC];
+#pragma unroll
+                for (int k = 0; k < NC; k++) w[k] = sA[k] * Y[k];
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    double s = 0;
+#pragma unroll
+                    for (int k = 0; k < NC; k++) s += omb(i, k) * w[k];
+                    t[i] = sA[i] * s;
+                }
+            }
+            const DzCoef dz(aj, bj, zj);
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                Ax[i] = 2 * t[i];
+                Zx[i] = dz(Ax[i], Bi[i]);
+            }
+            const double zmb  = zj - bj;
+            const double G    = (zj + D1 * bj) / (zj + D2 * bj);
+            const double lnG  = log(G);
+            const double ib   = 1.0 / bj;
+            const double zd2  = zj + D2 * bj;
+            const double gfac = D1MD2 / zd2 / zd2;
+            double       fx[NC][NC];
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                const double E = -aj / (D1MD2 * bj) * (Ax[i] / aj - Bi[i] * ib);
+#pragma unroll
+                for (int k = 0; k < NC; k++) {
+                    const double a_ik = omb(i, k) * sA[i] * sA[k];
+                    // 1/C * Cxk with C = Y_i P / (z - b)
+                    const double cterm = (zmb * dlt(i, k) - Y[i] * (Zx[k] - Bi[k])) / (Y[i] * zmb);
+                    const double Dxk   = Bi[i] * ib * (Zx[k] - Bi[k] * (zj - 1) * ib);
+                    double       Exk   = (2 * (aj * ib * Bi[k] * Bi[i] + bj * a_ik) - Ax[i] * Bi[k] -
+                                  Ax[k] * Bi[i]) *
+                                 (ib * ib);
+                    Exk /= -D1MD2;
+                    const double Gxk = gfac * (zj * Bi[k] - Zx[k] * bj);
+                    fx[i][k]         = cterm + Dxk + Exk * lnG + E / G * Gxk;
+                }
+            }
+            // AssembleJmatSTA: J[i][j] = (fx[i][j] - sum_k Y_k fx[i][k] + 1) / Yt;
+            // symmetric matrix from J's lower triangle.
+            const double iYt = 1.0 / Yt_;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                double s = 0;
+#pragma unroll
+                for (int k = 0; k < NC; k++) s += Y[k] * fx[i][k];
+#pragma unroll
+                for (int j = 0; j <= i; j++) {
+                    M[i][j] = (fx[i][j] - s + 1) * iYt;
+                    M[j][i] = M[i][j];
+                }
+            }
+        }
+        double B[NC][1];
+#pragma unroll
+        for (int i = 0; i < NC; i++) B[i][0] = res[i];
+        if (gauss_solve<NC, 1>(M, B)) {
+#pragma unroll
+            for (int i = 0; i < NC; i++) res[i] = B[i][0];
+        } else {
+            status |= ST_SINGULAR;  // dsysv leaves the right-hand side unchanged
+        }
+        double ys = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            Y[i] = Y[i] * Yt_ + res[i];
+            ys += Y[i];
+        }
+        Yt_            = ys;
+        const double r = 1 / Yt_;
+#pragma unroll
+        for (int i = 0; i < NC; i++) Y[i] *= r;
+    }
+
+    // StableNR, src/MixtureComp.cpp:1590-1636
     __device__ bool stable_nr(const double* fugId, double* Y, double* fugSta, double& Asta,
                               double& Bsta, double& Zsta)
     {
@@ -141,88 +231,7 @@ struct CellFlash {
         Se       = sqrt(Se);
         int iter = 0;
         while (Se > F.nrsta_tol) {
-            // CalFugXSTA, src/MixtureComp.cpp:1638-1714
-            double       M[NC][NC];
-            {
-                const double aj = Asta, bj = Bsta, zj = Zsta;
-                double       Ax[NC], Zx[NC];
-                double       t[NC];
-                {
-                    double w[NC];
-#pragma unroll
-                    for (int k = 0; k < NC; k++) w[k] = sA[k] * Y[k];
-#pragma unroll
-                    for (int i = 0; i < NC; i++) {
-                        double s = 0;
-#pragma unroll
-                        for (int k = 0; k < NC; k++) s += omb(i, k) * w[k];
-                        t[i] = sA[i] * s;
-                    }
-                }
-                const DzCoef dz(aj, bj, zj);
-#pragma unroll
-                for (int i = 0; i < NC; i++) {
-                    Ax[i] = 2 * t[i];
-                    Zx[i] = dz(Ax[i], Bi[i]);
-                }
-                const double zmb  = zj - bj;
-                const double G    = (zj + D1 * bj) / (zj + D2 * bj);
-                const double lnG  = log(G);
-                const double ib   = 1.0 / bj;
-                const double zd2  = zj + D2 * bj;
-                const double gfac = D1MD2 / zd2 / zd2;
-                double       fx[NC][NC];
-#pragma unroll
-                for (int i = 0; i < NC; i++) {
-                    const double E = -aj / (D1MD2 * bj) * (Ax[i] / aj - Bi[i] * ib);
-#pragma unroll
-                    for (int k = 0; k < NC; k++) {
-                        const double a_ik = omb(i, k) * sA[i] * sA[k];
-                        // 1/C * Cxk with C = Y_i P / (z - b)
-                        const double cterm = (zmb * dlt(i, k) - Y[i] * (Zx[k] - Bi[k])) / (Y[i] * zmb);
-                        const double Dxk   = Bi[i] * ib * (Zx[k] - Bi[k] * (zj - 1) * ib);
-                        double       Exk   = (2 * (aj * ib * Bi[k] * Bi[i] + bj * a_ik) - Ax[i] * Bi[k] -
-                                      Ax[k] * Bi[i]) *
-                                     (ib * ib);
-                        Exk /= -D1MD2;
-                        const double Gxk = gfac * (zj * Bi[k] - Zx[k] * bj);
-                        fx[i][k]         = cterm + Dxk + Exk * lnG + E / G * Gxk;
-                    }
-                }
-                // AssembleJmatSTA: J[i][j] = (fx[i][j] - sum_k Y_k fx[i][k] + 1) / Yt;
-                // symmetric matrix from J's lower triangle.
-                const double iYt = 1.0 / Yt;
-#pragma unroll
-                for (int i = 0; i < NC; i++) {
-                    double s = 0;
-#pragma unroll
-                    for (int k = 0; k < NC; k++) s += Y[k] * fx[i][k];
-#pragma unroll
-                    for (int j = 0; j <= i; j++) {
-                        M[i][j] = (fx[i][j] - s + 1) * iYt;
-                        M[j][i] = M[i][j];
-                    }
-                }
-            }
-            double B[NC][1];
-#pragma unroll
-            for (int i = 0; i < NC; i++) B[i][0] = res[i];
-            if (gauss_solve<NC, 1>(M, B)) {
-#pragma unroll
-                for (int i = 0; i < NC; i++) res[i] = B[i][0];
-            } else {
-                status |= ST_SINGULAR;  // dsysv leaves the right-hand side unchanged
-            }
-            double ys = 0;
-#pragma unroll
-            for (int i = 0; i < NC; i++) {
-                Y[i] = Y[i] * Yt + res[i];
-                ys += Y[i];
-            }
-            Yt             = ys;
-            const double r = 1 / Yt;
-#pragma unroll
-            for (int i = 0; i < NC; i++) Y[i] *= r;
+            sta_nr_update(Y, Yt, res, Asta, Bsta, Zsta);
             fug_phi(Y, nullptr, fugSta, Asta, Bsta, Zsta);
             Se = 0;
 #pragma unroll
@@ -556,8 +565,64 @@ struct CellFlash {
         }
     }
 
-    // SplitNR with CalResSP / AssembleJmatSP / CalStepNRsp (NP = 2),
-    // src/MixtureComp.cpp:2057-2166, 2265-2319
+    // One Newton update of the phase split (the body of SplitNR,
+    // src/MixtureComp.cpp:2075-2131): Jacobian (fugN of both phases,
+    // AssembleJmatSP :2265-2299), SYSSolve, step limit (CalStepNRsp
+    // :2301-2319), new phase moles, amounts and compositions. res holds
+    // ln(f1/f0) on entry; returns en, the step length of the convergence test
+    // (computed before the fugacity update it does not depend on).
+    __device__ double sp_nr_update(double* res)
+    {
+        double ln0[NC], ln1[NC];
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            ln0[i] = n[0][i];
+            ln1[i] = n[1][i];
+        }
+        double J[NC][NC];
+        double Zn_[NC];
+        fugn_phase(0, J, false, nullptr, Zn_);
+        fugn_phase(1, J, true, nullptr, Zn_);
+        double B[NC][1];
+#pragma unroll
+        for (int i = 0; i < NC; i++) B[i][0] = res[i];
+        if (gauss_solve<NC, 1>(J, B)) {
+#pragma unroll
+            for (int i = 0; i < NC; i++) res[i] = B[i][0];
+        } else {
+            status |= ST_SINGULAR;
+        }
+        double alpha = 1;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            const double tmp = n[0][i] + alpha * res[i];
+            if (tmp < 0) alpha *= 0.9 * fabs(n[0][i] / res[i]);
+        }
+        double s0 = 0, s1 = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            n[0][i] += alpha * res[i];
+            n[1][i] = zi[i] + -1 * n[0][i];
+            s0 += n[0][i];
+            s1 += n[1][i];
+        }
+        nu[0] = s0;
+        nu[1] = s1;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            x[0][i] = fabs(n[0][i] / nu[0]);
+            x[1][i] = fabs(n[1][i] / nu[1]);
+        }
+        double e0 = 0, e1 = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            e0 += sq(ln0[i] + -1 * n[0][i]);
+            e1 += sq(ln1[i] + -1 * n[1][i]);
+        }
+        return sqrt(e0) + sqrt(e1);
+    }
+
+    // SplitNR with CalResSP (NP = 2), src/MixtureComp.cpp:2057-2166
     __device__ void split_nr()
     {
         nrsp_conflag = false;
@@ -576,46 +641,7 @@ struct CellFlash {
         const double eNR0 = eNR;
         int          iter = 0;
         while (eNR > F.nrsp_tol) {
-            double ln0[NC], ln1[NC];
-#pragma unroll
-            for (int i = 0; i < NC; i++) {
-                ln0[i] = n[0][i];
-                ln1[i] = n[1][i];
-            }
-            double J[NC][NC];
-            double Zn_[NC];
-            fugn_phase(0, J, false, nullptr, Zn_);
-            fugn_phase(1, J, true, nullptr, Zn_);
-            double B[NC][1];
-#pragma unroll
-            for (int i = 0; i < NC; i++) B[i][0] = res[i];
-            if (gauss_solve<NC, 1>(J, B)) {
-#pragma unroll
-                for (int i = 0; i < NC; i++) res[i] = B[i][0];
-            } else {
-                status |= ST_SINGULAR;
-            }
-            double alpha = 1;
-#pragma unroll
-            for (int i = 0; i < NC; i++) {
-                const double tmp = n[0][i] + alpha * res[i];
-                if (tmp < 0) alpha *= 0.9 * fabs(n[0][i] / res[i]);
-            }
-            double s0 = 0, s1 = 0;
-#pragma unroll
-            for (int i = 0; i < NC; i++) {
-                n[0][i] += alpha * res[i];
-                n[1][i] = zi[i] + -1 * n[0][i];
-                s0 += n[0][i];
-                s1 += n[1][i];
-            }
-            nu[0] = s0;
-            nu[1] = s1;
-#pragma unroll
-            for (int i = 0; i < NC; i++) {
-                x[0][i] = fabs(n[0][i] / nu[0]);
-                x[1][i] = fabs(n[1][i] / nu[1]);
-            }
+            const double en = sp_nr_update(res);
             fug_phi_all();
             eNR = 0;
 #pragma unroll
@@ -626,13 +652,6 @@ struct CellFlash {
             eNR = sqrt(eNR);
             iter++;
             if (eNR > eNR0 || iter > F.nrsp_maxit) break;
-            double e0 = 0, e1 = 0;
-#pragma unroll
-            for (int i = 0; i < NC; i++) {
-                e0 += sq(ln0[i] + -1 * n[0][i]);
-                e1 += sq(ln1[i] + -1 * n[1][i]);
-            }
-            const double en = sqrt(e0) + sqrt(e1);
             if (en / (2 * NC) < 1e-8) {
                 nrsp_conflag = true;
                 break;

@@ -54,6 +54,7 @@ constexpr uint16_t ST_COLLAPSED  = OCPF_CELL_COLLAPSED;
 constexpr uint16_t ST_SINGULAR   = OCPF_CELL_SINGULAR;
 constexpr uint16_t ST_NONFINITE  = OCPF_CELL_NONFINITE;
 constexpr uint16_t ST_SPLIT_CAP  = OCPF_CELL_SPLIT_CAP;
+constexpr uint16_t ST_GUARD      = OCPF_CELL_GUARD;
 
 // Bound on PhaseSplit's restart loop (src/MixtureComp.cpp:1752-1757 has none).
 constexpr int SPLIT_RESTART_CAP = 1000;

@@ -114,15 +114,15 @@ struct FimCell : CellFlash<NC> {
         return (double)min_eig_sym<NC>(A);
     }
 
-    // Flash of cell n_ of arrays whose field stride (SoA) is `stride`.
-    __device__ void run(int64_t n_, int64_t stride, const ocpf_fim_in& in, const ocpf_skip& sk,
-                        const ocpf_fim_out& out)
+    // Reads cell n_'s inputs (SoA with field stride `stride`) and decides the
+    // flash type: FlashFIM up to CalFtypeFIM (src/MixtureComp.cpp:501-515).
+    // Everything is read before any output is written, so the caller may pass
+    // the same xij and S arrays in and out.
+    __device__ __forceinline__ void load_inputs(int64_t n_, int64_t stride, const ocpf_fim_in& in,
+                                                const ocpf_skip& sk)
     {
         const int64_t N = stride;
         auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
-
-        // ---- inputs (read everything before any output is written: the
-        // caller may pass the same xij and S arrays in and out)
         const double Pin = in.P[n_];
         const double Tin = in.T[n_];
 #pragma unroll
@@ -163,9 +163,28 @@ struct FimCell : CellFlash<NC> {
         for (int i = 0; i < NC; i++) zi[i] = Ni[i] / Nh;
 
         ftype = cal_ftype(Sin, skflag, skEig, skP, skT, skz);
+    }
 
-        // ---- CalFlash, src/MixtureComp.cpp:697-708
+    // The whole FlashFIM of one cell on this thread.
+    __device__ void run(int64_t n_, int64_t stride, const ocpf_fim_in& in, const ocpf_skip& sk,
+                        const ocpf_fim_out& out)
+    {
+        load_inputs(n_, stride, in, sk);
         this->phase_equilibrium();
+        finalize(n_, stride, sk, out);
+    }
+
+    // Everything after PhaseEquilibrium: CalFlash's property tail, the
+    // derivatives, the water block, dXsdXp, the partials, the skip cache and
+    // the copy-out of PassFlashValue. Needs load_inputs' state, cal_ai_bi's
+    // Ai/Bi and the equilibrium (NP, x, nu as phase fractions, Aj/Bj/Zj of
+    // each phase, n from the split, flagSkip, ePEC, counters, status).
+    __device__ void finalize(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out)
+    {
+        const int64_t N = stride;
+        auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
+
+        // ---- CalFlash, src/MixtureComp.cpp:697-708 (after PhaseEquilibrium)
 #pragma unroll
         for (int j = 0; j < 2; j++)
             if (j < NP) nu[j] *= Nh;

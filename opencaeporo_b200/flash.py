@@ -21,12 +21,12 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import FORM_FAST, FORM_PLAIN, NPH, check, lib, make_fluid
+from ._lib import FORM_BATCHED, FORM_FAST, FORM_MIXED, FORM_PLAIN, NPH, check, lib, make_fluid
 
 _TORCH_DT = {"f64": "float64", "u32": "int32", "i32": "int32", "u16": "int16", "u8": "uint8"}
 _NP_DT = {"f64": np.float64, "u32": np.uint32, "i32": np.int32, "u16": np.uint16, "u8": np.uint8}
 
-FORMS = {"plain": FORM_PLAIN, "fast": FORM_FAST}
+FORMS = {"plain": FORM_PLAIN, "batched": FORM_BATCHED, "mixed": FORM_MIXED, "fast": FORM_FAST}
 
 
 def _torch():
@@ -155,6 +155,10 @@ class MixtureCompBatch:
         rc = lib().ocpf_flash_fim(self._h, st.ncell, C.byref(fin), C.byref(sk), C.byref(fo),
                                   FORMS[form], C.c_void_p(stream.cuda_stream))
         check(rc, "ocpf_flash_fim")
+
+    def reserve(self, ncell: int):
+        """Pre-allocates the batched forms' device scratch for ncell cells."""
+        check(lib().ocpf_reserve(self._h, int(ncell)), "ocpf_reserve")
 
     def last_kernel_ms(self) -> float:
         ms = C.c_float(0)

@@ -46,10 +46,11 @@ def _run_gpu(fl, inp, form="plain"):
     return res
 
 
+@pytest.mark.parametrize("form", ["plain", "batched"])
 @pytest.mark.parametrize("case", GOLDEN_CASES)
-def test_plain_matches_reference_goldens(case):
+def test_matches_reference_goldens(case, form):
     fl, inp, ref, fragile = load_golden(case)
-    got = _run_gpu(fl, inp)
+    got = _run_gpu(fl, inp, form=form)
     chk = CMP.check(got, ref, fl.nc, noise=ref["noise"], fragile=fragile)
     assert chk["ok"], f"{case}: {CMP.check_summary(chk)}"
     res = CMP.compare(got, ref, fl.nc)
@@ -63,9 +64,10 @@ def test_plain_matches_reference_goldens(case):
     assert np.all(np.abs(a - b) <= 0.10 * np.maximum(b, 1) + 10), (a, b)
 
 
-def test_plain_skip_cache_matches_reference():
+@pytest.mark.parametrize("form", ["plain", "batched"])
+def test_skip_cache_matches_reference(form):
     fl, inp, ref, fragile = load_golden("warm_nc6")
-    got = _run_gpu(fl, inp)
+    got = _run_gpu(fl, inp, form=form)
     ok = (got["phaseNum"] == ref["phaseNum"]) & ~fragile
     sg, sr = got["skip"], ref["skip"]
     assert np.array_equal(sg["flag"][ok].astype(int), sr["flag"][ok].astype(int))
@@ -126,8 +128,9 @@ def _port_noise(fl, inp, base, runs=4):
     return noise, frag
 
 
+@pytest.mark.parametrize("form", ["plain", "batched"])
 @pytest.mark.parametrize("nc,seed", [(6, 1234), (12, 7)])
-def test_plain_matches_port_4096(nc, seed):
+def test_matches_port_4096(nc, seed, form):
     """4096 seeded states (the 6-component workload distribution; and a
     12-component fluid) against the plain-C oracle."""
     from opencaeporo_b200.fluid import synthetic_fluid
@@ -138,7 +141,7 @@ def test_plain_matches_port_4096(nc, seed):
     noise, frag = _port_noise(fl, inp, port)
     full = dict(inp, S=np.zeros((4096, 3)), lastNP=np.zeros(4096, np.int32),
                 xij=np.zeros((4096, 3, nc + 1)), skip=O.new_skip(4096, nc))
-    got = _run_gpu(fl, full)
+    got = _run_gpu(fl, full, form=form)
     chk = CMP.check(got, port, nc, noise=noise, fragile=frag)
     assert chk["ok"], CMP.check_summary(chk)
     assert len(chk["np_mismatch_all"]) <= 4
@@ -166,4 +169,44 @@ def test_zero_cells_is_a_noop():
     m = MixtureCompBatch(load_golden("spe5")[0])
     st = m.new_state(0)
     m.flash_fim(st)
+    m.close()
+
+
+@pytest.mark.parametrize("case", ["uniform_nc6", "warm_nc6", "uniform_nc12"])
+def test_batched_equals_plain(case):
+    """The batched form takes the reference's steps in the same order with
+    the same arithmetic as the plain form: outputs and iteration counters
+    agree bit for bit."""
+    fl, inp, ref, _ = load_golden(case)
+    a = _run_gpu(fl, inp, form="plain")
+    b = _run_gpu(fl, inp, form="batched")
+    for k in ("phaseNum", "iters", "status", "ftype"):
+        np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    for k in ("S", "xi", "mu", "xij", "vfi", "dSec_dPri", "mux", "ePEC"):
+        np.testing.assert_array_equal(np.nan_to_num(a[k]), np.nan_to_num(b[k]), err_msg=k)
+    sa, sb = a["skip"], b["skip"]
+    for k in sa:
+        np.testing.assert_array_equal(sa[k], sb[k], err_msg="skip " + k)
+
+
+def test_batched_host_path_and_reserve():
+    """Host-buffer path of the batched form (two streams, separate scratch
+    parts) equals its device path; ocpf_reserve pre-sizes the scratch."""
+    from opencaeporo_b200.flash import MixtureCompBatch
+    torch = _torch()
+    fl, inp, ref, _ = load_golden("uniform_nc6")
+    dev = _run_gpu(fl, inp, form="batched")
+    m = MixtureCompBatch(fl)
+    m.reserve(4096)
+    n = len(inp["P"])
+    hs = m.new_host_state(n)
+    hs["P"].copy_(torch.as_tensor(inp["P"]))
+    hs["T"].copy_(torch.as_tensor(inp["T"]))
+    hs["Ni"].copy_(torch.as_tensor(np.ascontiguousarray(inp["Ni"].T)))
+    m.flash_fim_host(hs, form="batched")
+    for k in ("phaseNum", "S", "dSec_dPri", "iters"):
+        a = hs["out"][k].numpy()
+        a = a.T if a.ndim == 2 else a
+        np.testing.assert_array_equal(np.nan_to_num(a.astype(np.float64)),
+                                      np.nan_to_num(dev[k].astype(np.float64)), err_msg=k)
     m.close()
