@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain", choices=["plain", "fast"])
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "mixed", "fast"])
     ap.add_argument("--ncell", type=int, default=NCELL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
