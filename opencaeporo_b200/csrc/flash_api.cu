@@ -7,7 +7,7 @@
 #include <cstring>
 #include <new>
 
-#include "flash_batched.cuh"
+#include "flash_phased.cuh"
 
 namespace ocpf {
 
@@ -25,28 +25,24 @@ using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const
                                       const ocpf_skip&, const ocpf_fim_out&, unsigned, int,
                                       cudaStream_t);
 
-// Batched-form launchers (flash_batched_ncN.cu).
-#define OCPF_DECL_BATCHED(N)                                                                       \
-    cudaError_t launch_batched_nc##N(const FluidConst& F, int64_t count, int64_t stride,           \
-                                     const ocpf_fim_in& in, const ocpf_skip& sk,                    \
-                                     const ocpf_fim_out& out, const EqBuf& eb,                      \
-                                     unsigned long long* queue, int eq_blocks, cudaStream_t st);
-OCPF_DECL_BATCHED(3)
-OCPF_DECL_BATCHED(6)
-OCPF_DECL_BATCHED(9)
-OCPF_DECL_BATCHED(12)
+// Batched-form launch sequences (flash_phased_ncN.cu).
+#define OCPF_DECL_PHASED(N)                                                           \
+    cudaError_t launch_phased_nc##N(const FluidConst& F, const PhasedArgs& a, cudaStream_t st); \
+    int         phased_state_doubles_nc##N();
+OCPF_DECL_PHASED(3)
+OCPF_DECL_PHASED(6)
+OCPF_DECL_PHASED(9)
+OCPF_DECL_PHASED(12)
 
-using BatchedLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const ocpf_fim_in&,
-                                        const ocpf_skip&, const ocpf_fim_out&, const EqBuf&,
-                                        unsigned long long*, int, cudaStream_t);
+using PhasedLauncher = cudaError_t (*)(const FluidConst&, const PhasedArgs&, cudaStream_t);
 
-static BatchedLauncher batched_kernel(int nc)
+static PhasedLauncher phased_kernel(int nc, int* ndbl)
 {
     switch (nc) {
-        case 3: return launch_batched_nc3;
-        case 6: return launch_batched_nc6;
-        case 9: return launch_batched_nc9;
-        case 12: return launch_batched_nc12;
+        case 3: *ndbl = phased_state_doubles_nc3(); return launch_phased_nc3;
+        case 6: *ndbl = phased_state_doubles_nc6(); return launch_phased_nc6;
+        case 9: *ndbl = phased_state_doubles_nc9(); return launch_phased_nc9;
+        case 12: *ndbl = phased_state_doubles_nc12(); return launch_phased_nc12;
         default: return nullptr;
     }
 }
@@ -132,10 +128,10 @@ struct ocpf_ctx {
     int64_t     stage_cap;
     void*       stage;
     cudaStream_t hs[2];
-    // batched-form scratch: per-cell equilibrium buffer and work queue
-    int64_t     eq_cap;
+    // batched-form scratch: per-cell phase state, cell lists and list
+    // counters, in parts of part_cap cells (the host path uses two parts)
+    int64_t     eq_cap;    // total cells the scratch holds
     void*       eq;
-    unsigned long long* queue;
 };
 
 static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
@@ -179,7 +175,6 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->hs[0] = c->hs[1] = nullptr;
     c->eq_cap    = 0;
     c->eq        = nullptr;
-    c->queue     = nullptr;
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         cudaSetDevice(prev);
@@ -200,7 +195,6 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     cudaEventDestroy(c->ev1);
     if (c->stage) cudaFree(c->stage);
     if (c->eq) cudaFree(c->eq);
-    if (c->queue) cudaFree(c->queue);
     for (auto& s : c->hs)
         if (s) cudaStreamDestroy(s);
     cudaSetDevice(prev);
@@ -221,33 +215,46 @@ static bool fim_args_ok(const ocpf_ctx* c, const ocpf_fim_in* in, const ocpf_ski
     return true;
 }
 
-static int ensure_scratch(ocpf_ctx* c, int64_t ncell)
+static size_t scratch_bytes_per_cell(int nc)
 {
-    if (!c->queue && cudaMalloc(&c->queue, 256) != cudaSuccess) return OCPF_ENOMEM;
-    if (c->eq_cap >= ncell) return OCPF_OK;
+    int nd = 0;
+    phased_kernel(nc, &nd);
+    return state_bytes_per_cell(nd) + 4 * (size_t)L_COUNT;
+}
+
+static size_t part_bytes(int nc, int64_t cap)
+{
+    return ((scratch_bytes_per_cell(nc) * (size_t)cap + 2 * 4 * L_COUNT + 255) / 256 + 1) * 256;
+}
+
+// Grows the scratch to hold `parts` parts of `cap` cells each.
+static int ensure_scratch(ocpf_ctx* c, int64_t cap, int parts = 1)
+{
+    const int64_t need = cap * parts;
+    if (c->eq_cap >= need && c->eq) return OCPF_OK;
     if (c->eq) {
         cudaDeviceSynchronize();  // the old scratch may still be in use by queued work
         cudaFree(c->eq);
     }
     c->eq     = nullptr;
     c->eq_cap = 0;
-    if (cudaMalloc(&c->eq, eqbuf_bytes_per_cell(c->fc.nc) * (size_t)ncell + 1024) != cudaSuccess)
-        return OCPF_ENOMEM;
-    c->eq_cap = ncell;
+    if (cudaMalloc(&c->eq, part_bytes(c->fc.nc, need) + 4096) != cudaSuccess) return OCPF_ENOMEM;
+    c->eq_cap = need;
     return OCPF_OK;
 }
 
-// View of part `part` of the scratch, each part holding `cap` cells (the
-// host path runs two chunks concurrently, one per part and stream).
-static EqBuf eqbuf_view(const ocpf_ctx* c, int part, int64_t cap)
+// Part `part` of the scratch laid out for `cap` cells.
+static void scratch_view(const ocpf_ctx* c, int part, int64_t cap, StateBuf& S, Lists& L)
 {
-    EqBuf e;
-    char* base = (char*)c->eq + (size_t)part * (((eqbuf_bytes_per_cell(c->fc.nc) * (size_t)cap) + 255) / 256 * 256);
-    e.cap      = cap;
-    e.d        = (double*)base;
-    e.iters    = (int32_t*)(e.d + (size_t)eq_dbl(c->fc.nc) * cap);
-    e.meta     = (uint32_t*)(e.iters + 5 * (size_t)cap);
-    return e;
+    int nd = 0;
+    phased_kernel(c->fc.nc, &nd);
+    char* base = (char*)c->eq + (size_t)part * part_bytes(c->fc.nc, cap);
+    S.cap      = cap;
+    S.d        = (double*)base;
+    S.i        = (int32_t*)(S.d + (size_t)nd * cap);
+    L.cap      = cap;
+    L.items    = S.i + (size_t)IF_COUNT * cap;
+    L.ctr      = (uint32_t*)(L.items + (size_t)L_COUNT * cap);
 }
 
 static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, const ocpf_fim_in& in,
@@ -266,24 +273,25 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         e = k(c->fc, count, stride, in, sk, out, (unsigned)blocks, bs, st);
         if (timed) cudaEventRecord(c->ev1, st);
     } else {
-        BatchedLauncher k = batched_kernel(c->fc.nc);
+        int            nd = 0;
+        PhasedLauncher k  = phased_kernel(c->fc.nc, &nd);
         if (!k) return OCPF_EUNSUPPORTED;
-        EqBuf               eb;
-        unsigned long long* q;
+        PhasedArgs args;
+        args.count  = count;
+        args.stride = stride;
+        args.in     = in;
+        args.sk     = sk;
+        args.out    = out;
         if (part < 0) {
-            if (c->eq_cap < count) {
-                const int rc = ensure_scratch(c, count);
-                if (rc != OCPF_OK) return rc;
-            }
-            eb = eqbuf_view(c, 0, c->eq_cap);
-            q  = c->queue;
+            const int rc = ensure_scratch(c, count);
+            if (rc != OCPF_OK) return rc;
+            scratch_view(c, 0, c->eq_cap, args.S, args.L);
         } else {
             // host path: scratch already sized for two parts of `stride` cells
-            eb = eqbuf_view(c, part, stride);
-            q  = c->queue + part;
+            scratch_view(c, part, stride, args.S, args.L);
         }
         if (timed) cudaEventRecord(c->ev0, st);
-        e = k(c->fc, count, stride, in, sk, out, eb, q, 0, st);
+        e = k(c->fc, args, st);
         if (timed) cudaEventRecord(c->ev1, st);
     }
     return e == cudaSuccess ? OCPF_OK : OCPF_ECUDA;
@@ -450,9 +458,7 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
         if (!s) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     const int64_t cap = c->stage_cap;
     if (form != OCPF_FORM_PLAIN) {
-        // two parts of cap cells each, rounded to 256 bytes per part
-        const int64_t need = 2 * (cap + 256);
-        const int     r2   = ensure_scratch(c, need);
+        const int r2 = ensure_scratch(c, cap, 2);
         if (r2 != OCPF_OK) {
             if (prev != c->device) cudaSetDevice(prev);
             return r2;

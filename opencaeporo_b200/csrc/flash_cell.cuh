@@ -9,6 +9,56 @@
 
 namespace ocpf {
 
+// Mixture parameters a = sum_i sum_k x_i x_k a_ik, b = sum_i B_i x_i and
+// the per-component sums t_i = sum_k a_ik x_k with
+// a_ik = (1 - k_ik) sqrt(A_i) sqrt(A_k) (CalAjBj, src/MixtureComp.cpp:939-969;
+// the inner sums of CalFugPhi, :1004-1008).
+template <int NC>
+__device__ __forceinline__ void mix_ab(const FluidConst& F, const double* sA, const double* Bi,
+                                       const double* xj, double* t, double& aj, double& bj)
+{
+    double w[NC];
+#pragma unroll
+    for (int k = 0; k < NC; k++) w[k] = sA[k] * xj[k];
+    aj = 0;
+    bj = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        double s = 0;
+#pragma unroll
+        for (int k = 0; k < NC; k++) s += F.omb[i * MAXNC + k] * w[k];
+        t[i] = sA[i] * s;
+        aj += xj[i] * t[i];
+        bj += Bi[i] * xj[i];
+    }
+}
+
+// CalFugPhi (src/MixtureComp.cpp:993-1101): the fugacity coefficients phi
+// and fugacities f = phi x P of composition xj (phiT may be null), with the
+// mixture's a, b and Z (SolEoS).
+template <int NC>
+__device__ __forceinline__ void fug_phi(const FluidConst& F, const double* sA, const double* Bi, double P,
+                                        const double* xj, double* phiT, double* fugT, double& aj,
+                                        double& bj, double& zj)
+{
+    double t[NC];
+    mix_ab<NC>(F, sA, Bi, xj, t, aj, bj);
+    zj               = sol_eos(aj, bj);
+    const double L1  = log(zj - bj);
+    const double L2  = log((zj + D1 * bj) / (zj + D2 * bj));
+    const double ib  = 1.0 / bj;
+    const double ia  = 1.0 / aj;
+    const double cf  = aj / D1MD2 * ib;
+    const double zm1 = zj - 1;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        const double bi = Bi[i] * ib;
+        const double ph = exp(bi * zm1 - L1 - cf * (2 * t[i] * ia - bi) * L2);
+        if (phiT) phiT[i] = ph;
+        if (fugT) fugT[i] = ph * xj[i] * P;
+    }
+}
+
 template <int NC>
 struct CellFlash {
     static constexpr int NUMCOM = NC + 1;
@@ -53,48 +103,19 @@ struct CellFlash {
         }
     }
 
-    // Mixture parameters and the per-component sums t_i = sum_k a_ik x_k with
-    // a_ik = (1 - k_ik) sqrt(A_i A_k) (CalAjBj, src/MixtureComp.cpp:939-969;
-    // the inner sums of CalFugPhi, :1004-1008).
+    // Mixture parameters and the per-component sums t_i = sum_k a_ik x_k
+    // (CalAjBj and the inner sums of CalFugPhi).
     __device__ __forceinline__ void mix_ab(const double* xj, double* t, double& aj, double& bj) const
     {
-        double w[NC];
-#pragma unroll
-        for (int k = 0; k < NC; k++) w[k] = sA[k] * xj[k];
-        aj = 0;
-        bj = 0;
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            double s = 0;
-#pragma unroll
-            for (int k = 0; k < NC; k++) s += omb(i, k) * w[k];
-            t[i] = sA[i] * s;
-            aj += xj[i] * t[i];
-            bj += Bi[i] * xj[i];
-        }
+        ocpf::mix_ab<NC>(F, sA, Bi, xj, t, aj, bj);
     }
 
-    // CalFugPhi (src/MixtureComp.cpp:993-1101): ln phi, phi and fugacity of
+    // CalFugPhi (src/MixtureComp.cpp:993-1101): phi and fugacity of
     // composition xj; phiT may be null. Returns the mixture a, b, Z.
     __device__ __forceinline__ void fug_phi(const double* xj, double* phiT, double* fugT, double& aj,
                                             double& bj, double& zj) const
     {
-        double t[NC];
-        mix_ab(xj, t, aj, bj);
-        zj               = sol_eos(aj, bj);
-        const double L1  = log(zj - bj);
-        const double L2  = log((zj + D1 * bj) / (zj + D2 * bj));
-        const double ib  = 1.0 / bj;
-        const double ia  = 1.0 / aj;
-        const double cf  = aj / D1MD2 * ib;
-        const double zm1 = zj - 1;
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            const double bi = Bi[i] * ib;
-            const double ph = exp(bi * zm1 - L1 - cf * (2 * t[i] * ia - bi) * L2);
-            if (phiT) phiT[i] = ph;
-            fugT[i] = ph * xj[i] * P;
-        }
+        ocpf::fug_phi<NC>(F, sA, Bi, P, xj, phiT, fugT, aj, bj, zj);
     }
 
     // CalFugPhiAll, src/MixtureComp.cpp:1103-1145

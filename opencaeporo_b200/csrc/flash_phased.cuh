@@ -1,0 +1,261 @@
+// flash_phased.cuh -- the batched form of the FIM flash, organised by phase.
+//
+// A one-thread-per-cell flash runs at ~20 % SIMT efficiency: the cells of a
+// warp need 2 to 400+ fugacity evaluations, take different branches, and the
+// fully inlined flash overflows the instruction cache. Here the flash of a
+// batch is a fixed sequence of small kernels; cells move between them through
+// device-side lists (appended with atomics, so each kernel sees only the
+// cells that need it):
+//
+//   init          every cell: inputs, flash type, fugacity of z; route
+//   S01 round k   relaxed stability trial k (StableSSM01), k = 0, 1:
+//                 prep -> persistent SSM -> end-of-trial logic
+//   strict round k (StableSSM trial k + StableNR), k = 0..3:
+//                 prep -> persistent SSM -> verdict -> Newton
+//   split round r (SplitSSM2 + SplitNR; r = 0 first try, r >= 1 restarts):
+//                 prep -> persistent SSM -> Newton start -> Newton
+//   slow path     cells still restarting after the last split round: the
+//                 rest of PhaseSplit on one thread each
+//   finalize      every cell: properties, derivatives, copy-out
+//
+// The persistent SSM kernels are where the time goes. Their loop body is one
+// fugacity evaluation plus an O(NC) update, the same for every lane; a lane
+// whose trial ends stores it and loads the next prepared item. Everything
+// irregular (trial set-up, Newton steps, routing) runs in the one-thread-per-
+// item kernels around them.
+//
+// Every cell takes exactly the reference's steps in the reference's order
+// (src/MixtureComp.cpp:1279-2166); only the schedule across cells changes.
+#pragma once
+
+#include "flash_fim.cuh"
+
+namespace ocpf {
+
+// ------------------------------------------------------------ cell state
+// Per-cell state kept across the phase kernels, structure of arrays with
+// field stride `cap`. Double fields first (ids below), then int fields.
+template <int NC>
+struct SF {  // double field ids
+    enum : int {
+        ePEC = 0, nu0, nu1, Aj0, Aj1, Bj0, Bj1, Zj0, Zj1,
+        x0, x1 = x0 + NC, n0 = x1 + NC, n1 = n0 + NC,          // finalize reads up to here
+        Yt = n1 + NC, SeSSM, rtSSMSTA, rtNRSTA, rtSSMSP, rtNRSP, SeSP, Stol, eNR, eNR0, Asta, Bsta, Zsta,
+        phiZ, Y = phiZ + NC, phiS = Y + NC, Ks = phiS + NC, phi0 = Ks + NC, phi1 = phi0 + NC,
+        di = phi1 + NC, sA = di + NC, Bi = sA + NC,
+        COUNT = Bi + NC
+    };
+};
+// int fields
+enum : int { IF_META = 0, IF_STATUS, IF_IT0, IF_IT1, IF_IT2, IF_IT3, IF_IT4, IF_MAXIT, IF_GUARD, IF_COUNT };
+
+// meta bits
+constexpr uint32_t M_NP_MASK   = 0xF;     // hydrocarbon phase count
+constexpr int      M_FTYPE_SH  = 4;       // 2 bits
+constexpr uint32_t M_FLAGSKIP  = 1u << 8;
+constexpr uint32_t M_C_SSMSTA  = 1u << 9;   // convergence flags of the four solvers
+constexpr uint32_t M_C_NRSTA   = 1u << 10;
+constexpr uint32_t M_C_SSMSP   = 1u << 11;
+constexpr uint32_t M_C_NRSP    = 1u << 12;
+constexpr uint32_t M_RESTART   = 1u << 13;  // next split SSM is a restart
+constexpr uint32_t M_STAB_RES  = 1u << 14;  // last stability verdict: stable
+constexpr uint32_t M_NRFLAG    = 1u << 15;  // flag of the last StableNR
+constexpr uint32_t M_SPPHASE   = 1u << 16;  // split loop: after a restart
+
+template <int NC>
+constexpr int state_doubles() { return SF<NC>::COUNT; }
+inline size_t state_bytes_per_cell(int nc_doubles) { return 8 * (size_t)nc_doubles + 4 * (size_t)IF_COUNT; }
+
+struct StateBuf {
+    double*  d;  // [COUNT][cap]
+    int32_t* i;  // [IF_COUNT][cap]
+    int64_t  cap;
+    __device__ __forceinline__ double& D(int f, int64_t c) const { return d[(int64_t)f * cap + c]; }
+    __device__ __forceinline__ int32_t& I(int f, int64_t c) const { return i[(int64_t)f * cap + c]; }
+};
+
+// ------------------------------------------------------------------ lists
+enum ListId : int {
+    L_S01_0 = 0, L_S01_1,
+    L_STA_0, L_STA_1, L_STA_2, L_STA_3,
+    L_NRSTA_0, L_NRSTA_1, L_NRSTA_2, L_NRSTA_3,
+    L_SP_0, L_SP_1, L_SP_2, L_SP_3,
+    L_SPNR_0, L_SPNR_1, L_SPNR_2, L_SPNR_3,
+    L_SLOW,
+    L_COUNT
+};
+constexpr int SPLIT_ROUNDS = 4;  // first try + 3 restarts on the fast path
+
+struct Lists {
+    int32_t*  items;  // [L_COUNT][cap]
+    uint32_t* ctr;    // [L_COUNT][2]: length, consumer head
+    int64_t   cap;
+    __device__ __forceinline__ void push(int id, int32_t cell) const
+    {
+        const uint32_t at         = atomicAdd(&ctr[2 * id], 1u);
+        items[(int64_t)id * cap + at] = cell;
+    }
+    __device__ __forceinline__ uint32_t len(int id) const { return *(volatile uint32_t*)&ctr[2 * id]; }
+    __device__ __forceinline__ int32_t item(int id, uint32_t k) const { return items[(int64_t)id * cap + k]; }
+    // next item for a persistent consumer, or -1
+    __device__ __forceinline__ int32_t take(int id, uint32_t n) const
+    {
+        const uint32_t k = atomicAdd(&ctr[2 * id + 1], 1u);
+        return k < n ? item(id, k) : -1;
+    }
+};
+
+struct PhasedArgs {
+    int64_t      count, stride;
+    ocpf_fim_in  in;
+    ocpf_skip    sk;
+    ocpf_fim_out out;
+    StateBuf     S;
+    Lists        L;
+};
+
+// Reads P, T and z of cell c into a CellFlash (InitPTN, bit for bit as
+// load_inputs forms them) and computes Ai, Bi.
+template <int NC>
+__device__ __forceinline__ void load_ptz(CellFlash<NC>& f, const PhasedArgs& a, int64_t c)
+{
+    const int64_t N = a.stride;
+    f.P             = a.in.P[c];
+    f.T             = a.in.T[c] + CONV5;
+    double Ni[NC];
+#pragma unroll
+    for (int i = 0; i < NC; i++) Ni[i] = a.in.Ni[(int64_t)i * N + c];
+    double Nh = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) Nh += fabs(Ni[i]);
+    f.Nh = Nh;
+#pragma unroll
+    for (int i = 0; i < NC; i++) f.zi[i] = Ni[i] / Nh;
+    f.cal_ai_bi();
+}
+
+// Bookkeeping of one cell that the thread-per-item kernels load and store.
+template <int NC>
+__device__ __forceinline__ void load_book(CellFlash<NC>& f, const StateBuf& S, int64_t c, uint32_t& meta)
+{
+    using F_ = SF<NC>;
+    meta             = (uint32_t)S.I(IF_META, c);
+    f.NP             = (int)(meta & M_NP_MASK);
+    f.ftype          = (int)((meta >> M_FTYPE_SH) & 3);
+    f.flagSkip       = (meta & M_FLAGSKIP) != 0;
+    f.ssmsta_conflag = (meta & M_C_SSMSTA) != 0;
+    f.nrsta_conflag  = (meta & M_C_NRSTA) != 0;
+    f.ssmsp_conflag  = (meta & M_C_SSMSP) != 0;
+    f.nrsp_conflag   = (meta & M_C_NRSP) != 0;
+    f.status         = (uint16_t)S.I(IF_STATUS, c);
+    f.it_ssmsta      = S.I(IF_IT0, c);
+    f.it_nrsta       = S.I(IF_IT1, c);
+    f.it_ssmsp       = S.I(IF_IT2, c);
+    f.it_nrsp        = S.I(IF_IT3, c);
+    f.it_rr          = S.I(IF_IT4, c);
+    f.ssmsta_realTol = S.D(F_::rtSSMSTA, c);
+    f.nrsta_realTol  = S.D(F_::rtNRSTA, c);
+    f.ssmsp_realTol  = S.D(F_::rtSSMSP, c);
+    f.nrsp_realTol   = S.D(F_::rtNRSP, c);
+    f.Yt             = S.D(F_::Yt, c);
+}
+
+template <int NC>
+__device__ __forceinline__ void store_book(const CellFlash<NC>& f, const StateBuf& S, int64_t c, uint32_t meta)
+{
+    using F_ = SF<NC>;
+    meta &= ~(M_NP_MASK | M_FLAGSKIP | M_C_SSMSTA | M_C_NRSTA | M_C_SSMSP | M_C_NRSP | (3u << M_FTYPE_SH));
+    meta |= (uint32_t)f.NP | ((uint32_t)f.ftype << M_FTYPE_SH) | (f.flagSkip ? M_FLAGSKIP : 0u) |
+            (f.ssmsta_conflag ? M_C_SSMSTA : 0u) | (f.nrsta_conflag ? M_C_NRSTA : 0u) |
+            (f.ssmsp_conflag ? M_C_SSMSP : 0u) | (f.nrsp_conflag ? M_C_NRSP : 0u);
+    S.I(IF_META, c)         = (int32_t)meta;
+    S.I(IF_STATUS, c)       = f.status;
+    S.I(IF_IT0, c)          = f.it_ssmsta;
+    S.I(IF_IT1, c)          = f.it_nrsta;
+    S.I(IF_IT2, c)          = f.it_ssmsp;
+    S.I(IF_IT3, c)          = f.it_nrsp;
+    S.I(IF_IT4, c)          = f.it_rr;
+    S.D(F_::rtSSMSTA, c)    = f.ssmsta_realTol;
+    S.D(F_::rtNRSTA, c)     = f.nrsta_realTol;
+    S.D(F_::rtSSMSP, c)     = f.ssmsp_realTol;
+    S.D(F_::rtNRSP, c)      = f.nrsp_realTol;
+    S.D(F_::Yt, c)          = f.Yt;
+}
+
+// Equilibrium of a single-phase cell for the finalize kernel: z with the
+// mixture a, b, Z of phase 0 (already stored).
+template <int NC>
+__device__ __forceinline__ void store_single_phase(const CellFlash<NC>& f, const StateBuf& S, int64_t c)
+{
+    using F_         = SF<NC>;
+    S.D(F_::nu0, c)  = 1.0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) S.D(F_::x0 + i, c) = f.zi[i];
+}
+
+template <int NC>
+__device__ __forceinline__ void store_split(const CellFlash<NC>& f, const StateBuf& S, int64_t c)
+{
+    using F_        = SF<NC>;
+    S.D(F_::nu0, c) = f.nu[0];
+    S.D(F_::nu1, c) = f.nu[1];
+    S.D(F_::Aj0, c) = f.Aj[0];
+    S.D(F_::Aj1, c) = f.Aj[1];
+    S.D(F_::Bj0, c) = f.Bj[0];
+    S.D(F_::Bj1, c) = f.Bj[1];
+    S.D(F_::Zj0, c) = f.Zj[0];
+    S.D(F_::Zj1, c) = f.Zj[1];
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        S.D(F_::x0 + i, c)   = f.x[0][i];
+        S.D(F_::x1 + i, c)   = f.x[1][i];
+        S.D(F_::n0 + i, c)   = f.n[0][i];
+        S.D(F_::n1 + i, c)   = f.n[1][i];
+        S.D(F_::phi0 + i, c) = f.phi[0][i];
+        S.D(F_::phi1 + i, c) = f.phi[1][i];
+    }
+}
+
+template <int NC>
+__device__ __forceinline__ void load_split(CellFlash<NC>& f, const StateBuf& S, int64_t c)
+{
+    using F_ = SF<NC>;
+    f.nu[0]  = S.D(F_::nu0, c);
+    f.nu[1]  = S.D(F_::nu1, c);
+    f.Aj[0]  = S.D(F_::Aj0, c);
+    f.Aj[1]  = S.D(F_::Aj1, c);
+    f.Bj[0]  = S.D(F_::Bj0, c);
+    f.Bj[1]  = S.D(F_::Bj1, c);
+    f.Zj[0]  = S.D(F_::Zj0, c);
+    f.Zj[1]  = S.D(F_::Zj1, c);
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        f.x[0][i]   = S.D(F_::x0 + i, c);
+        f.x[1][i]   = S.D(F_::x1 + i, c);
+        f.n[0][i]   = S.D(F_::n0 + i, c);
+        f.n[1][i]   = S.D(F_::n1 + i, c);
+        f.phi[0][i] = S.D(F_::phi0 + i, c);
+        f.phi[1][i] = S.D(F_::phi1 + i, c);
+        f.fug[0][i] = f.phi[0][i] * f.x[0][i] * f.P;
+        f.fug[1][i] = f.phi[1][i] * f.x[1][i] * f.P;
+        f.Ks[i]     = S.D(F_::Ks + i, c);
+    }
+}
+
+// PhaseEquilibrium's ePEC and the final flagSkip of a finished cell
+// (src/MixtureComp.cpp:1297-1316, 1339-1345).
+template <int NC>
+__device__ __forceinline__ void finish_epec(CellFlash<NC>& f)
+{
+    if (f.ftype == 1) {
+        f.ePEC = 0.0;
+        return;
+    }
+    if (f.ftype == 0 && f.NP > 1) f.flagSkip = false;
+    if (f.ftype == 0 && f.NP == 1)
+        f.ePEC = f.nrsta_conflag ? f.nrsta_realTol : (f.ssmsta_conflag ? f.ssmsta_realTol : 1e8);
+    else
+        f.ePEC = f.nrsp_conflag ? f.nrsp_realTol : (f.ssmsp_conflag ? f.ssmsp_realTol : 1e8);
+}
+
+}  // namespace ocpf

@@ -1,0 +1,792 @@
+// flash_phased_kernels.cuh -- bodies of the phase kernels of the batched
+// FIM flash (see flash_phased.cuh for the schedule).
+#pragma once
+
+#include "flash_phased.cuh"
+
+namespace ocpf {
+
+// Thread-per-item kernels walk their list with a grid-stride loop: the grid
+// is fixed at launch (the list length is only known on the device).
+#define OCPF_FOR_ITEMS(A, LIST, c)                                                              \
+    for (uint32_t _k = blockIdx.x * blockDim.x + threadIdx.x, _n = (A).L.len(LIST); _k < _n; \
+         _k += gridDim.x * blockDim.x)                                                          \
+        if (const int64_t c = (A).L.item(LIST, _k); true)
+
+// ------------------------------------------------------------------ init
+// FlashFIM up to PhaseEquilibrium's first fork (src/MixtureComp.cpp:494-515,
+// 1279-1293, 1319-1337): inputs, flash type, Ai/Bi, and the mixture (and for
+// ftype 0 the fugacity coefficients) of z. Routes the cell to the relaxed or
+// strict stability test, to the split, or finishes it (ftype 1).
+template <int NC>
+__device__ void init_body(const FluidConst& F, const PhasedArgs& a)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        FimCell<NC> f(F);
+        f.load_inputs(c, a.stride, a.in, a.sk);
+        f.cal_ai_bi();
+        uint32_t meta = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            S.D(F_::sA + i, c) = f.sA[i];
+            S.D(F_::Bi + i, c) = f.Bi[i];
+        }
+        S.I(IF_GUARD, c) = 0;
+        if (f.ftype == 0 || f.ftype == 1) {
+            f.flagSkip = true;
+            f.NP       = 1;
+            double phiz[NC];
+            f.fug_phi(f.zi, phiz, nullptr, f.Aj[0], f.Bj[0], f.Zj[0]);
+            S.D(F_::Aj0, c) = f.Aj[0];
+            S.D(F_::Bj0, c) = f.Bj[0];
+            S.D(F_::Zj0, c) = f.Zj[0];
+            if (f.ftype == 1) {
+                finish_epec(f);
+                S.D(F_::ePEC, c) = f.ePEC;
+                store_single_phase(f, S, c);
+            } else {
+#pragma unroll
+                for (int i = 0; i < NC; i++) S.D(F_::phiZ + i, c) = phiz[i];
+                a.L.push(f.lNP == 0 ? L_STA_0 : L_S01_0, (int32_t)c);
+            }
+        } else {
+            f.flagSkip = false;
+            f.NP       = 2;
+            f.Yt       = 1.01;
+            a.L.push(L_SP_0, (int32_t)c);
+        }
+        store_book(f, S, c, meta);
+    }
+}
+
+// ------------------------------------------------------ strict stability
+// Trial k set-up of StableSSM (src/MixtureComp.cpp:1514-1524): Y = z / Kw_k,
+// normalised, and d_i = phi_z,i z_i.
+template <int NC>
+__device__ void sta_prep_body(const FluidConst& F, const PhasedArgs& a, int k)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_STA_0 + k, c)
+    {
+        CellFlash<NC> f(F);
+        load_ptz(f, a, c);
+        f.cal_kwilson();
+        double Yt = 0, Y[NC];
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            Y[i] = f.zi[i] / f.kw(k, i);
+            Yt += Y[i];
+        }
+        const double r = 1 / Yt;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            S.D(F_::Y + i, c)  = Y[i] * r;
+            S.D(F_::di + i, c) = S.D(F_::phiZ + i, c) * f.zi[i];
+        }
+        S.D(F_::Yt, c) = Yt;
+    }
+}
+
+// The successive substitution of one StableSSM trial (src/MixtureComp.cpp:
+// 1525-1564) on a persistent grid. Per lane: Y (next composition), d, the
+// mixture terms, Yt and the iteration count. Each loop turn is one fugacity
+// evaluation and an O(NC) update for every active lane.
+template <int NC>
+__device__ void sta_ssm_body(const FluidConst& F, const PhasedArgs& a, int k)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S    = a.S;
+    const int       list = L_STA_0 + k;
+    const uint32_t  n    = a.L.len(list);
+    double          Y[NC], di[NC], sA[NC], Bi[NC];
+    double          P = 0, Yt = 0;
+    int             iter = 0;
+    bool            first = true;
+    int64_t         c     = a.L.take(list, n);
+    auto load = [&]() {
+        P  = a.in.P[c];
+        Yt = S.D(F_::Yt, c);
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            Y[i]  = S.D(F_::Y + i, c);
+            di[i] = S.D(F_::di + i, c);
+            sA[i] = S.D(F_::sA + i, c);
+            Bi[i] = S.D(F_::Bi + i, c);
+        }
+        iter  = 0;
+        first = true;
+    };
+    if (c >= 0) load();
+    while (__any_sync(0xffffffffu, c >= 0)) {
+        if (c >= 0) {
+            double phi[NC], aj, bj, zj;
+            fug_phi<NC>(F, sA, Bi, P, Y, phi, nullptr, aj, bj, zj);
+            double Se = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) Se += sq(log((phi[i] * Y[i] * P) / (di[i] * P) * Yt));
+            bool done;
+            if (first) {
+                first = false;
+                done  = !(Se > F.ssmsta_tol2);
+            } else {
+                iter++;
+                done = (iter > F.ssmsta_maxit) || !(Se > F.ssmsta_tol2);
+                if (iter > F.ssmsta_maxit) S.I(IF_STATUS, c) |= ST_SSMSTA_CAP;
+            }
+            if (done) {
+                S.D(F_::SeSSM, c) = Se;
+                S.D(F_::Yt, c)    = Yt;
+                S.D(F_::Asta, c)  = aj;
+                S.D(F_::Bsta, c)  = bj;
+                S.D(F_::Zsta, c)  = zj;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    S.D(F_::Y + i, c)    = Y[i];
+                    S.D(F_::phiS + i, c) = phi[i];
+                }
+                S.I(IF_IT0, c) += iter;
+                c = a.L.take(list, n);
+                if (c >= 0) load();
+            } else {
+                Yt = 0;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    Y[i] = di[i] / phi[i];
+                    Yt += Y[i];
+                }
+                const double r = 1 / Yt;
+#pragma unroll
+                for (int i = 0; i < NC; i++) Y[i] *= r;
+            }
+        }
+    }
+}
+
+// The verdict of StableSSM trial k (src/MixtureComp.cpp:1567-1578) once
+// StableNR is done: unstable -> split; stable -> next trial or finished.
+template <int NC>
+__device__ __forceinline__ void sta_decide(CellFlash<NC>& f, const PhasedArgs& a, int64_t c, uint32_t meta,
+                                           int k, bool flag)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S  = a.S;
+    const double    Se = S.D(F_::SeSSM, c);
+    if (flag && f.Yt > 1 + f.F.ssmsta_eyt) {
+        f.ssmsta_conflag = true;
+        f.ssmsta_realTol = sqrt(Se);
+        f.NP             = 2;
+        store_book(f, S, c, meta & ~(M_RESTART | M_SPPHASE));
+        a.L.push(L_SP_0, (int32_t)c);
+    } else if (k < 3) {
+        store_book(f, S, c, meta);
+        a.L.push(L_STA_0 + k + 1, (int32_t)c);
+    } else {
+        f.ssmsta_realTol = sqrt(Se);
+        finish_epec(f);
+        S.D(F_::ePEC, c) = f.ePEC;
+        store_single_phase(f, S, c);
+        store_book(f, S, c, meta);
+    }
+}
+
+// Start of StableNR (src/MixtureComp.cpp:1592-1598): residual of the
+// trial's end point; converged cells get their verdict here, the rest go to
+// the Newton kernel.
+template <int NC>
+__device__ void sta_verdict_body(const FluidConst& F, const PhasedArgs& a, int k)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_STA_0 + k, c)
+    {
+        CellFlash<NC> f(F);
+        uint32_t      meta;
+        load_book(f, S, c, meta);
+        const double P = a.in.P[c];
+        double       Se = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            const double fz = S.D(F_::di + i, c) * P;
+            const double fs = S.D(F_::phiS + i, c) * S.D(F_::Y + i, c) * P;
+            Se += sq(log(fz / (fs * f.Yt)));
+        }
+        Se = sqrt(Se);
+        if (Se > F.nrsta_tol) {
+            a.L.push(L_NRSTA_0 + k, (int32_t)c);
+        } else {
+            f.nrsta_conflag = true;
+            f.nrsta_realTol = Se;
+            sta_decide(f, a, c, meta, k, true);
+        }
+    }
+}
+
+// StableNR iterations (src/MixtureComp.cpp:1600-1635), one thread per cell.
+template <int NC>
+__device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_NRSTA_0 + k, c)
+    {
+        CellFlash<NC> f(F);
+        uint32_t      meta;
+        load_book(f, S, c, meta);
+        f.P = a.in.P[c];
+        double fugId[NC], Y[NC], fugSta[NC], res[NC];
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            f.sA[i]   = S.D(F_::sA + i, c);
+            f.Bi[i]   = S.D(F_::Bi + i, c);
+            fugId[i]  = S.D(F_::di + i, c) * f.P;
+            Y[i]      = S.D(F_::Y + i, c);
+            fugSta[i] = S.D(F_::phiS + i, c) * Y[i] * f.P;
+            res[i]    = log(fugId[i] / (fugSta[i] * f.Yt));
+        }
+        double Asta = S.D(F_::Asta, c), Bsta = S.D(F_::Bsta, c), Zsta = S.D(F_::Zsta, c);
+        double Se = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) Se += res[i] * res[i];
+        Se        = sqrt(Se);
+        int  iter = 0;
+        bool flag = true;
+        while (Se > F.nrsta_tol) {
+            f.sta_nr_update(Y, f.Yt, res, Asta, Bsta, Zsta);
+            f.fug_phi(Y, nullptr, fugSta, Asta, Bsta, Zsta);
+            Se = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                res[i] = log(fugId[i] / (fugSta[i] * f.Yt));
+                Se += res[i] * res[i];
+            }
+            Se = sqrt(Se);
+            iter++;
+            if (iter > F.nrsta_maxit) {
+                f.status |= ST_NRSTA_FAIL;
+                flag = false;
+                break;
+            }
+        }
+        f.it_nrsta += iter;
+        f.nrsta_conflag = flag;
+        f.nrsta_realTol = Se;
+        sta_decide(f, a, c, meta, k, flag);
+    }
+}
+
+// --------------------------------------------------------- relaxed stability
+// StableSSM01 trial k set-up (src/MixtureComp.cpp:1413-1421): K = Kw_k.
+template <int NC>
+__device__ void s01_prep_body(const FluidConst& F, const PhasedArgs& a, int k)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_S01_0 + k, c)
+    {
+        CellFlash<NC> f(F);
+        load_ptz(f, a, c);
+        f.cal_kwilson();
+#pragma unroll
+        for (int i = 0; i < NC; i++) S.D(F_::Ks + i, c) = f.kw(k, i);
+    }
+}
+
+// The iterations of one StableSSM01 trial (src/MixtureComp.cpp:1421-1466) on
+// a persistent grid: per turn, Y from K, the step test, one fugacity
+// evaluation, and the K update with its two convergence tests.
+template <int NC>
+__device__ void s01_ssm_body(const FluidConst& F, const PhasedArgs& a, int k)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S    = a.S;
+    const int       list = L_S01_0 + k;
+    const uint32_t  n    = a.L.len(list);
+    double          z[NC], ks[NC], dY_[NC], fid[NC], sA[NC], Bi[NC], Y[NC];
+    double          P = 0, Yt = 0, Se = 0, Sk = 0;
+    int             iter = 0;
+    int64_t         c    = a.L.take(list, n);
+    auto load = [&]() {
+        P = a.in.P[c];
+        double Ni[NC], Nh = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
+            Nh += fabs(Ni[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            z[i]   = Ni[i] / Nh;
+            ks[i]  = S.D(F_::Ks + i, c);
+            sA[i]  = S.D(F_::sA + i, c);
+            Bi[i]  = S.D(F_::Bi + i, c);
+            fid[i] = S.D(F_::phiZ + i, c) * z[i] * P;
+            dY_[i] = 0;
+        }
+        iter = 0;
+    };
+    auto finish = [&](bool flag) {
+        S.D(F_::SeSSM, c) = Se;
+        S.D(F_::SeSP, c)  = Sk;  // StableSSM01's Sk
+        S.D(F_::Yt, c)    = Yt;
+        S.I(IF_IT0, c) += iter;
+        S.I(IF_GUARD, c) = flag ? 1 : 0;  // the trial's convergence flag
+        c                = a.L.take(list, n);
+        if (c >= 0) load();
+    };
+    if (c >= 0) load();
+    while (__any_sync(0xffffffffu, c >= 0)) {
+        bool need = false;
+        if (c >= 0) {
+            Yt = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                Y[i] = z[i] * ks[i];
+                Yt += Y[i];
+            }
+            const double r = 1 / Yt;
+#pragma unroll
+            for (int i = 0; i < NC; i++) Y[i] *= r;
+            bool conv = false;
+            if (iter > 0) {
+                double dY = 0;
+#pragma unroll
+                for (int i = 0; i < NC; i++) dY += sq(Y[i] - dY_[i]);
+                conv = dY < 1e-6;  // dYtol, include/MixtureComp.hpp:34
+            }
+            if (conv)
+                finish(true);
+            else
+                need = true;
+        }
+        if (need) {
+            double fs[NC], aj, bj, zj;
+            fug_phi<NC>(F, sA, Bi, P, Y, nullptr, fs, aj, bj, zj);
+            Se = 0;
+            Sk = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                const double d = fid[i] / (fs[i] * Yt);
+                ks[i] *= d;
+                Se += sq(d - 1);
+                Sk += sq(log(ks[i]));
+            }
+            iter++;
+            if (Se < F.ssmsta_tol2 || Sk < 1e-4) {  // Ktol, include/MixtureComp.hpp:33
+                finish(true);
+            } else if (iter > F.ssmsta_maxit) {
+                S.I(IF_STATUS, c) |= ST_SSMSTA_CAP;
+                finish(false);
+            } else {
+#pragma unroll
+                for (int i = 0; i < NC; i++) dY_[i] = Y[i];
+            }
+        }
+    }
+}
+
+// End of StableSSM01 trial k (src/MixtureComp.cpp:1475-1489) and, after the
+// last trial or an unstable one, PhaseStable's fall-back to the strict test
+// when the verdict contradicts the last phase count (:1373-1383).
+template <int NC>
+__device__ void s01_end_body(const FluidConst& F, const PhasedArgs& a, int k)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_S01_0 + k, c)
+    {
+        CellFlash<NC> f(F);
+        uint32_t      meta;
+        load_book(f, S, c, meta);
+        const bool   flag = S.I(IF_GUARD, c) != 0;
+        const double Se   = S.D(F_::SeSSM, c);
+        const double Sk   = S.D(F_::SeSP, c);
+        S.I(IF_GUARD, c)  = 0;
+        if (flag && f.Yt > 1 - 0.1 && Sk > 1) f.flagSkip = false;
+        int verdict;  // 0 unstable, 1 stable, -1 next trial
+        if (flag && f.Yt > 1 + F.ssmsta_eyt) {
+            f.ssmsta_conflag = true;
+            f.ssmsta_realTol = sqrt(Se);
+            verdict          = 0;
+        } else if (k < 1) {
+            verdict = -1;
+        } else {
+            f.ssmsta_realTol = sqrt(Se);
+            verdict          = 1;
+        }
+        if (verdict < 0) {
+            store_book(f, S, c, meta);
+            a.L.push(L_S01_1, (int32_t)c);
+            continue;
+        }
+        // lNP of the cell (the last phase count, water excluded)
+        const uint32_t lastNP = a.in.lastNP[c];
+        const int      lNP    = lastNP > 0 ? (int)lastNP - 1 : 0;
+        const int      tmpNP  = f.NP + (verdict ? 0 : 1);
+        if (tmpNP != lNP) {
+            f.flagSkip = false;
+            store_book(f, S, c, meta);
+            a.L.push(L_STA_0, (int32_t)c);
+        } else if (verdict == 0) {
+            f.NP = 2;
+            store_book(f, S, c, meta & ~(M_RESTART | M_SPPHASE));
+            a.L.push(L_SP_0, (int32_t)c);
+        } else {
+            finish_epec(f);
+            S.D(F_::ePEC, c) = f.ePEC;
+            store_single_phase(f, S, c);
+            store_book(f, S, c, meta);
+        }
+    }
+}
+
+// ----------------------------------------------------------------- split
+// SplitSSM2 set-up (src/MixtureComp.cpp:1849-1879): initial K (last step's
+// K, or Wilson's) or the restart's, and the tolerance and iteration cap.
+template <int NC>
+__device__ void sp_prep_body(const FluidConst& F, const PhasedArgs& a, int r)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_SP_0 + r, c)
+    {
+        CellFlash<NC> f(F);
+        uint32_t      meta;
+        load_book(f, S, c, meta);
+        const bool restart = (meta & M_RESTART) != 0;
+        if (!restart) {
+            f.ssmsp_conflag = false;  // PhaseSplit, :1745-1749
+            f.nrsp_conflag  = false;
+            const uint32_t lastNP = a.in.lastNP[c];
+            const int      lNP    = lastNP > 0 ? (int)lastNP - 1 : 0;
+            if (lNP == 2) {
+                const int64_t N = a.stride;
+#pragma unroll
+                for (int i = 0; i < NC; i++)
+                    S.D(F_::Ks + i, c) = a.in.xij[(int64_t)i * N + c] / a.in.xij[(int64_t)(i + NC + 1) * N + c];
+            } else {
+                load_ptz(f, a, c);
+                f.cal_kwilson();
+#pragma unroll
+                for (int i = 0; i < NC; i++) S.D(F_::Ks + i, c) = f.Kw0[i];
+            }
+        }
+        f.ssmsp_conflag = true;
+        double Stol     = F.ssmsp_tol2;
+        int    maxIt    = F.ssmsp_maxit;
+        if (restart) {
+            Stol *= 1e-1;
+            maxIt *= 2;
+        }
+        if (f.Yt < 1.1) {
+            Stol *= 1e-1;
+            maxIt *= 2;
+        }
+        S.D(F_::Stol, c)  = Stol;
+        S.I(IF_MAXIT, c)  = maxIt;
+        store_book(f, S, c, meta);
+    }
+}
+
+// SplitSSM2's iterations (src/MixtureComp.cpp:1881-1902) on a persistent
+// grid: per turn, Rachford-Rice, the phase compositions, the fugacities of
+// both phases, and the K update.
+template <int NC>
+__device__ void sp_ssm_body(const FluidConst& F, const PhasedArgs& a, int r)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S    = a.S;
+    const int       list = L_SP_0 + r;
+    const uint32_t  n    = a.L.len(list);
+    CellFlash<NC>   f(F);  // holds z, K, x, phi, nu, Aj/Bj/Zj, sA, Bi
+    double          Stol = 0;
+    int             maxIt = 0, iter = 0;
+    int64_t         c     = a.L.take(list, n);
+    auto load = [&]() {
+        f.P = a.in.P[c];
+        double Ni[NC], Nh = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
+            Nh += fabs(Ni[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            f.zi[i] = Ni[i] / Nh;
+            f.Ks[i] = S.D(F_::Ks + i, c);
+            f.sA[i] = S.D(F_::sA + i, c);
+            f.Bi[i] = S.D(F_::Bi + i, c);
+        }
+        Stol     = S.D(F_::Stol, c);
+        maxIt    = S.I(IF_MAXIT, c);
+        iter     = 0;
+        f.it_rr  = 0;
+        f.NP     = 2;
+    };
+    if (c >= 0) load();
+    while (__any_sync(0xffffffffu, c >= 0)) {
+        if (c >= 0) {
+            f.rachford_rice2();
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                const double tmp = 1 + f.nu[0] * (f.Ks[i] - 1);
+                f.x[1][i]        = f.zi[i] / tmp;
+                f.x[0][i]        = f.Ks[i] * f.x[1][i];
+            }
+            double fug0[NC], fug1[NC];
+            fug_phi<NC>(F, f.sA, f.Bi, f.P, f.x[0], f.phi[0], fug0, f.Aj[0], f.Bj[0], f.Zj[0]);
+            fug_phi<NC>(F, f.sA, f.Bi, f.P, f.x[1], f.phi[1], fug1, f.Aj[1], f.Bj[1], f.Zj[1]);
+            double Se = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                Se += sq(fug1[i] / fug0[i] - 1);
+                f.Ks[i] = f.phi[1][i] / f.phi[0][i];
+            }
+            iter++;
+            const bool cap = iter > maxIt;
+            if (cap || !(Se > Stol)) {
+                if (cap) S.I(IF_META, c) &= ~(int32_t)M_C_SSMSP;
+                S.D(F_::SeSP, c) = Se;
+                S.I(IF_IT2, c) += iter;
+                S.I(IF_IT4, c) += f.it_rr;
+#pragma unroll
+                for (int i = 0; i < NC; i++) S.D(F_::Ks + i, c) = f.Ks[i];
+                store_split(f, S, c);
+                c = a.L.take(list, n);
+                if (c >= 0) load();
+            }
+        }
+    }
+}
+
+// End of PhaseSplit once SplitNR is done (src/MixtureComp.cpp:1750-1758,
+// 1784-1836): accept, restart the SSM, or collapse to one phase.
+template <int NC>
+__device__ __forceinline__ void sp_after_nr(CellFlash<NC>& f, const PhasedArgs& a, int64_t c, uint32_t meta,
+                                            int r, double eNR, int iter)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    f.nrsp_realTol    = eNR;
+    if (eNR < f.F.nrsp_tol) f.nrsp_conflag = true;
+    f.it_nrsp += iter;
+    bool restart = false;
+    if (!(meta & M_SPPHASE)) {
+        if (!f.nrsp_conflag) {
+            restart = true;
+            meta |= M_SPPHASE | M_RESTART;
+            S.I(IF_GUARD, c) = 1;
+        }
+    } else if (!f.check_split()) {
+        // collapsed: the final check below is a no-op
+    } else if (f.ssmsp_conflag || f.nrsp_conflag) {
+        // loop ends
+    } else {
+        const int g      = S.I(IF_GUARD, c) + 1;
+        S.I(IF_GUARD, c) = g;
+        if (g > SPLIT_RESTART_CAP)
+            f.status |= ST_SPLIT_CAP;
+        else
+            restart = true;
+    }
+    if (restart) {
+        store_split(f, S, c);
+        store_book(f, S, c, meta);
+        a.L.push(r + 1 < SPLIT_ROUNDS ? L_SP_0 + r + 1 : L_SLOW, (int32_t)c);
+        return;
+    }
+    f.check_split();
+    if (!f.ssmsp_conflag) f.status |= ST_SSMSP_FAIL;
+    if (!f.nrsp_conflag) f.status |= ST_NRSP_FAIL;
+    finish_epec(f);
+    S.D(F_::ePEC, c) = f.ePEC;
+    if (f.NP == 1) {
+        S.D(F_::Aj0, c) = f.Aj[0];
+        S.D(F_::Bj0, c) = f.Bj[0];
+        S.D(F_::Zj0, c) = f.Zj[0];
+        store_single_phase(f, S, c);
+    } else {
+        store_split(f, S, c);
+    }
+    store_book(f, S, c, meta);
+}
+
+// Loads a split cell into a CellFlash for the thread-per-item kernels.
+template <int NC>
+__device__ __forceinline__ void load_split_cell(CellFlash<NC>& f, const PhasedArgs& a, int64_t c, uint32_t& meta)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    load_book(f, S, c, meta);
+    f.P      = a.in.P[c];
+    double Ni[NC], Nh = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
+        Nh += fabs(Ni[i]);
+    }
+    f.Nh = Nh;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        f.zi[i] = Ni[i] / Nh;
+        f.sA[i] = S.D(F_::sA + i, c);
+        f.Bi[i] = S.D(F_::Bi + i, c);
+    }
+    load_split(f, S, c);
+}
+
+// Start of SplitNR (src/MixtureComp.cpp:2059-2069): n = nu x and the
+// residual; converged cells finish PhaseSplit here, the rest go to Newton.
+template <int NC>
+__device__ void sp_nrinit_body(const FluidConst& F, const PhasedArgs& a, int r)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_SP_0 + r, c)
+    {
+        CellFlash<NC> f(F);
+        uint32_t      meta;
+        load_split_cell(f, a, c, meta);
+        f.ssmsp_realTol = sqrt(S.D(F_::SeSP, c));
+        f.nrsp_conflag  = false;
+        double eNR      = 0;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            f.n[0][i] = f.nu[0] * f.x[0][i];
+            f.n[1][i] = f.nu[1] * f.x[1][i];
+            const double res = log(f.fug[1][i] / f.fug[0][i]);
+            eNR += res * res;
+        }
+        eNR = sqrt(eNR);
+        if (eNR > F.nrsp_tol) {
+            S.D(F_::eNR0, c) = eNR;
+            store_split(f, S, c);
+            store_book(f, S, c, meta);
+            a.L.push(L_SPNR_0 + r, (int32_t)c);
+        } else {
+            sp_after_nr(f, a, c, meta, r, eNR, 0);
+        }
+    }
+}
+
+// SplitNR iterations (src/MixtureComp.cpp:2071-2152), one thread per cell.
+template <int NC>
+__device__ void sp_nr_body(const FluidConst& F, const PhasedArgs& a, int r)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_SPNR_0 + r, c)
+    {
+        CellFlash<NC> f(F);
+        uint32_t      meta;
+        load_split_cell(f, a, c, meta);
+        const double eNR0 = S.D(F_::eNR0, c);
+        double       res[NC];
+#pragma unroll
+        for (int i = 0; i < NC; i++) res[i] = log(f.fug[1][i] / f.fug[0][i]);
+        double eNR  = eNR0;
+        int    iter = 0;
+        while (eNR > F.nrsp_tol) {
+            const double en = f.sp_nr_update(res);
+            f.fug_phi_all();
+            eNR = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                res[i] = log(f.fug[1][i] / f.fug[0][i]);
+                eNR += res[i] * res[i];
+            }
+            eNR = sqrt(eNR);
+            iter++;
+            if (eNR > eNR0 || iter > F.nrsp_maxit) break;
+            if (en / (2 * NC) < 1e-8) {
+                f.nrsp_conflag = true;
+                break;
+            }
+        }
+        sp_after_nr(f, a, c, meta, r, eNR, iter);
+    }
+}
+
+// The rest of PhaseSplit's restart loop for cells still restarting after the
+// last split round (rare), on one thread each, with the plain form's code.
+template <int NC>
+__device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_SLOW, c)
+    {
+        CellFlash<NC> f(F);
+        uint32_t      meta;
+        load_split_cell(f, a, c, meta);
+        f.T = a.in.T[c] + CONV5;
+        f.cal_kwilson();
+        int guard = S.I(IF_GUARD, c);
+        while (true) {
+            f.split_ssm2(true);
+            f.split_nr();
+            if (!f.check_split()) break;
+            if (f.ssmsp_conflag || f.nrsp_conflag) break;
+            if (++guard > SPLIT_RESTART_CAP) {
+                f.status |= ST_SPLIT_CAP;
+                break;
+            }
+        }
+        f.check_split();
+        if (!f.ssmsp_conflag) f.status |= ST_SSMSP_FAIL;
+        if (!f.nrsp_conflag) f.status |= ST_NRSP_FAIL;
+        finish_epec(f);
+        S.D(F_::ePEC, c) = f.ePEC;
+        if (f.NP == 1) {
+            S.D(F_::Aj0, c) = f.Aj[0];
+            S.D(F_::Bj0, c) = f.Bj[0];
+            S.D(F_::Zj0, c) = f.Zj[0];
+            store_single_phase(f, S, c);
+        } else {
+            store_split(f, S, c);
+        }
+        store_book(f, S, c, meta);
+    }
+}
+
+// --------------------------------------------------------------- finalize
+template <int NC>
+__device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        FimCell<NC> f(F);
+        f.load_inputs(c, a.stride, a.in, a.sk);
+        uint32_t meta;
+        load_book(f, S, c, meta);
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            f.sA[i] = S.D(F_::sA + i, c);
+            f.Bi[i] = S.D(F_::Bi + i, c);
+        }
+        f.ePEC  = S.D(F_::ePEC, c);
+        f.nu[0] = S.D(F_::nu0, c);
+        f.nu[1] = S.D(F_::nu1, c);
+        f.Aj[0] = S.D(F_::Aj0, c);
+        f.Aj[1] = S.D(F_::Aj1, c);
+        f.Bj[0] = S.D(F_::Bj0, c);
+        f.Bj[1] = S.D(F_::Bj1, c);
+        f.Zj[0] = S.D(F_::Zj0, c);
+        f.Zj[1] = S.D(F_::Zj1, c);
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            f.x[0][i] = S.D(F_::x0 + i, c);
+            f.x[1][i] = S.D(F_::x1 + i, c);
+            f.n[0][i] = S.D(F_::n0 + i, c);
+            f.n[1][i] = S.D(F_::n1 + i, c);
+        }
+        f.finalize(c, a.stride, a.sk, a.out);
+    }
+}
+
+}  // namespace ocpf
