@@ -182,15 +182,20 @@ __device__ __forceinline__ void store_book(const CellFlash<NC>& f, const StateBu
     S.D(F_::Yt, c)          = f.Yt;
 }
 
-// Equilibrium of a single-phase cell for the finalize kernel: z with the
-// mixture a, b, Z of phase 0 (already stored).
+// Equilibrium of a single-phase cell for the finalize kernel: nu0 = 1 with
+// x0 = z and the mixture a, b, Z of phase 0. init stores x0 = z for every
+// cell; only kernels that overwrote x0 (the split) pass write_x = true and
+// must have f.zi loaded.
 template <int NC>
-__device__ __forceinline__ void store_single_phase(const CellFlash<NC>& f, const StateBuf& S, int64_t c)
+__device__ __forceinline__ void store_single_phase(const CellFlash<NC>& f, const StateBuf& S, int64_t c,
+                                                   bool write_x = false)
 {
-    using F_         = SF<NC>;
-    S.D(F_::nu0, c)  = 1.0;
+    using F_        = SF<NC>;
+    S.D(F_::nu0, c) = 1.0;
+    if (write_x) {
 #pragma unroll
-    for (int i = 0; i < NC; i++) S.D(F_::x0 + i, c) = f.zi[i];
+        for (int i = 0; i < NC; i++) S.D(F_::x0 + i, c) = f.zi[i];
+    }
 }
 
 template <int NC>

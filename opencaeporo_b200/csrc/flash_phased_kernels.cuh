@@ -35,6 +35,7 @@ __device__ void init_body(const FluidConst& F, const PhasedArgs& a)
             S.D(F_::Bi + i, c) = f.Bi[i];
         }
         S.I(IF_GUARD, c) = 0;
+        store_single_phase(f, S, c, true);  // x0 = z until a split replaces it
         if (f.ftype == 0 || f.ftype == 1) {
             f.flagSkip = true;
             f.NP       = 1;
@@ -607,7 +608,7 @@ __device__ __forceinline__ void sp_after_nr(CellFlash<NC>& f, const PhasedArgs& 
         S.D(F_::Aj0, c) = f.Aj[0];
         S.D(F_::Bj0, c) = f.Bj[0];
         S.D(F_::Zj0, c) = f.Zj[0];
-        store_single_phase(f, S, c);
+        store_single_phase(f, S, c, true);
     } else {
         store_split(f, S, c);
     }
@@ -744,7 +745,7 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
             S.D(F_::Aj0, c) = f.Aj[0];
             S.D(F_::Bj0, c) = f.Bj[0];
             S.D(F_::Zj0, c) = f.Zj[0];
-            store_single_phase(f, S, c);
+            store_single_phase(f, S, c, true);
         } else {
             store_split(f, S, c);
         }
