@@ -46,6 +46,10 @@ extern "C" {
 #define OCPF_ECUDA 2        /* a CUDA runtime call failed */
 #define OCPF_ENOMEM 3       /* device allocation failed */
 #define OCPF_EUNSUPPORTED 4 /* e.g. no sm_100 device */
+#define OCPF_ERANGE 5       /* batch larger than OCPF_NOALLOC_MAX_CELLS (ocpf_flash_fim_noalloc) */
+
+/* largest batch ocpf_flash_fim_noalloc accepts */
+#define OCPF_NOALLOC_MAX_CELLS 4096
 
 /* per-cell status bits (ocpf_fim_out.status) */
 #define OCPF_CELL_SSMSTA_CAP 0x01  /* a stability SSM trial hit maxIt */
@@ -182,6 +186,28 @@ int ocpf_flash_fim(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_ski
  * first call that needs more. No reference counterpart (the reference keeps
  * its scratch inside each MixtureComp object). */
 int ocpf_reserve(ocpf_ctx* ctx, int64_t ncell);
+
+/* The batched form (OCPF_FORM_BATCHED) for callers that cannot allocate
+ * device memory: applications that own all of the GPU's memory through their
+ * own pool or arena, run under a fixed device-memory budget, or must not let
+ * a flash call synchronise the device (cudaMalloc and cudaFree may). Its
+ * scratch -- per-cell phase state and cell lists, ~1.5 KB per cell for up to
+ * 12 components -- lives in one array compiled into the library, of
+ * OCPF_NOALLOC_MAX_CELLS cells (about 6.3 MB, held on every GPU that loads
+ * the library until the process exits). The caller passes inputs and outputs
+ * as for ocpf_flash_fim; the call allocates nothing and is asynchronous on
+ * `stream`. Returns OCPF_ERANGE, without touching the GPU, when ncell exceeds
+ * OCPF_NOALLOC_MAX_CELLS.
+ * The first call on a device looks up the array's device address there
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * Every call on a device uses the same array and leaves its contents behind;
+ * the call clears what must start empty itself. Calls whose work overlaps on
+ * the GPU (two streams, or two host threads) race on the array and corrupt
+ * each other: issue them one after another on one stream.
+ * No counterpart in the reference (it keeps its scratch inside each
+ * MixtureComp object on the host). */
+int ocpf_flash_fim_noalloc(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
+                           ocpf_fim_out* out, void* stream);
 
 /* Same call with every array in HOST memory (pinned memory is faster). The
  * cells are streamed through device staging buffers owned by the context in

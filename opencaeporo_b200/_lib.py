@@ -15,7 +15,8 @@ LIB_PATH = os.path.join(PKG, "libocpflash.so")
 MAX_NC = 16
 NPH = 3
 
-OCPF_OK, OCPF_EINVAL, OCPF_ECUDA, OCPF_ENOMEM, OCPF_EUNSUPPORTED = 0, 1, 2, 3, 4
+OCPF_OK, OCPF_EINVAL, OCPF_ECUDA, OCPF_ENOMEM, OCPF_EUNSUPPORTED, OCPF_ERANGE = 0, 1, 2, 3, 4, 5
+NOALLOC_MAX_CELLS = 4096  # OCPF_NOALLOC_MAX_CELLS
 FORM_PLAIN, FORM_BATCHED, FORM_MIXED, FORM_FAST = 0, 1, 2, 3
 
 CELL_SSMSTA_CAP = 0x01
@@ -31,7 +32,7 @@ CELL_GUARD = 0x100
 # Every function the header declares (checked by the CPU test suite).
 EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_flash_fim", "ocpf_flash_fim_host", "ocpf_last_kernel_ms",
-           "ocpf_measure_fma_peak", "ocpf_reserve")
+           "ocpf_measure_fma_peak", "ocpf_reserve", "ocpf_flash_fim_noalloc")
 
 _vp = C.c_void_p
 
@@ -128,6 +129,9 @@ def lib():
     L.ocpf_measure_fma_peak.restype = C.c_int
     L.ocpf_reserve.argtypes = [_vp, C.c_int64]
     L.ocpf_reserve.restype = C.c_int
+    L.ocpf_flash_fim_noalloc.argtypes = [_vp, C.c_int64, C.POINTER(FimIn), C.POINTER(Skip),
+                                         C.POINTER(FimOut), _vp]
+    L.ocpf_flash_fim_noalloc.restype = C.c_int
     _LIB = L
     return L
 

@@ -146,6 +146,7 @@ extern "C" const char* ocpf_status_string(int code)
         case OCPF_ECUDA: return "CUDA runtime error";
         case OCPF_ENOMEM: return "device allocation failed";
         case OCPF_EUNSUPPORTED: return "unsupported";
+        case OCPF_ERANGE: return "batch larger than OCPF_NOALLOC_MAX_CELLS";
         default: return "unknown";
     }
 }
@@ -561,3 +562,13 @@ extern "C" int ocpf_reserve(ocpf_ctx* c, int64_t ncell)
     if (prev != c->device) cudaSetDevice(prev);
     return rc;
 }
+
+// Accessors for the library's other translation units.
+namespace ocpf {
+const FluidConst* ctx_fluid_const(const ocpf_ctx* c) { return &c->fc; }
+int               ctx_device(const ocpf_ctx* c) { return c->device; }
+bool ctx_fim_args_ok(const ocpf_ctx* c, const ocpf_fim_in* in, const ocpf_skip* sk, const ocpf_fim_out* o)
+{
+    return fim_args_ok(c, in, sk, o);
+}
+}  // namespace ocpf
