@@ -145,6 +145,17 @@ def flash_fim(kind: str, fluid, P, T, Ni, S=None, lastNP=None, xij=None, skip=No
     nc = fluid.nc
     ncom = nc + 1
     n = int(np.asarray(P).shape[0])
+    if kind == "reference" and not fluid.controls.use_skip:
+        # The reference's FlashFIM sets SkipStaAnaly::flag[bulkId] after every
+        # flash (CalSkipForNextStep, src/MixtureComp.cpp:5253 ->
+        # include/AcceleratePVT.hpp:36) even when the skip option is off and
+        # the array was never allocated (src/MixtureComp.cpp:5130-5131): a
+        # write through an empty vector that crashes. Run it with the option
+        # on and a fresh cache (flag 0: no cell skips, every cell takes the
+        # full path), which gives the same flash; the cache it fills is
+        # discarded.
+        fluid = fluid.with_controls(use_skip=True)
+        skip = None
     P = np.ascontiguousarray(P, dtype=np.float64)
     T = np.ascontiguousarray(T, dtype=np.float64)
     Ni = np.ascontiguousarray(np.asarray(Ni, dtype=np.float64).reshape(n, ncom))

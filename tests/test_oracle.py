@@ -98,3 +98,19 @@ def test_compare_flags_planted_error():
     bad["phaseNum"][1] = 2
     res = CMP.compare(bad, ref, fl.nc)
     assert list(res["np_mismatch"]) == [1]
+
+
+@pytest.mark.skipif(not O.available("reference"), reason="oracle/_ref not built")
+def test_reference_with_skip_option_off():
+    """With the skip option off the reference's FlashFIM writes its skip flag
+    through an unallocated array; the loader runs it with the option on and a
+    fresh cache instead, which must give the same flash as the port with the
+    option off."""
+    fl, inp, _, _ = load_golden("uniform_nc6")
+    fl = fl.with_controls(use_skip=False)
+    P = np.full(64, 72.5)
+    T, Ni = inp["T"][:64], inp["Ni"][:64]
+    a = O.flash_fim("reference", fl, P, T, Ni, nthreads=2)
+    b = O.flash_fim("port", fl, P, T, Ni, nthreads=2)
+    assert np.array_equal(a["NPhc"], b["NPhc"])
+    assert np.array_equal(a["ftype"], np.zeros(64, np.int32))
