@@ -37,7 +37,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "flash states/s at 1M cells: mixed+learned vs plain FP64 GPU, err vs FP64 oracle"
 NCELL = 1 << 20
-SEED = 2025
+from opencaeporo_b200.workload import BISECT_STEPS, SEED  # noqa: E402
 
 
 def parse():
@@ -111,45 +111,7 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- workload
-def bench_fluid():
-    from opencaeporo_b200.fluid import synthetic_fluid
-    return synthetic_fluid(6, 1234)
-
-
-def gpu_phase_counter(fluid, device, chunk=1 << 18):
-    """Hydrocarbon phase count of (P, T, Ni) batches with the plain GPU flash
-    (used only to place the near-envelope states)."""
-    import torch
-    from opencaeporo_b200.flash import MixtureCompBatch
-    fl = fluid.with_controls(use_skip=False)
-    m = MixtureCompBatch(fl, device)
-    st = m.new_state(chunk)
-
-    def count(P, T, Ni):
-        n = len(P)
-        res = np.empty(n, np.int64)
-        for c0 in range(0, n, chunk):
-            c1 = min(n, c0 + chunk)
-            k = c1 - c0
-            P_ = np.full(chunk, 1000.0)
-            T_ = np.full(chunk, 100.0)
-            N_ = np.tile(Ni[c0:c0 + 1], (chunk, 1))
-            P_[:k], T_[:k], N_[:k] = P[c0:c1], T[c0:c1], Ni[c0:c1]
-            st.load(P_, T_, N_)
-            st.out["phaseNum"].zero_()
-            m.flash_fim(st, diagnostics=False)
-            res[c0:c1] = st.out["phaseNum"][:k].cpu().numpy() - 1
-        return res
-
-    return count, m
-
-
-def make_workload(fluid, n, seed, device):
-    from opencaeporo_b200 import synth
-    count, m = gpu_phase_counter(fluid, device)
-    w = synth.mixed_states(fluid, n, seed, count, near_frac=0.3)
-    m.close()
-    return w
+from opencaeporo_b200.workload import bench_fluid, gpu_phase_counter, make_workload  # noqa: E402
 
 
 # ------------------------------------------------------------ reference arm
@@ -167,7 +129,7 @@ def reference_arm(args):
     def pc(P, T, Ni):
         return O.flash_fim(kind, fl.with_controls(use_skip=False), P, T, Ni, nthreads=cores)["NPhc"]
 
-    w = synth.mixed_states(fl, ns, SEED, pc, near_frac=0.3)
+    w = synth.mixed_states(fl, ns, SEED, pc, near_frac=0.3, steps=BISECT_STEPS)
     times = []
     for s in range(args.warmup + args.steps):
         r = O.flash_fim(kind, fl, w["P"], w["T"], w["Ni"], nthreads=cores)

@@ -228,6 +228,46 @@ int ocpf_last_kernel_ms(ocpf_ctx* ctx, float* ms);
  * counterpart (measurement utility). */
 int ocpf_measure_fma_peak(int device, int bits, double* tflops);
 
+/* ---- Learned initialiser (no counterpart in the reference) -------------
+ * A small MLP predicts, from a cell's (ln P, T, z), whether its feed is
+ * unstable (a logit) and the ln K of the split. Layers nin -> 64 -> 64 ->
+ * nout with SiLU, BF16 weights and activations, FP32 accumulation, run on the
+ * tensor cores. For an NC-component fluid nin = NC + 2 and nout = NC + 1
+ * (output 0: logit of "unstable"; outputs 1..NC: ln K_i = ln(y_i / x_i),
+ * vapour over liquid). Parameters are one FP32 vector of
+ * ocpf_mlp_param_count() floats: W1[64][16] b1[64] W2[64][64] b2[64]
+ * W3[16][64] b3[16], row-major [out][in], zero beyond nin / nout.
+ * Arrays are device memory, feature-major: x[f * n + s]. */
+#define OCPF_MLP_HIDDEN 64
+#define OCPF_MLP_MAX_IO 16
+
+int ocpf_mlp_param_count(void);
+
+/* y[j * n + s] = MLP(x[:, s])_j for j < nout. */
+int ocpf_mlp_forward(int nin, int nout, int64_t n, const float* params, const float* x, float* y, void* stream);
+
+/* Adds to grad (ocpf_mlp_param_count() floats) the gradient of the mean loss
+ *   1/n sum_s [ softplus(o_0) - t_0 o_0 + lnk_weight w_s / (nout-1) sum_{j>=1} (o_j - t_j)^2 ]
+ * (targets t[j * n + s], t_0 in {0, 1}; w_s = wmask[s], 0 for samples with
+ * no split) and adds the two loss sums (logistic, ln K) to loss[0], loss[1]. */
+int ocpf_mlp_grad(int nin, int nout, int64_t n, const float* params, const float* x, const float* target,
+                  const float* wmask, float lnk_weight, float* grad, float* loss, void* stream);
+
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8, bias-corrected at `step` >= 1)
+ * of the FP32 parameters from grad, with moment buffers m, v; zeroes grad. */
+int ocpf_mlp_adam(float* params, float* grad, float* m, float* v, int step, float lr, void* stream);
+
+/* Attaches a trained initialiser to a context for OCPF_FORM_FAST: params
+ * (host, ocpf_mlp_param_count() floats), the input normalisation
+ * (feature f = (raw_f - in_mean[f]) / in_scale[f] for the raw features
+ * ln(P / psia), T / degF, z_1..z_NC; host arrays of NC + 2) and the
+ * confidence at or above which a fresh cell's predicted instability is
+ * acted on (the split starts from the predicted K; the stability test runs
+ * only if that split fails). Without one, OCPF_FORM_FAST runs as
+ * OCPF_FORM_MIXED. */
+int ocpf_set_initializer(ocpf_ctx* ctx, const float* params, const float* in_mean, const float* in_scale,
+                         float confidence);
+
 #ifdef __cplusplus
 }
 #endif

@@ -32,7 +32,9 @@ CELL_GUARD = 0x100
 # Every function the header declares (checked by the CPU test suite).
 EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_flash_fim", "ocpf_flash_fim_host", "ocpf_last_kernel_ms",
-           "ocpf_measure_fma_peak", "ocpf_reserve", "ocpf_flash_fim_noalloc")
+           "ocpf_measure_fma_peak", "ocpf_reserve", "ocpf_flash_fim_noalloc",
+           "ocpf_mlp_param_count", "ocpf_mlp_forward", "ocpf_mlp_grad", "ocpf_mlp_adam",
+           "ocpf_set_initializer")
 
 _vp = C.c_void_p
 
@@ -132,6 +134,16 @@ def lib():
     L.ocpf_flash_fim_noalloc.argtypes = [_vp, C.c_int64, C.POINTER(FimIn), C.POINTER(Skip),
                                          C.POINTER(FimOut), _vp]
     L.ocpf_flash_fim_noalloc.restype = C.c_int
+    L.ocpf_mlp_param_count.restype = C.c_int
+    L.ocpf_mlp_forward.argtypes = [C.c_int, C.c_int, C.c_int64, _vp, _vp, _vp, _vp]
+    L.ocpf_mlp_forward.restype = C.c_int
+    L.ocpf_mlp_grad.argtypes = [C.c_int, C.c_int, C.c_int64, _vp, _vp, _vp, _vp, C.c_float, _vp, _vp, _vp]
+    L.ocpf_mlp_grad.restype = C.c_int
+    L.ocpf_mlp_adam.argtypes = [_vp, _vp, _vp, _vp, C.c_int, C.c_float, _vp]
+    L.ocpf_mlp_adam.restype = C.c_int
+    L.ocpf_set_initializer.argtypes = [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                       C.c_float]
+    L.ocpf_set_initializer.restype = C.c_int
     _LIB = L
     return L
 

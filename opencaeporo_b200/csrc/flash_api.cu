@@ -104,7 +104,8 @@ bool make_fluid_const(const ocpf_fluid& in, FluidConst& f)
         f.lbc2[i]    = std::pow(in.Pc[i], 2.0 / 3);
         for (int k = 0; k < nc; k++) {
             if (in.BIC[i * nc + k] != in.BIC[k * nc + i]) return false;
-            f.omb[i * MAXNC + k] = 1 - in.BIC[i * nc + k];
+            f.omb[i * MAXNC + k]  = 1 - in.BIC[i * nc + k];
+            f.ombf[i * MAXNC + k] = (float)f.omb[i * MAXNC + k];
         }
     }
     for (int k = 0; k < 5; k++) {
@@ -132,6 +133,8 @@ struct ocpf_ctx {
     // counters, in parts of part_cap cells (the host path uses two parts)
     int64_t     eq_cap;    // total cells the scratch holds
     void*       eq;
+    // learned initialiser parameters (device, MLP_NPARAM floats) or null
+    float*      mlp;
 };
 
 static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
@@ -176,6 +179,7 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->hs[0] = c->hs[1] = nullptr;
     c->eq_cap    = 0;
     c->eq        = nullptr;
+    c->mlp       = nullptr;
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         cudaSetDevice(prev);
@@ -196,6 +200,7 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     cudaEventDestroy(c->ev1);
     if (c->stage) cudaFree(c->stage);
     if (c->eq) cudaFree(c->eq);
+    if (c->mlp) cudaFree(c->mlp);
     for (auto& s : c->hs)
         if (s) cudaStreamDestroy(s);
     cudaSetDevice(prev);
@@ -283,6 +288,9 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         args.in     = in;
         args.sk     = sk;
         args.out    = out;
+        args.opts   = form >= OCPF_FORM_MIXED ? PH_MIXED : 0u;
+        args.mlp    = c->mlp;
+        if (form == OCPF_FORM_FAST && c->mlp && c->fc.learn_on) args.opts |= PH_LEARN;
         if (part < 0) {
             const int rc = ensure_scratch(c, count);
             if (rc != OCPF_OK) return rc;
@@ -559,6 +567,38 @@ extern "C" int ocpf_reserve(ocpf_ctx* c, int64_t ncell)
     cudaGetDevice(&prev);
     if (prev != c->device) cudaSetDevice(c->device);
     const int rc = ensure_scratch(c, ncell);
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+extern "C" int ocpf_set_initializer(ocpf_ctx* c, const float* params, const float* in_mean, const float* in_scale,
+                                    float confidence)
+{
+    if (!c || !params || !in_mean || !in_scale || !(confidence > 0.5f) || !(confidence < 1.0f)) return OCPF_EINVAL;
+    const int nf = c->fc.nc + 2;
+    for (int f = 0; f < nf; f++)
+        if (!(in_scale[f] > 0.f) || !std::isfinite(in_mean[f])) return OCPF_EINVAL;
+    const int np = ocpf_mlp_param_count();
+    for (int i = 0; i < np; i++)
+        if (!std::isfinite(params[i])) return OCPF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    int rc = OCPF_OK;
+    if (!c->mlp && cudaMalloc(&c->mlp, sizeof(float) * np) != cudaSuccess) {
+        c->mlp = nullptr;
+        rc     = OCPF_ENOMEM;
+    }
+    if (rc == OCPF_OK && cudaMemcpy(c->mlp, params, sizeof(float) * np, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = OCPF_ECUDA;
+    if (rc == OCPF_OK) {
+        for (int f = 0; f < nf; f++) {
+            c->fc.lin_mean[f]  = in_mean[f];
+            c->fc.lin_scale[f] = in_scale[f];
+        }
+        c->fc.learn_conf = confidence;
+        c->fc.learn_on   = 1;
+    }
     if (prev != c->device) cudaSetDevice(prev);
     return rc;
 }

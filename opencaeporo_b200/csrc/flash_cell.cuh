@@ -33,6 +33,20 @@ __device__ __forceinline__ void mix_ab(const FluidConst& F, const double* sA, co
     }
 }
 
+// phi_i of CalFugPhi (src/MixtureComp.cpp:1009-1013) from bi = B_i / b,
+// t_i, 1/a, Z - 1, ln(Z - b), a / ((d1 - d2) b) and ln((Z + d1 b) / (Z + d2 b)).
+// One expression shared by every form so that each evaluates it alike.
+__device__ __forceinline__ double phi_term(double bi, double ti, double ia, double zm1, double L1, double cf,
+                                           double L2)
+{
+    return exp(bi * zm1 - L1 - cf * (2 * ti * ia - bi) * L2);
+}
+
+// The per-phase logarithms of CalFugPhi, ln(Z - b) and ln((Z + d1 b) /
+// (Z + d2 b)), as separate pieces (a warp forms them on different lanes).
+__device__ __forceinline__ double fug_L1(double zj, double bj) { return log(zj - bj); }
+__device__ __forceinline__ double fug_L2(double zj, double bj) { return log((zj + D1 * bj) / (zj + D2 * bj)); }
+
 // CalFugPhi (src/MixtureComp.cpp:993-1101): the fugacity coefficients phi
 // and fugacities f = phi x P of composition xj (phiT may be null), with the
 // mixture's a, b and Z (SolEoS).
@@ -44,16 +58,15 @@ __device__ __forceinline__ void fug_phi(const FluidConst& F, const double* sA, c
     double t[NC];
     mix_ab<NC>(F, sA, Bi, xj, t, aj, bj);
     zj               = sol_eos(aj, bj);
-    const double L1  = log(zj - bj);
-    const double L2  = log((zj + D1 * bj) / (zj + D2 * bj));
+    const double L1  = fug_L1(zj, bj);
+    const double L2  = fug_L2(zj, bj);
     const double ib  = 1.0 / bj;
     const double ia  = 1.0 / aj;
     const double cf  = aj / D1MD2 * ib;
     const double zm1 = zj - 1;
 #pragma unroll
     for (int i = 0; i < NC; i++) {
-        const double bi = Bi[i] * ib;
-        const double ph = exp(bi * zm1 - L1 - cf * (2 * t[i] * ia - bi) * L2);
+        const double ph = phi_term(Bi[i] * ib, t[i], ia, zm1, L1, cf, L2);
         if (phiT) phiT[i] = ph;
         if (fugT) fugT[i] = ph * xj[i] * P;
     }

@@ -43,6 +43,11 @@ struct FluidConst {
     double  L[5];                // LBC coefficients x 10
     double  pvtw[5];
     double  std_rho_w;
+    float   ombf[MAXNC * MAXNC];  // omb in FP32, for the mixed form's fugacities
+    // learned initialiser (OCPF_FORM_FAST): input normalisation, confidence
+    float   lin_mean[MAXNC + 2], lin_scale[MAXNC + 2];
+    float   learn_conf;
+    int32_t learn_on;
 };
 
 // per-cell status bits mirror OCPF_CELL_*

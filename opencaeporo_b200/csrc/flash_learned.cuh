@@ -1,0 +1,93 @@
+// flash_learned.cuh -- the learned initialiser inside the fast form
+// (OCPF_FORM_FAST): fresh cells (no last phase count) are run through the
+// MLP of learned.cuh on the tensor cores, 16 cells per warp. A cell whose
+// predicted probability of being unstable reaches the confidence goes
+// straight to a split (round LEARN_ROUND) started from the predicted K; the
+// rest, and every cell whose learned split fails its checks
+// (learned_after_nr), take the strict stability test as in the other forms.
+// No counterpart in the reference.
+#pragma once
+
+#include "flash_phased.cuh"
+#include "learned.cuh"
+
+namespace ocpf {
+
+struct LearnSmem {
+    MlpSmemW w;
+    bf16     xs[64 * MLP_IO];
+    bf16     h1[64 * MLP_H], h2[64 * MLP_H];
+    float    out[64 * MLP_IO];
+};
+
+// One CTA of 128 threads takes the fresh-cell list in tiles of 64 cells.
+// Features: ln(P / psia), T / degF, z_1..z_NC, each normalised by the
+// initialiser's mean and scale.
+template <int NC>
+__device__ void learn_body(const FluidConst& F, const PhasedArgs& a, LearnSmem& sm)
+{
+    using F_ = SF<NC>;
+    static_assert(NC + 2 <= MLP_IO && NC + 1 <= MLP_IO, "network width");
+    const StateBuf& S = a.S;
+    const uint32_t  n = a.L.len(L_FRESH);
+    const int       m0 = 16 * (threadIdx.x >> 5);
+    mlp_load_weights(sm.w, a.mlp);
+    for (uint32_t base = blockIdx.x * 64u; base < n; base += gridDim.x * 64u) {
+        __syncthreads();  // weights loaded / previous tile's outputs consumed
+        if (threadIdx.x < 64) {
+            const uint32_t k = base + threadIdx.x;
+            float          f[MLP_IO];
+#pragma unroll
+            for (int j = 0; j < MLP_IO; j++) f[j] = 0.f;
+            if (k < n) {
+                const int64_t c = a.L.item(L_FRESH, k);
+                double        Ni[NC], Nh = 0;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
+                    Nh += fabs(Ni[i]);
+                }
+                f[0] = (float)log(a.in.P[c]);
+                f[1] = (float)a.in.T[c];
+#pragma unroll
+                for (int i = 0; i < NC; i++) f[2 + i] = (float)(Ni[i] / Nh);
+#pragma unroll
+                for (int j = 0; j < NC + 2; j++) f[j] = (f[j] - F.lin_mean[j]) / F.lin_scale[j];
+            }
+#pragma unroll
+            for (int j = 0; j < MLP_IO; j++) sm.xs[threadIdx.x * MLP_IO + j] = __float2bfloat16(f[j]);
+        }
+        __syncthreads();
+        mlp_forward_warp(sm.w, sm.xs, m0, sm.h1, sm.h2, nullptr, nullptr, sm.out + m0 * MLP_IO);
+        __syncthreads();
+        if (threadIdx.x < 64) {
+            const uint32_t k = base + threadIdx.x;
+            if (k < n) {
+                const int64_t c  = a.L.item(L_FRESH, k);
+                const float*  o  = sm.out + threadIdx.x * MLP_IO;
+                const float   pu = 1.f / (1.f + __expf(-o[0]));
+                bool          go = pu >= F.learn_conf;
+                double        K[NC];
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    K[i] = exp((double)o[1 + i]);
+                    go   = go && K[i] > 0 && isfinite(K[i]);
+                }
+                if (go) {
+                    // a two-phase start, as for a cell whose stability test
+                    // failed with Yt < 1.1 (the tighter split settings)
+                    const uint32_t meta = (uint32_t)S.I(IF_META, c);
+#pragma unroll
+                    for (int i = 0; i < NC; i++) S.D(F_::Ks + i, c) = K[i];
+                    S.D(F_::Yt, c)    = 1.01;
+                    S.I(IF_META, c)   = (int32_t)((meta & ~M_NP_MASK) | 2u | M_LEARNED);
+                    a.L.push(L_SP_LEARN, (int32_t)c);
+                } else {
+                    a.L.push(L_STA_0, (int32_t)c);
+                }
+            }
+        }
+    }
+}
+
+}  // namespace ocpf

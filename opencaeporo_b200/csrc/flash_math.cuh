@@ -31,40 +31,114 @@ __device__ __forceinline__ double nt_polish(double root, double a, double b, dou
 
 __device__ __forceinline__ double signD(double d) { return d > 0 ? 1.0 : (d < 0 ? -1.0 : 0.0); }
 
-// Z factor of the PR cubic for mixture parameters (aj, bj): Cardano /
-// trigonometric roots with the reference's truncated pi, Newton polish, and
-// for three roots the Gibbs-energy choice between the smallest and largest
-// (SolEoS + CubicRoot, src/MixtureComp.cpp:889-914, 4999-5056).
-__device__ __forceinline__ double sol_eos(double aj, double bj)
-{
-    const double a  = (D1PD2 - 1) * bj - 1;
-    const double b  = (aj + D1TD2 * bj * bj - D1PD2 * bj * (bj + 1));
-    const double c  = -(aj * bj + D1TD2 * bj * bj * (bj + 1));
-    const double Q  = (a * a - 3 * b) / 9;
-    const double R  = (2 * a * a * a - 9 * a * b + 27 * c) / 54;
-    const double Q3 = Q * Q * Q;
-    const double M  = R * R - Q3;
-    if (M <= 0) {
-        const double theta = acos(R / sqrt(Q3));
-        const double s2    = -2 * sqrt(Q);
-        const double a3    = a / 3;
-        double       z0    = nt_polish(s2 * cos(theta / 3) - a3, a, b, c);
-        double       z1    = nt_polish(s2 * cos((theta + 2 * PI_TRUNC) / 3) - a3, a, b, c);
-        double       z2    = nt_polish(s2 * cos((theta - 2 * PI_TRUNC) / 3) - a3, a, b, c);
-        const double zmin  = fmin(z0, fmin(z1, z2));
-        const double zmax  = fmax(z0, fmax(z1, z2));
-        const double dG    = (zmax - zmin) + log((zmin - bj) / (zmax - bj)) -
-                          aj / (bj * (D2 - D1)) *
-                              log((zmin + D1 * bj) * (zmax + D2 * bj) /
-                                  ((zmin + D2 * bj) * (zmax + D1 * bj)));
-        return dG > 0 ? zmin : zmax;
-    } else {
+// The PR cubic Z^3 + a Z^2 + b Z + c = 0 of mixture parameters (aj, bj) with
+// Cardano's Q, R and discriminant M = R^2 - Q^3 (CubicRoot,
+// src/MixtureComp.cpp:4999-5013).
+struct PrCubic {
+    double a, b, c, Q, R, Q3, M;
+    __device__ __forceinline__ PrCubic(double aj, double bj)
+    {
+        a  = (D1PD2 - 1) * bj - 1;
+        b  = (aj + D1TD2 * bj * bj - D1PD2 * bj * (bj + 1));
+        c  = -(aj * bj + D1TD2 * bj * bj * (bj + 1));
+        Q  = (a * a - 3 * b) / 9;
+        R  = (2 * a * a * a - 9 * a * b + 27 * c) / 54;
+        Q3 = Q * Q * Q;
+        M  = R * R - Q3;
+    }
+    // Root k (0, 1, 2) of the trigonometric form (M <= 0), polished; theta =
+    // acos(R / sqrt(Q^3)), with the reference's truncated pi.
+    __device__ __forceinline__ double trig_root(int k, double theta) const
+    {
+        const double s2  = -2 * sqrt(Q);
+        const double a3  = a / 3;
+        const double arg = k == 1 ? (theta + 2 * PI_TRUNC) / 3 : (k == 2 ? (theta - 2 * PI_TRUNC) / 3 : theta / 3);
+        return nt_polish(s2 * cos(arg) - a3, a, b, c);
+    }
+    // The single real root (M > 0), polished.
+    __device__ __forceinline__ double cardano_root() const
+    {
         const double sM = sqrt(M);
         const double t1 = -R + sM;
         const double t2 = R + sM;
         const double S  = signD(t1) * cbrt(fabs(t1));
         const double T  = -signD(t2) * cbrt(fabs(t2));
         return nt_polish(S + T - a / 3, a, b, c);
+    }
+};
+
+// SolEoS's choice among three real roots: the smallest or the largest by the
+// sign of the Gibbs-energy difference (src/MixtureComp.cpp:895-911), in
+// pieces (two logarithms and a coefficient) that a warp can form on
+// different lanes; pick_root_from combines them in one fixed expression.
+__device__ __forceinline__ double gibbs_log1(double zmin, double zmax, double bj)
+{
+    return log((zmin - bj) / (zmax - bj));
+}
+__device__ __forceinline__ double gibbs_log2(double zmin, double zmax, double bj)
+{
+    return log((zmin + D1 * bj) * (zmax + D2 * bj) / ((zmin + D2 * bj) * (zmax + D1 * bj)));
+}
+__device__ __forceinline__ double gibbs_coef(double aj, double bj) { return aj / (bj * (D2 - D1)); }
+__device__ __forceinline__ double pick_root_from(double zmin, double zmax, double g1, double g2, double k)
+{
+    const double dG = (zmax - zmin) + g1 - k * g2;
+    return dG > 0 ? zmin : zmax;
+}
+__device__ __forceinline__ double pick_root(double z0, double z1, double z2, double aj, double bj)
+{
+    const double zmin = fmin(z0, fmin(z1, z2));
+    const double zmax = fmax(z0, fmax(z1, z2));
+    return pick_root_from(zmin, zmax, gibbs_log1(zmin, zmax, bj), gibbs_log2(zmin, zmax, bj), gibbs_coef(aj, bj));
+}
+
+// Z factor of the PR cubic for mixture parameters (aj, bj): Cardano /
+// trigonometric roots with the reference's truncated pi, Newton polish, and
+// for three roots the Gibbs-energy choice between the smallest and largest
+// (SolEoS + CubicRoot, src/MixtureComp.cpp:889-914, 4999-5056).
+__device__ __forceinline__ double sol_eos(double aj, double bj)
+{
+    const PrCubic cu(aj, bj);
+    if (cu.M <= 0) {
+        const double theta = acos(cu.R / sqrt(cu.Q3));
+        const double z0    = cu.trig_root(0, theta);
+        const double z1    = cu.trig_root(1, theta);
+        const double z2    = cu.trig_root(2, theta);
+        return pick_root(z0, z1, z2, aj, bj);
+    } else {
+        return cu.cardano_root();
+    }
+}
+
+// sol_eos for a group of lanes that all hold the same (aj, bj): lanes
+// `base`, `base`+1 and `base`+2 each polish one of the three trigonometric
+// roots and then form one piece of the Gibbs-energy choice; every lane of
+// `mask` (which holds them) picks the same root. Same value as sol_eos, bit
+// for bit.
+__device__ __forceinline__ double sol_eos_group(double aj, double bj, unsigned mask, int base, int rank)
+{
+    const PrCubic cu(aj, bj);
+    if (cu.M <= 0) {
+        const double theta = acos(cu.R / sqrt(cu.Q3));
+        const double zk    = cu.trig_root(rank < 3 ? rank : 0, theta);
+        const double z0    = __shfl_sync(mask, zk, base);
+        const double z1    = __shfl_sync(mask, zk, base + 1);
+        const double z2    = __shfl_sync(mask, zk, base + 2);
+        const double zmin  = fmin(z0, fmin(z1, z2));
+        const double zmax  = fmax(z0, fmax(z1, z2));
+        double       piece;
+        if (rank == 0)
+            piece = gibbs_log1(zmin, zmax, bj);
+        else if (rank == 1)
+            piece = gibbs_log2(zmin, zmax, bj);
+        else
+            piece = gibbs_coef(aj, bj);
+        const double g1 = __shfl_sync(mask, piece, base);
+        const double g2 = __shfl_sync(mask, piece, base + 1);
+        const double k  = __shfl_sync(mask, piece, base + 2);
+        return pick_root_from(zmin, zmax, g1, g2, k);
+    } else {
+        return cu.cardano_root();
     }
 }
 

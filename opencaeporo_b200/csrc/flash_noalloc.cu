@@ -82,6 +82,8 @@ extern "C" int ocpf_flash_fim_noalloc(ocpf_ctx* ctx, int64_t ncell, const ocpf_f
         a.in     = *in;
         a.sk     = sk ? *sk : ocpf_skip{};
         a.out    = *out;
+        a.opts   = 0;
+        a.mlp    = nullptr;
         a.S.cap  = kMaxCells;
         a.S.d    = (double*)base;
         a.S.i    = (int32_t*)(a.S.d + (size_t)nd * kMaxCells);

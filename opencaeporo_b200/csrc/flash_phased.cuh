@@ -43,7 +43,8 @@ struct SF {  // double field ids
         Yt = n1 + NC, SeSSM, rtSSMSTA, rtNRSTA, rtSSMSP, rtNRSP, SeSP, Stol, eNR, eNR0, Asta, Bsta, Zsta,
         phiZ, Y = phiZ + NC, phiS = Y + NC, Ks = phiS + NC, phi0 = Ks + NC, phi1 = phi0 + NC,
         di = phi1 + NC, sA = di + NC, Bi = sA + NC,
-        COUNT = Bi + NC
+        lnY = Bi + NC, lndi = lnY + NC,  // mixed form: FP32 stability trial in log form
+        COUNT = lndi + NC
     };
 };
 // int fields
@@ -61,6 +62,8 @@ constexpr uint32_t M_RESTART   = 1u << 13;  // next split SSM is a restart
 constexpr uint32_t M_STAB_RES  = 1u << 14;  // last stability verdict: stable
 constexpr uint32_t M_NRFLAG    = 1u << 15;  // flag of the last StableNR
 constexpr uint32_t M_SPPHASE   = 1u << 16;  // split loop: after a restart
+constexpr uint32_t M_LEARNED   = 1u << 17;  // split started from the learned initialiser's K
+constexpr uint32_t M_STC       = 1u << 18;  // mixed form: stability trial continued in FP64
 
 template <int NC>
 constexpr int state_doubles() { return SF<NC>::COUNT; }
@@ -75,16 +78,26 @@ struct StateBuf {
 };
 
 // ------------------------------------------------------------------ lists
+// Split rounds 0..3 are PhaseSplit's first try and three restarts; round
+// LEARN_ROUND is the learned initialiser's split of fresh cells (before any
+// stability test), whose failures fall back to the stability test.
 enum ListId : int {
     L_S01_0 = 0, L_S01_1,
     L_STA_0, L_STA_1, L_STA_2, L_STA_3,
     L_NRSTA_0, L_NRSTA_1, L_NRSTA_2, L_NRSTA_3,
-    L_SP_0, L_SP_1, L_SP_2, L_SP_3,
-    L_SPNR_0, L_SPNR_1, L_SPNR_2, L_SPNR_3,
+    L_SP_0, L_SP_1, L_SP_2, L_SP_3, L_SP_LEARN,
+    L_SPNR_0, L_SPNR_1, L_SPNR_2, L_SPNR_3, L_SPNR_LEARN,
     L_SLOW,
+    L_FRESH,  // fresh cells awaiting the learned initialiser
+    // mixed form: stability trials whose Newton polish failed from the FP32
+    // end point, continued by FP64 substitution, and their Newton step
+    L_STC_0, L_STC_1, L_STC_2, L_STC_3,
+    L_NRSTC_0, L_NRSTC_1, L_NRSTC_2, L_NRSTC_3,
     L_COUNT
 };
 constexpr int SPLIT_ROUNDS = 4;  // first try + 3 restarts on the fast path
+constexpr int LEARN_ROUND  = SPLIT_ROUNDS;
+static_assert(L_SP_0 + LEARN_ROUND == L_SP_LEARN && L_SPNR_0 + LEARN_ROUND == L_SPNR_LEARN, "list order");
 
 struct Lists {
     int32_t*  items;  // [L_COUNT][cap]
@@ -105,8 +118,14 @@ struct Lists {
     }
 };
 
+// PhasedArgs::opts bits
+constexpr uint32_t PH_MIXED = 1u;  // FP32 successive substitution (flash_mixed.cuh)
+constexpr uint32_t PH_LEARN = 2u;  // learned initialiser for fresh cells (flash_learned.cuh)
+
 struct PhasedArgs {
     int64_t      count, stride;
+    uint32_t     opts;
+    const float* mlp;  // learned initialiser parameters (PH_LEARN)
     ocpf_fim_in  in;
     ocpf_skip    sk;
     ocpf_fim_out out;

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "flash_phased.cuh"
+#include "flash_warp.cuh"
 
 namespace ocpf {
 
@@ -51,7 +52,7 @@ __device__ void init_body(const FluidConst& F, const PhasedArgs& a)
             } else {
 #pragma unroll
                 for (int i = 0; i < NC; i++) S.D(F_::phiZ + i, c) = phiz[i];
-                a.L.push(f.lNP == 0 ? L_STA_0 : L_S01_0, (int32_t)c);
+                a.L.push(f.lNP == 0 ? ((a.opts & PH_LEARN) ? L_FRESH : L_STA_0) : L_S01_0, (int32_t)c);
             }
         } else {
             f.flagSkip = false;
@@ -89,6 +90,14 @@ __device__ void sta_prep_body(const FluidConst& F, const PhasedArgs& a, int k)
             S.D(F_::di + i, c) = S.D(F_::phiZ + i, c) * f.zi[i];
         }
         S.D(F_::Yt, c) = Yt;
+        if (a.opts & PH_MIXED) {  // the FP32 trial's start in log form
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                S.D(F_::lnY + i, c)  = log(Y[i] * r);
+                S.D(F_::lndi + i, c) = log(S.D(F_::di + i, c));
+            }
+        }
+        S.I(IF_MAXIT, c) = F.ssmsta_maxit;
     }
 }
 
@@ -97,20 +106,20 @@ __device__ void sta_prep_body(const FluidConst& F, const PhasedArgs& a, int k)
 // mixture terms, Yt and the iteration count. Each loop turn is one fugacity
 // evaluation and an O(NC) update for every active lane.
 template <int NC>
-__device__ void sta_ssm_body(const FluidConst& F, const PhasedArgs& a, int k)
+__device__ void sta_ssm_body(const FluidConst& F, const PhasedArgs& a, int list)
 {
     using F_ = SF<NC>;
-    const StateBuf& S    = a.S;
-    const int       list = L_STA_0 + k;
-    const uint32_t  n    = a.L.len(list);
+    const StateBuf& S     = a.S;
+    const uint32_t  n     = a.L.len(list);
     double          Y[NC], di[NC], sA[NC], Bi[NC];
     double          P = 0, Yt = 0;
-    int             iter = 0;
+    int             iter = 0, maxit = 0;
     bool            first = true;
     int64_t         c     = a.L.take(list, n);
     auto load = [&]() {
-        P  = a.in.P[c];
-        Yt = S.D(F_::Yt, c);
+        P     = a.in.P[c];
+        Yt    = S.D(F_::Yt, c);
+        maxit = S.I(IF_MAXIT, c);  // the cap, or what an FP32 start left of it
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             Y[i]  = S.D(F_::Y + i, c);
@@ -135,8 +144,8 @@ __device__ void sta_ssm_body(const FluidConst& F, const PhasedArgs& a, int k)
                 done  = !(Se > F.ssmsta_tol2);
             } else {
                 iter++;
-                done = (iter > F.ssmsta_maxit) || !(Se > F.ssmsta_tol2);
-                if (iter > F.ssmsta_maxit) S.I(IF_STATUS, c) |= ST_SSMSTA_CAP;
+                done = (iter > maxit) || !(Se > F.ssmsta_tol2);
+                if (iter > maxit) S.I(IF_STATUS, c) |= ST_SSMSTA_CAP;
             }
             if (done) {
                 S.D(F_::SeSSM, c) = Se;
@@ -198,26 +207,52 @@ __device__ __forceinline__ void sta_decide(CellFlash<NC>& f, const PhasedArgs& a
 // trial's end point; converged cells get their verdict here, the rest go to
 // the Newton kernel.
 template <int NC>
-__device__ void sta_verdict_body(const FluidConst& F, const PhasedArgs& a, int k)
+__device__ void sta_verdict_body(const FluidConst& F, const PhasedArgs& a, int k, int list, int nrlist, bool from32)
 {
     using F_ = SF<NC>;
     const StateBuf& S = a.S;
-    OCPF_FOR_ITEMS(a, L_STA_0 + k, c)
+    OCPF_FOR_ITEMS(a, list, c)
     {
         CellFlash<NC> f(F);
         uint32_t      meta;
         load_book(f, S, c, meta);
         const double P = a.in.P[c];
-        double       Se = 0;
+        if (from32) {
+            // the FP32 trial's end point in FP64: Y (normalised), Yt, and
+            // the trial phase's phi, a, b, Z
+            double Y[NC], phi[NC], s = 0;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                f.sA[i] = S.D(F_::sA + i, c);
+                f.Bi[i] = S.D(F_::Bi + i, c);
+                Y[i]    = exp(S.D(F_::lnY + i, c));
+                s += Y[i];
+            }
+            f.P = P;
+            double aj, bj, zj;
+#pragma unroll
+            for (int i = 0; i < NC; i++) Y[i] /= s;
+            f.fug_phi(Y, phi, nullptr, aj, bj, zj);
+            S.D(F_::Asta, c) = aj;
+            S.D(F_::Bsta, c) = bj;
+            S.D(F_::Zsta, c) = zj;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                S.D(F_::Y + i, c)    = Y[i];
+                S.D(F_::phiS + i, c) = phi[i];
+            }
+        }
+        double Se = 0;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             const double fz = S.D(F_::di + i, c) * P;
             const double fs = S.D(F_::phiS + i, c) * S.D(F_::Y + i, c) * P;
             Se += sq(log(fz / (fs * f.Yt)));
         }
+        if (from32) S.D(F_::SeSSM, c) = Se;
         Se = sqrt(Se);
         if (Se > F.nrsta_tol) {
-            a.L.push(L_NRSTA_0 + k, (int32_t)c);
+            a.L.push(nrlist, (int32_t)c);
         } else {
             f.nrsta_conflag = true;
             f.nrsta_realTol = Se;
@@ -228,11 +263,11 @@ __device__ void sta_verdict_body(const FluidConst& F, const PhasedArgs& a, int k
 
 // StableNR iterations (src/MixtureComp.cpp:1600-1635), one thread per cell.
 template <int NC>
-__device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k)
+__device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k, int list, int fallback)
 {
     using F_ = SF<NC>;
     const StateBuf& S = a.S;
-    OCPF_FOR_ITEMS(a, L_NRSTA_0 + k, c)
+    OCPF_FOR_ITEMS(a, list, c)
     {
         CellFlash<NC> f(F);
         uint32_t      meta;
@@ -273,9 +308,19 @@ __device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k)
             }
         }
         f.it_nrsta += iter;
+        if (!flag && fallback >= 0) {
+            // mixed form: Newton did not converge from the FP32 end point;
+            // continue the substitution there in FP64 to the reference's
+            // tolerance, then Newton again
+            f.status &= (uint16_t)~ST_NRSTA_FAIL;
+            f.Yt = S.D(F_::Yt, c);
+            store_book(f, S, c, meta | M_STC);
+            a.L.push(fallback, (int32_t)c);
+            continue;
+        }
         f.nrsta_conflag = flag;
         f.nrsta_realTol = Se;
-        sta_decide(f, a, c, meta, k, flag);
+        sta_decide(f, a, c, meta & ~M_STC, k, flag);
     }
 }
 
@@ -461,6 +506,8 @@ __device__ void sp_prep_body(const FluidConst& F, const PhasedArgs& a, int r)
         if (!restart) {
             f.ssmsp_conflag = false;  // PhaseSplit, :1745-1749
             f.nrsp_conflag  = false;
+        }
+        if (!restart && r != LEARN_ROUND) {  // the learned round's K is the prediction
             const uint32_t lastNP = a.in.lastNP[c];
             const int      lNP    = lastNP > 0 ? (int)lastNP - 1 : 0;
             if (lNP == 2) {
@@ -563,6 +610,56 @@ __device__ void sp_ssm_body(const FluidConst& F, const PhasedArgs& a, int r)
     }
 }
 
+// End of the learned initialiser's split (no reference counterpart). The
+// split is kept when SplitNR converged to two phases (CheckSplit's accept
+// branch, src/MixtureComp.cpp:1790-1797) that differ (sum ln^2 K > 1e-4,
+// StableSSM01's trivial-solution bound) and whose Gibbs energy is below the
+// feed's: sum_i z_i (ln f_i - ln f_i(z)) < 0, so the feed is unstable and the
+// stability test would send it to this split. Otherwise the cell returns,
+// as a fresh single-phase cell, to the strict stability test.
+template <int NC>
+__device__ __forceinline__ void learned_after_nr(CellFlash<NC>& f, const PhasedArgs& a, int64_t c, uint32_t meta)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S     = a.S;
+    const double    nuMax = f.nu[0] < f.nu[1] ? f.nu[1] : f.nu[0];
+    double          eX = 0, tk = 0, dg = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        eX += sq(f.x[0][i] - f.x[1][i]);
+        tk += sq(log(f.x[0][i] / f.x[1][i]));
+        dg += f.zi[i] * log(f.fug[0][i] / (S.D(F_::phiZ + i, c) * f.zi[i] * f.P));
+    }
+    const bool keep = f.nrsp_conflag && f.NP == 2 && nuMax < 1 && 1 - nuMax >= 1e-3 && isfinite(eX) &&
+                      tk > 1e-4 && dg < 0;
+    if (keep) {
+        f.check_split();
+        if (!f.ssmsp_conflag) f.status |= ST_SSMSP_FAIL;
+        finish_epec(f);
+        S.D(F_::ePEC, c) = f.ePEC;
+        store_split(f, S, c);
+        store_book(f, S, c, meta);
+        return;
+    }
+    // fall back: the fresh single-phase state init left (x0 = z, the
+    // mixture of z), then the strict stability test
+    f.NP            = 1;
+    f.nu[0]         = 1;
+    f.ssmsp_conflag = false;
+    f.nrsp_conflag  = false;
+    f.status &= (uint16_t) ~(ST_SINGULAR | ST_COLLAPSED | ST_SSMSP_FAIL | ST_NRSP_FAIL);
+    double t[NC];
+    f.mix_ab(f.zi, t, f.Aj[0], f.Bj[0]);
+    f.Zj[0]          = sol_eos(f.Aj[0], f.Bj[0]);
+    S.D(F_::Aj0, c)  = f.Aj[0];
+    S.D(F_::Bj0, c)  = f.Bj[0];
+    S.D(F_::Zj0, c)  = f.Zj[0];
+    S.I(IF_GUARD, c) = 0;
+    store_single_phase(f, S, c, true);
+    store_book(f, S, c, meta & ~(M_LEARNED | M_RESTART | M_SPPHASE));
+    a.L.push(L_STA_0, (int32_t)c);
+}
+
 // End of PhaseSplit once SplitNR is done (src/MixtureComp.cpp:1750-1758,
 // 1784-1836): accept, restart the SSM, or collapse to one phase.
 template <int NC>
@@ -574,6 +671,10 @@ __device__ __forceinline__ void sp_after_nr(CellFlash<NC>& f, const PhasedArgs& 
     f.nrsp_realTol    = eNR;
     if (eNR < f.F.nrsp_tol) f.nrsp_conflag = true;
     f.it_nrsp += iter;
+    if (r == LEARN_ROUND) {
+        learned_after_nr(f, a, c, meta);
+        return;
+    }
     bool restart = false;
     if (!(meta & M_SPPHASE)) {
         if (!f.nrsp_conflag) {
@@ -711,24 +812,29 @@ __device__ void sp_nr_body(const FluidConst& F, const PhasedArgs& a, int r)
     }
 }
 
-// The rest of PhaseSplit's restart loop for cells still restarting after the
-// last split round (rare), on one thread each, with the plain form's code.
+// The rest of PhaseSplit's restart loop (src/MixtureComp.cpp:1750-1758) for
+// the cells still restarting after the last split round (rare), one warp per
+// cell (flash_warp.cuh); lane 0 stores the result.
 template <int NC>
 __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
 {
     using F_ = SF<NC>;
-    const StateBuf& S = a.S;
-    OCPF_FOR_ITEMS(a, L_SLOW, c)
-    {
+    const StateBuf& S    = a.S;
+    const uint32_t  n    = a.L.len(L_SLOW);
+    const uint32_t  nw   = (gridDim.x * blockDim.x) >> 5;
+    const bool      lead = (threadIdx.x & 31) == 0;
+    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n; k += nw) {
+        const int64_t c = a.L.item(L_SLOW, k);
         CellFlash<NC> f(F);
         uint32_t      meta;
         load_split_cell(f, a, c, meta);
         f.T = a.in.T[c] + CONV5;
         f.cal_kwilson();
-        int guard = S.I(IF_GUARD, c);
+        WarpSplit<NC> w(f);
+        int           guard = S.I(IF_GUARD, c);
         while (true) {
-            f.split_ssm2(true);
-            f.split_nr();
+            w.split_ssm2(true);
+            w.split_nr();
             if (!f.check_split()) break;
             if (f.ssmsp_conflag || f.nrsp_conflag) break;
             if (++guard > SPLIT_RESTART_CAP) {
@@ -740,16 +846,18 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
         if (!f.ssmsp_conflag) f.status |= ST_SSMSP_FAIL;
         if (!f.nrsp_conflag) f.status |= ST_NRSP_FAIL;
         finish_epec(f);
-        S.D(F_::ePEC, c) = f.ePEC;
-        if (f.NP == 1) {
-            S.D(F_::Aj0, c) = f.Aj[0];
-            S.D(F_::Bj0, c) = f.Bj[0];
-            S.D(F_::Zj0, c) = f.Zj[0];
-            store_single_phase(f, S, c, true);
-        } else {
-            store_split(f, S, c);
+        if (lead) {
+            S.D(F_::ePEC, c) = f.ePEC;
+            if (f.NP == 1) {
+                S.D(F_::Aj0, c) = f.Aj[0];
+                S.D(F_::Bj0, c) = f.Bj[0];
+                S.D(F_::Zj0, c) = f.Zj[0];
+                store_single_phase(f, S, c, true);
+            } else {
+                store_split(f, S, c);
+            }
+            store_book(f, S, c, meta);
         }
-        store_book(f, S, c, meta);
     }
 }
 

@@ -75,7 +75,7 @@ def saturation_pressure(phase_count, T, Ni, p_lo_mpa=0.5, p_hi_mpa=80.0, steps=4
 
 
 def near_envelope_states(fluid: Fluid, n: int, seed: int, phase_count, t_k=(340.0, 400.0),
-                         alpha: float = 1.0, band=(0.95, 1.05), max_rounds: int = 20):
+                         alpha: float = 1.0, band=(0.95, 1.05), max_rounds: int = 20, steps: int = 40):
     """n states with P within ``band`` of the seeded state's saturation
     pressure. Candidates that have no upper saturation pressure in range are
     redrawn (deterministically, from the same generator stream)."""
@@ -87,7 +87,7 @@ def near_envelope_states(fluid: Fluid, n: int, seed: int, phase_count, t_k=(340.
     while have < n and rounds < max_rounds:
         m = max(2 * (n - have), 64)
         cand = uniform_states(fluid, m, int(rng.integers(1 << 62)), t_k=t_k, alpha=alpha)
-        psat, ok = saturation_pressure(phase_count, cand["T"], cand["Ni"])
+        psat, ok = saturation_pressure(phase_count, cand["T"], cand["Ni"], steps=steps)
         idx = np.nonzero(ok)[0][: n - have]
         outT.append(cand["T"][idx])
         outNi.append(cand["Ni"][idx])
@@ -100,7 +100,7 @@ def near_envelope_states(fluid: Fluid, n: int, seed: int, phase_count, t_k=(340.
             "Ni": np.concatenate(outNi)[:n].reshape(n, nc + 1)}
 
 
-def mixed_states(fluid: Fluid, n: int, seed: int, phase_count, near_frac: float = 0.3):
+def mixed_states(fluid: Fluid, n: int, seed: int, phase_count, near_frac: float = 0.3, steps: int = 40):
     """Uniform states with ``near_frac`` of them replaced by near-envelope
     states at seeded positions."""
     base = uniform_states(fluid, n, seed)
@@ -109,7 +109,7 @@ def mixed_states(fluid: Fluid, n: int, seed: int, phase_count, near_frac: float 
         return base
     rng = np.random.default_rng(seed + 1)
     pos = np.sort(rng.choice(n, size=m, replace=False))
-    near = near_envelope_states(fluid, m, seed + 2, phase_count)
+    near = near_envelope_states(fluid, m, seed + 2, phase_count, steps=steps)
     for k in ("P", "T", "Ni"):
         base[k][pos] = near[k]
     base["near_mask"] = np.zeros(n, bool)

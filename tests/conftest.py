@@ -12,7 +12,7 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 GOLDEN_CASES = ("spe5", "uniform_nc6", "warm_nc6", "uniform_nc3", "uniform_nc9", "uniform_nc12",
-                "near_nc6")
+                "near_nc6", "restart_nc6")
 
 
 def pytest_configure(config):
@@ -47,3 +47,34 @@ def load_golden(name):
 @pytest.fixture(scope="session")
 def golden():
     return load_golden
+
+
+def run_gpu(fl, inp, form="plain", init=None):
+    """One flash of a fixture's inputs through the C ABI on cuda:0 (warm-start
+    state and skip cache from the fixture); ``init``: a learned initialiser
+    to attach (fast form). Returns host outputs."""
+    import torch
+    from opencaeporo_b200.flash import MixtureCompBatch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    m = MixtureCompBatch(fl)
+    if init is not None:
+        init.attach(m)
+    n = len(inp["P"])
+    st = m.new_state(n)
+    st.load(inp["P"], inp["T"], inp["Ni"])
+    o = st.out
+    o["S"].copy_(torch.as_tensor(np.ascontiguousarray(inp["S"].T)))
+    o["phaseNum"].copy_(torch.as_tensor(inp["lastNP"].astype(np.int32)))
+    ncom = fl.nc + 1
+    o["xij"].copy_(torch.as_tensor(np.ascontiguousarray(inp["xij"].reshape(n, 3 * ncom).T)))
+    sk = inp["skip"]
+    st.skip["flag"].copy_(torch.as_tensor(sk["flag"].astype(np.int32)))
+    for k in ("minEig", "P", "T"):
+        st.skip[k].copy_(torch.as_tensor(np.asarray(sk[k], dtype=np.float64)))
+    st.skip["z"].copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(sk["z"]).T)))
+    m.flash_fim(st, form=form)
+    torch.cuda.synchronize()
+    res = st.to_host()
+    m.close()
+    return res

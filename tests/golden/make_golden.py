@@ -11,6 +11,7 @@ edge of an iteration cap or a stability threshold; any implementation whose
 rounding differs from the reference's may legitimately land on either side.
 
     python tests/golden/make_golden.py            # writes tests/golden/*.npz
+    python tests/golden/make_golden.py restart_nc6   # one case only
 """
 from __future__ import annotations
 
@@ -109,9 +110,25 @@ def run_case(name, fl, inp, keep=None, note=""):
     return r
 
 
-def main():
+def restart_case():
+    """Cells whose PhaseSplit keeps restarting: the 48 states of the 1M-state
+    bench workload with the most split successive-substitution iterations
+    (found on a GPU by find_restart_cells.py; each restart runs up to 2x or
+    4x the iteration cap, and the batched form runs cells still restarting
+    after three restarts on its warp-per-cell path), plus 16 ordinary ones."""
+    fl = synthetic_fluid(6, 1234)
+    d = np.load(os.path.join(HERE, "restart_nc6_cells.npz"))
+    inp = {"P": d["P"], "T": d["T"], "Ni": d["Ni"]}
+    run_case("restart_nc6", fl, inp, note="synthetic nc=6: bench-workload states with the most split restarts")
+
+
+def main(only=()):
     if not O.available("reference"):
         raise SystemExit("oracle/_ref/libocpref.so missing: run `make -C oracle ref` first")
+    if only:
+        for name in only:
+            {"restart_nc6": restart_case}[name]()
+        return
 
     # 1) SPE5 fluid (examples/spe5/EGOIL.in) at 160 degF, the deck's initial composition
     fl = spe5_fluid()
@@ -160,6 +177,9 @@ def main():
     inp = synth.near_envelope_states(fl, 256, 2024, pc)
     run_case("near_nc6", fl, inp, note="synthetic nc=6, P = Psat * U(0.95, 1.05)")
 
+    # 6) cells with long split-restart chains
+    restart_case()
+
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

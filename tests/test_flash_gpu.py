@@ -8,7 +8,7 @@ sensitivity in the cells where the reference is ill-conditioned."""
 import numpy as np
 import pytest
 
-from conftest import GOLDEN_CASES, load_golden
+from conftest import GOLDEN_CASES, load_golden, run_gpu
 from oracle import compare as CMP
 from oracle import oracle as O
 
@@ -23,27 +23,7 @@ def _torch():
 
 
 def _run_gpu(fl, inp, form="plain"):
-    from opencaeporo_b200.flash import MixtureCompBatch
-    torch = _torch()
-    m = MixtureCompBatch(fl)
-    n = len(inp["P"])
-    st = m.new_state(n)
-    st.load(inp["P"], inp["T"], inp["Ni"])
-    o = st.out
-    o["S"].copy_(torch.as_tensor(np.ascontiguousarray(inp["S"].T)))
-    o["phaseNum"].copy_(torch.as_tensor(inp["lastNP"].astype(np.int32)))
-    ncom = fl.nc + 1
-    o["xij"].copy_(torch.as_tensor(np.ascontiguousarray(inp["xij"].reshape(n, 3 * ncom).T)))
-    sk = inp["skip"]
-    st.skip["flag"].copy_(torch.as_tensor(sk["flag"].astype(np.int32)))
-    for k in ("minEig", "P", "T"):
-        st.skip[k].copy_(torch.as_tensor(np.asarray(sk[k], dtype=np.float64)))
-    st.skip["z"].copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(sk["z"]).T)))
-    m.flash_fim(st, form=form)
-    torch.cuda.synchronize()
-    res = st.to_host()
-    m.close()
-    return res
+    return run_gpu(fl, inp, form)
 
 
 @pytest.mark.parametrize("form", ["plain", "batched"])
@@ -66,7 +46,25 @@ def test_matches_reference_goldens(case, form):
     assert abs(wa - wb) <= 0.05 * wb, (got["iters"].sum(axis=0), ref["iters"].sum(axis=0))
 
 
-@pytest.mark.parametrize("form", ["plain", "batched"])
+@pytest.mark.parametrize("case", GOLDEN_CASES)
+def test_mixed_matches_reference_goldens(case):
+    """Mixed form (FP32 successive substitution; FP64 cubic roots near the
+    discriminant, Rachford-Rice and Newton polish) against the reference:
+    the same bar as the FP64 forms -- identical phase counts except on
+    knife-edge cells, every output within 1e-8 relative or 10x the
+    reference's own 1-ulp sensitivity where that is larger."""
+    fl, inp, ref, fragile = load_golden(case)
+    got = _run_gpu(fl, inp, form="mixed")
+    chk = CMP.check(got, ref, fl.nc, noise=ref["noise"], fragile=fragile)
+    assert chk["ok"], f"{case}: {CMP.check_summary(chk)}"
+    res = CMP.compare(got, ref, fl.nc)
+    for k in ("phaseExist", "bRowSizedSdP", "pSderExist", "pVnumCom"):
+        assert res[k + "_mismatch"] == 0, f"{case}: {k}"
+    same = got["phaseNum"] == ref["phaseNum"]
+    assert np.array_equal(got["ftype"][same], ref["ftype"][same])
+
+
+@pytest.mark.parametrize("form", ["plain", "batched", "mixed"])
 def test_skip_cache_matches_reference(form):
     fl, inp, ref, fragile = load_golden("warm_nc6")
     got = _run_gpu(fl, inp, form=form)
@@ -130,7 +128,7 @@ def _port_noise(fl, inp, base, runs=4):
     return noise, frag
 
 
-@pytest.mark.parametrize("form", ["plain", "batched"])
+@pytest.mark.parametrize("form", ["plain", "batched", "mixed"])
 @pytest.mark.parametrize("nc,seed", [(6, 1234), (12, 7)])
 def test_matches_port_4096(nc, seed, form):
     """4096 seeded states (the 6-component workload distribution; and a

@@ -1,0 +1,189 @@
+"""The learned initialiser: its network kernels against the NumPy oracle
+(oracle/mlp.py), the oracle against finite differences, training, and the
+fast form that uses a trained network (parity with the reference and what
+the network saves)."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp as M
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+MODEL = os.path.join(ROOT, "opencaeporo_b200", "models", "learned_init_nc6.npz")
+
+
+def _problem(n=300, nin=8, nout=7, seed=3):
+    rng = np.random.default_rng(seed)
+    from opencaeporo_b200.learn import init_params
+    p = init_params(nin, nout, seed).astype(np.float64)
+    p[M.OFF_B1:M.OFF_W2] = rng.normal(0, 0.1, M.H)
+    p[M.OFF_B2:M.OFF_W3] = rng.normal(0, 0.1, M.H)
+    p[M.OFF_B3:M.OFF_B3 + nout] = rng.normal(0, 0.1, nout)
+    x = rng.normal(0, 1, (nin, n))
+    t = np.vstack([rng.integers(0, 2, n), rng.normal(0, 2, (nout - 1, n))])
+    w = (rng.uniform(size=n) < 0.6).astype(np.float64)
+    return p.astype(np.float32), x.astype(np.float32), t.astype(np.float32), w.astype(np.float32)
+
+
+def test_oracle_gradient_matches_finite_differences():
+    """The oracle's hand-derived backward pass (float64) is the derivative
+    of its loss."""
+    p, x, t, w = _problem(n=40)
+    p = p.astype(np.float64)
+    lam = 0.7
+    _, g = M.loss_and_grad(p, x, t, w, lam, bf16=False)
+    rng = np.random.default_rng(0)
+    nin, nout = x.shape[0], t.shape[0]
+    live = [i for i in range(M.NPARAM)
+            if not (M.OFF_W1 <= i < M.OFF_B1 and (i - M.OFF_W1) % M.IO >= nin)
+            and not (M.OFF_W3 <= i < M.OFF_B3 and (i - M.OFF_W3) // M.H >= nout)
+            and not (M.OFF_B3 + nout <= i < M.NPARAM)]
+    n = x.shape[1]
+
+    def L(q):
+        s, _ = M.loss_and_grad(q, x, t, w, lam, bf16=False)
+        return (s[0] + lam * s[1]) / n
+
+    for i in rng.choice(live, 60, replace=False):
+        h = 1e-6
+        q1, q2 = p.copy(), p.copy()
+        q1[i] += h
+        q2[i] -= h
+        fd = (L(q1) - L(q2)) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+
+
+def test_bf16_rounding():
+    a = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 0.0], np.float32)
+    r = M.bf16_round(a)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[2] == 1.0078125
+    assert abs(r[3] - (-3.140625)) < 1e-9 and r[4] == 0.0
+
+
+@pytest.mark.gpu
+def test_mlp_forward_matches_oracle():
+    import torch
+    from opencaeporo_b200 import learn
+    p, x, t, w = _problem(n=1000)
+    dev = torch.device("cuda", 0)
+    y = learn.forward(torch.as_tensor(p, device=dev), torch.as_tensor(x, device=dev), 7).cpu().numpy()
+    ref, _ = M.forward(p, x, bf16=True)
+    err = np.abs(y - ref[:7])
+    assert np.max(err) < 2e-2 * (1 + np.max(np.abs(ref[:7]))), np.max(err)
+    assert np.mean(err) < 2e-3, np.mean(err)
+
+
+@pytest.mark.gpu
+def test_mlp_gradient_matches_oracle():
+    """Gradient of the BF16 tensor-core kernel against the CPU oracle with
+    the same BF16 roundings; and against the exact float64 gradient to
+    BF16 accuracy."""
+    import torch
+    from opencaeporo_b200 import learn
+    p, x, t, w = _problem(n=777)
+    dev = torch.device("cuda", 0)
+    g = torch.zeros(M.NPARAM, dtype=torch.float32, device=dev)
+    loss = torch.zeros(2, dtype=torch.float32, device=dev)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    learn.grad(T(p), T(x), T(t), T(w), 0.5, g, loss)
+    gk = g.cpu().numpy().astype(np.float64)
+    lk = loss.cpu().numpy().astype(np.float64)
+    lo, go = M.loss_and_grad(p, x, t, w, 0.5, bf16=True)
+    np.testing.assert_allclose(lk, lo, rtol=2e-3)
+    rel = np.linalg.norm(gk - go) / np.linalg.norm(go)
+    assert rel < 1e-2, rel
+    cos = gk @ go / (np.linalg.norm(gk) * np.linalg.norm(go))
+    assert cos > 0.9999, cos
+    _, gx = M.loss_and_grad(p, x, t, w, 0.5, bf16=False)
+    assert np.linalg.norm(gk - gx) / np.linalg.norm(gx) < 5e-2
+
+
+@pytest.mark.gpu
+def test_training_fits_a_known_function():
+    """The training kernels (grad + Adam) fit a smooth target: the logit
+    classifies a half-space and the regression rows learn linear maps."""
+    from opencaeporo_b200 import learn
+    rng = np.random.default_rng(11)
+    n, nin, nout = 65536, 8, 7
+    x = rng.normal(0, 1, (nin, n)).astype(np.float32)
+    t = np.zeros((nout, n), np.float32)
+    t[0] = (x[0] + 0.5 * x[1] > 0)
+    A = rng.normal(0, 0.5, (nout - 1, nin))
+    t[1:] = A @ x
+    w = np.ones(n, np.float32)
+    logs = []
+    params = learn.train(x, t, w, epochs=6, batch=4096, lr=3e-3, log=logs.append)
+    import torch
+    y = learn.forward(torch.as_tensor(params, device="cuda"), torch.as_tensor(x, device="cuda"), nout).cpu().numpy()
+    acc = np.mean((y[0] > 0) == (t[0] > 0.5))
+    mse = np.mean((y[1:] - t[1:]) ** 2)
+    assert acc > 0.97, (acc, logs)
+    assert mse < 0.02 * np.mean(t[1:] ** 2), (mse, logs)
+
+
+def _model():
+    from opencaeporo_b200.learn import Initializer
+    if not os.path.exists(MODEL):
+        pytest.fail(f"trained initialiser missing: {MODEL} (python -m opencaeporo_b200.learn)")
+    return Initializer.load(MODEL)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["uniform_nc6", "near_nc6"])
+def test_fast_matches_reference_goldens(case):
+    """Fast form (mixed + trained initialiser) against the reference: the
+    same bar as every other form (identical phase counts except knife-edge
+    cells; outputs within 1e-8 relative or 10x the reference's own 1-ulp
+    sensitivity)."""
+    from conftest import load_golden, run_gpu
+    from oracle import compare as CMP
+    fl, inp, ref, fragile = load_golden(case)
+    got = run_gpu(fl, inp, form="fast", init=_model())
+    chk = CMP.check(got, ref, fl.nc, noise=ref["noise"], fragile=fragile)
+    assert chk["ok"], f"{case}: {CMP.check_summary(chk)}"
+
+
+@pytest.mark.gpu
+def test_initialiser_gain_over_mixed():
+    """What the trained network buys on 65,536 held-out states of the
+    workload distribution (a seed it was not trained on): the fast form ends
+    with the same phase counts as the mixed form (up to a handful of
+    knife-edge cells) while doing less work -- fewer stability iterations
+    and less modelled FP64 work -- and taking less time."""
+    import torch
+    from opencaeporo_b200 import roofline
+    from opencaeporo_b200.flash import MixtureCompBatch
+    from opencaeporo_b200.workload import bench_fluid, make_workload
+    fl = bench_fluid()
+    n = 1 << 16
+    w = make_workload(fl, n, 424242, 0)
+    res, ms = {}, {}
+    for form in ("mixed", "fast"):
+        m = MixtureCompBatch(fl)
+        if form == "fast":
+            _model().attach(m)
+        st = m.new_state(n)
+        best = 1e9
+        for _ in range(3):
+            st.load(w["P"], w["T"], w["Ni"])
+            st.skip["flag"].zero_()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            m.flash_fim(st, form=form, fresh=True)
+            b.record()
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b))
+        res[form], ms[form] = st.to_host(), best
+        m.close()
+    mix, fast = res["mixed"], res["fast"]
+    mism = np.count_nonzero(mix["phaseNum"] != fast["phaseNum"])
+    assert mism <= max(3, n // 10000), mism
+    it_m, it_f = mix["iters"].sum(axis=0), fast["iters"].sum(axis=0)
+    work_m = roofline.flops(fl.nc, mix["iters"], mix["phaseNum"] - 1)
+    work_f = roofline.flops(fl.nc, fast["iters"], fast["phaseNum"] - 1)
+    print(f"mixed {ms['mixed']:.2f} ms iters {it_m.tolist()}  fast {ms['fast']:.2f} ms iters {it_f.tolist()}  "
+          f"model work {work_f / work_m:.3f}x")
+    assert it_f[0] < 0.9 * it_m[0], (it_m, it_f)
+    assert work_f < 0.95 * work_m, (work_m, work_f)
