@@ -18,7 +18,15 @@ FMA throughput (its binding pipe), with the HBM view beside it;
 ``cpu_baseline`` is the reference's own MixtureComp (compiled from its
 sources) on a bounded sample on this host's cores.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--form plain|fast]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--form fast|mixed|batched|plain]
+
+The default form is ``fast``: FP32 successive substitution with FP64 cubic
+roots near the discriminant, Rachford-Rice and Newton polish, batched phase
+kernels, and the learned initialiser (opencaeporo_b200/models). The line
+also carries the plain FP64 GPU form timed on the same states
+(``plain_fp64_gpu``) and, on the CPU sample, every output's error against
+the FP64 reference.
 """
 from __future__ import annotations
 
@@ -46,10 +54,11 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="plain", choices=["plain", "batched", "mixed", "fast"])
+    ap.add_argument("--form", default="fast", choices=["plain", "batched", "mixed", "fast"])
     ap.add_argument("--ncell", type=int, default=NCELL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain FP64 form beside the form")
     ap.add_argument("--workload-cache", default=None,
                     help="npz file: load the workload from it if present, else generate and save it")
     return ap.parse_args()
@@ -190,6 +199,16 @@ def our_arm(args):
     nc = fl.nc
 
     m = MixtureCompBatch(fl, dev)
+    init_note = None
+    if args.form == "fast":
+        from opencaeporo_b200.learn import DEFAULT_MODEL, Initializer
+        if os.path.exists(DEFAULT_MODEL):
+            init = Initializer.load(DEFAULT_MODEL)
+            init.attach(m)
+            init_note = {"model": os.path.relpath(DEFAULT_MODEL, ROOT), "confidence": init.confidence,
+                         "train_states": int(init.meta.get("train_states", 0))}
+        else:
+            init_note = "no trained initialiser found: the fast form ran as the mixed form"
     st = m.new_state(n)
     st.load(w["P"], w["T"], w["Ni"])
     stream = torch.cuda.current_stream(dev)
@@ -223,6 +242,25 @@ def our_arm(args):
         dist.barrier()
     ms_total = t0.elapsed_time(t1)
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    res = st.to_host()
+
+    # the plain FP64 GPU form on the same states, for the headline ratio
+    plain = None
+    if args.form != "plain" and not args.no_plain:
+        pe = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+        times = []
+        for s_ in range(3):
+            flush.zero_()
+            st.skip["flag"].zero_()
+            pe[0].record(stream)
+            m.flash_fim(st, form="plain", fresh=True)
+            pe[1].record(stream)
+            torch.cuda.synchronize()
+            if s_ > 0:
+                times.append(pe[0].elapsed_time(pe[1]))
+        pms = float(np.mean(times))
+        plain = {"value": n / (pms * 1e-3), "unit": "states/s", "ms_per_step": pms,
+                 "form_speedup": pms / kern_ms}
     if world > 1:
         t = torch.tensor([ms_total, kern_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -231,7 +269,6 @@ def our_arm(args):
     value = world * n / (ms_step * 1e-3)
 
     # roofline of the flash kernel (work model from the device's iteration counters)
-    res = st.to_host()
     nphc = res["phaseNum"] - 1
     fl_launch = roofline.flops(nc, res["iters"], nphc)
     by_launch = roofline.batch_bytes(nc, nphc, fl.controls.use_skip)
@@ -270,6 +307,8 @@ def our_arm(args):
         "roofline_hbm": {"bound": "hbm", "achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": ach_gbs / hbm_peak, "bytes_per_launch": by_launch,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "plain_fp64_gpu": plain,
+        "initializer": init_note,
         "iters_per_cell": {k: float(v) for k, v in zip(("ssmsta", "nrsta", "ssmsp", "nrsp", "rr"),
                                                          res["iters"].mean(axis=0))},
         "status_cells": int(np.count_nonzero(res["status"] & 0xC0)),
@@ -337,6 +376,7 @@ def cpu_baseline(fl, w, gpu_res):
         worst = np.fmax(worst, np.nan_to_num(e[k], nan=0.0))
     det = same & ((r["NPhc"] == 1) | (r["ePEC"] <= 1e-9))
     ill = same & ~det
+    per_output = {k: float(np.max(np.nan_to_num(e[k][det], nan=0.0), initial=0.0)) for k in CMP.FLOAT_KEYS}
     return {"value": ns / r["seconds"], "unit": "states/s", "cores": cores, "kind": kind,
             "sample": f"first {ns} states of the 1M-cell workload, one flash each, {cores} threads",
             "parity_on_sample": {
@@ -345,6 +385,7 @@ def cpu_baseline(fl, w, gpu_res):
                 "max_rel_err_well_determined": float(np.max(worst[det], initial=0.0)),
                 "share_well_determined_le_1e-8": float(np.mean(worst[det] <= 1e-8)) if det.any() else None,
                 "ill_determined_cells": int(ill.sum()),
+                "max_rel_err_per_output_well_determined": per_output,
                 "metric": "max over outputs of |gpu-ref|/max(|ref|, 1e-12 field scale); dSec_dPri "
                           "entries against max(|ref|, 1e-4 column scale)"}}
 

@@ -209,6 +209,19 @@ int ocpf_reserve(ocpf_ctx* ctx, int64_t ncell);
 int ocpf_flash_fim_noalloc(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
                            ocpf_fim_out* out, void* stream);
 
+/* Several PVT regions at once -- the batched counterpart of a Bulk whose
+ * cells belong to different regions (flashCal[PVTNUM[n]] in
+ * src/OCPFluidMethod.cpp:1108-1120), with the cells grouped by region.
+ * Region r flashes ncell[r] cells of in[r] / skip[r] / out[r] through
+ * ctx[r] (distinct contexts; fluids of different component counts may be
+ * mixed). Each region runs on its context's own stream, forked from and
+ * joined back into `stream`, so regions of uneven cost overlap on the GPU;
+ * the call is asynchronous on `stream` like ocpf_flash_fim. skip may be null
+ * when no region uses the skip cache. Results equal one ocpf_flash_fim per
+ * region. */
+int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
+                           ocpf_skip* skip, ocpf_fim_out* out, int form, void* stream);
+
 /* Same call with every array in HOST memory (pinned memory is faster). The
  * cells are streamed through device staging buffers owned by the context in
  * chunks, copies overlapping the flash on two streams; returns after the
@@ -267,6 +280,13 @@ int ocpf_mlp_adam(float* params, float* grad, float* m, float* v, int step, floa
  * OCPF_FORM_MIXED. */
 int ocpf_set_initializer(ocpf_ctx* ctx, const float* params, const float* in_mean, const float* in_scale,
                          float confidence);
+
+/* Measures, on one thread with clock64, the latency in cycles of FP64
+ * operations that bound a single cell's chain of dependent iterations:
+ * cycles[0] division, [1] division when twelve independent ones are issued
+ * together (per division), [2] FMA, [3] exp, [4] log, [5] acos + cos. No
+ * reference counterpart (measurement utility). */
+int ocpf_measure_fp64_latency(int device, double* cycles);
 
 #ifdef __cplusplus
 }

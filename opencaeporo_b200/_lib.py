@@ -34,7 +34,7 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_flash_fim", "ocpf_flash_fim_host", "ocpf_last_kernel_ms",
            "ocpf_measure_fma_peak", "ocpf_reserve", "ocpf_flash_fim_noalloc",
            "ocpf_mlp_param_count", "ocpf_mlp_forward", "ocpf_mlp_grad", "ocpf_mlp_adam",
-           "ocpf_set_initializer")
+           "ocpf_set_initializer", "ocpf_flash_fim_regions", "ocpf_measure_fp64_latency")
 
 _vp = C.c_void_p
 
@@ -144,6 +144,11 @@ def lib():
     L.ocpf_set_initializer.argtypes = [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
                                        C.c_float]
     L.ocpf_set_initializer.restype = C.c_int
+    L.ocpf_flash_fim_regions.argtypes = [C.c_int, C.POINTER(_vp), C.POINTER(C.c_int64), C.POINTER(FimIn),
+                                         C.POINTER(Skip), C.POINTER(FimOut), C.c_int, _vp]
+    L.ocpf_flash_fim_regions.restype = C.c_int
+    L.ocpf_measure_fp64_latency.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.ocpf_measure_fp64_latency.restype = C.c_int
     _LIB = L
     return L
 
@@ -178,6 +183,14 @@ def check(rc: int, what: str):
     if rc != OCPF_OK:
         msg = lib().ocpf_status_string(rc).decode()
         raise RuntimeError(f"{what} failed: {msg} ({rc})")
+
+
+def fp64_latency_cycles(device: int = 0) -> dict:
+    """One-thread latencies (cycles) of FP64 division, division issued twelve
+    at a time (per division), FMA, exp, log and acos + cos."""
+    v = (C.c_double * 6)()
+    check(lib().ocpf_measure_fp64_latency(int(device), v), "ocpf_measure_fp64_latency")
+    return dict(zip(("div", "div_x12_each", "fma", "exp", "log", "acos_cos"), list(v)))
 
 
 def fma_peak_tflops(device: int = 0, bits: int = 64) -> float:

@@ -135,6 +135,9 @@ struct ocpf_ctx {
     void*       eq;
     // learned initialiser parameters (device, MLP_NPARAM floats) or null
     float*      mlp;
+    // ocpf_flash_fim_regions: this region's stream and its fork/join events
+    cudaStream_t rs;
+    cudaEvent_t  evf, evj;
 };
 
 static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
@@ -180,6 +183,8 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->eq_cap    = 0;
     c->eq        = nullptr;
     c->mlp       = nullptr;
+    c->rs        = nullptr;
+    c->evf = c->evj = nullptr;
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         cudaSetDevice(prev);
@@ -201,6 +206,9 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     if (c->stage) cudaFree(c->stage);
     if (c->eq) cudaFree(c->eq);
     if (c->mlp) cudaFree(c->mlp);
+    if (c->rs) cudaStreamDestroy(c->rs);
+    if (c->evf) cudaEventDestroy(c->evf);
+    if (c->evj) cudaEventDestroy(c->evj);
     for (auto& s : c->hs)
         if (s) cudaStreamDestroy(s);
     cudaSetDevice(prev);
@@ -321,6 +329,53 @@ extern "C" int ocpf_flash_fim(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in* in,
     const int rc = launch_form(c, form, ncell, ncell, *in, s, *out, (cudaStream_t)stream, true);
     c->timed     = (rc == OCPF_OK && ncell > 0);
     if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+extern "C" int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
+                                      ocpf_skip* sk, ocpf_fim_out* out, int form, void* stream)
+{
+    if (nreg < 0) return OCPF_EINVAL;
+    if (nreg == 0) return OCPF_OK;
+    if (!ctx || !ncell || !in || !out) return OCPF_EINVAL;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    for (int r = 0; r < nreg; r++) {
+        if (!ctx[r] || ncell[r] < 0 || ctx[r]->device != ctx[0]->device) return OCPF_EINVAL;
+        for (int q = 0; q < r; q++)
+            if (ctx[q] == ctx[r]) return OCPF_EINVAL;  // one context owns one scratch and stream
+        if (ncell[r] > 0 && !fim_args_ok(ctx[r], &in[r], sk ? &sk[r] : nullptr, &out[r])) return OCPF_EINVAL;
+    }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    const int dev = ctx[0]->device;
+    if (prev != dev) cudaSetDevice(dev);
+    int rc = OCPF_OK;
+    for (int r = 0; r < nreg && rc == OCPF_OK; r++) {
+        ocpf_ctx* c = ctx[r];
+        if (!c->rs && cudaStreamCreateWithFlags(&c->rs, cudaStreamNonBlocking) != cudaSuccess) rc = OCPF_ECUDA;
+        if (rc == OCPF_OK && !c->evf && cudaEventCreateWithFlags(&c->evf, cudaEventDisableTiming) != cudaSuccess)
+            rc = OCPF_ECUDA;
+        if (rc == OCPF_OK && !c->evj && cudaEventCreateWithFlags(&c->evj, cudaEventDisableTiming) != cudaSuccess)
+            rc = OCPF_ECUDA;
+    }
+    // fork: every region's stream starts after the work already on `stream`
+    if (rc == OCPF_OK && cudaEventRecord(ctx[0]->evf, (cudaStream_t)stream) != cudaSuccess) rc = OCPF_ECUDA;
+    for (int r = 0; r < nreg && rc == OCPF_OK; r++) {
+        ocpf_ctx* c = ctx[r];
+        if (cudaStreamWaitEvent(c->rs, ctx[0]->evf, 0) != cudaSuccess) {
+            rc = OCPF_ECUDA;
+            break;
+        }
+        ocpf_skip s{};
+        if (sk) s = sk[r];
+        if (ncell[r] > 0) rc = launch_form(c, form, ncell[r], ncell[r], in[r], s, out[r], c->rs, false);
+        c->timed = false;
+        // join: `stream` continues after every region
+        if (rc == OCPF_OK && (cudaEventRecord(c->evj, c->rs) != cudaSuccess ||
+                              cudaStreamWaitEvent((cudaStream_t)stream, c->evj, 0) != cudaSuccess))
+            rc = OCPF_ECUDA;
+    }
+    if (prev != dev) cudaSetDevice(prev);
     return rc;
 }
 

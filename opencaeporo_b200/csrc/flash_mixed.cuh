@@ -1,18 +1,21 @@
 // flash_mixed.cuh -- the mixed-precision form's successive substitution:
-// the iterations of the strict stability test (StableSSM) and of the split's
-// first try (SplitSSM2) with the fugacities in FP32, while FP64 keeps
+// the iterations of the strict stability test (StableSSM) with the
+// fugacities in FP32, while FP64 keeps
 //   * the cubic's coefficients, its root count (the discriminant's sign) and
 //     a Newton polish of every root, and the root choice where the Gibbs
 //     difference is small (the full FP64 SolEoS where the discriminant
 //     itself is small),
-//   * the bracketed Rachford-Rice Newton,
+//   * the phase split: SplitSSM2 with its bracketed Rachford-Rice Newton,
+//     and SplitNR. In FP32 the split's successive substitution changes the
+//     outcome of the cells whose SplitNR the reference itself cannot settle
+//     (it stops on a small step with a residual far above its tolerance;
+//     such cells' results follow the exact arithmetic path), so it stays
+//     FP64 and bit-identical to the batched form,
 //   * the end of every successive substitution: FP32 iterations stop at a
 //     residual FP32 can resolve (SSM32_TOL2 below). A stability trial's end
 //     point is then evaluated in FP64 and polished by StableNR; where that
 //     Newton step fails (it has no globalisation), the trial continues by
 //     FP64 substitution to the reference's tolerance and Newton runs again.
-//     A split continues by FP64 substitution to the reference's tolerance
-//     before SplitNR (whose convergence depends on a tight start).
 // Converged answers therefore agree with the FP64 form's to the reference's
 // tolerances. Iteration counts differ from the reference's (they count FP32
 // and FP64 iterations alike).
@@ -22,9 +25,8 @@
 
 namespace ocpf {
 
-// FP32 end tests: sum of squared log residuals (stability) or of squared
-// relative fugacity differences (split). FP32 fugacities carry ~1e-6
-// relative error, so these sit two decades above that floor.
+// FP32 end test: the sum of squared log residuals. FP32 fugacities carry
+// ~1e-6 relative error, so it sits two decades above that floor.
 constexpr float SSM32_TOL2 = 1e-10f;
 
 // FP32 mixing rule: t_i = sqrt(A_i) sum_k (1 - k_ik) sqrt(A_k) x_k,
@@ -190,128 +192,6 @@ __device__ void sta_ssm32_body(const FluidConst& F, const PhasedArgs& a, int k)
 #pragma unroll
                 for (int i = 0; i < NC; i++) lnY[i] -= lnYt;
             }
-        }
-    }
-}
-
-// ------------------------------------------------------- split (FP32)
-// Rachford-Rice (RachfordRice2, src/MixtureComp.cpp:1907-1959) in FP64:
-// Newton on the bracket (1/(1-Kmax), 1/(1-Kmin)), halving towards the
-// bracket's end when a step leaves it; started from v0 when v0 lies inside
-// (the root of the previous substitution step), else from the midpoint.
-// One reciprocal per component per step. Returns nu_0.
-template <int NC>
-__device__ __forceinline__ double rr_mixed(const double* z, const double* K, double v0, double tol, int maxit,
-                                           int& iters)
-{
-    double Kmin = K[0], Kmax = K[0];
-#pragma unroll
-    for (int i = 1; i < NC; i++) {
-        Kmin = fmin(Kmin, K[i]);
-        Kmax = fmax(Kmax, K[i]);
-    }
-    const double numin = 1 / (1 - Kmax);
-    const double numax = 1 / (1 - Kmin);
-    double       v     = (v0 > numin && v0 < numax) ? v0 : 0.5 * (numin + numax);
-    int          it    = 0;
-    while (true) {
-        double rj = 0, J = 0;
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            const double km1 = K[i] - 1;
-            const double inv = 1 / (1 + v * km1);
-            const double q   = z[i] * km1 * inv;
-            rj += q;
-            J -= q * km1 * inv;
-        }
-        if (fabs(rj) < tol || it > maxit) break;
-        const double d  = -rj / J;
-        const double vn = v + d;
-        if (vn < numax && vn > numin)
-            v = vn;
-        else if (d > 0)
-            v = (v + numax) / 2;
-        else
-            v = (v + numin) / 2;
-        it++;
-    }
-    iters += it;
-    return v;
-}
-
-// SplitSSM2's first try (src/MixtureComp.cpp:1881-1902) with FP32
-// fugacities on a persistent grid: per turn, FP64 Rachford-Rice, the phase
-// compositions, FP32 ln phi of both phases and the K update, until
-// max(SSM32_TOL2, Stol) or the iteration cap. The FP64 kernel (sp_ssm)
-// then continues from the K reached, with what is left of the cap, to the
-// reference's tolerance before SplitNR. With x_0 = K x_1, f_1 / f_0 =
-// K_new / K, so the end test needs no compositions.
-template <int NC>
-__device__ void sp_ssm32_body(const FluidConst& F, const PhasedArgs& a, int r)
-{
-    using F_ = SF<NC>;
-    const StateBuf& S    = a.S;
-    const int       list = L_SP_0 + r;
-    const uint32_t  n    = a.L.len(list);
-    double          z[NC], K[NC], v = 0.5;
-    float           sA[NC], Bi[NC];
-    double          Stol = 0;
-    int             maxIt = 0, iter = 0, itrr = 0;
-    int64_t         c     = a.L.take(list, n);
-    auto load = [&]() {
-        double Ni[NC], Nh = 0;
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
-            Nh += fabs(Ni[i]);
-        }
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            z[i]  = Ni[i] / Nh;
-            K[i]  = S.D(F_::Ks + i, c);
-            sA[i] = (float)S.D(F_::sA + i, c);
-            Bi[i] = (float)S.D(F_::Bi + i, c);
-        }
-        Stol  = fmax(S.D(F_::Stol, c), (double)SSM32_TOL2);
-        maxIt = S.I(IF_MAXIT, c);
-        iter  = 0;
-        itrr  = 0;
-        v     = -1e300;
-    };
-    auto finish = [&]() {
-        S.I(IF_IT2, c) += iter;
-        S.I(IF_IT4, c) += itrr;
-        S.I(IF_MAXIT, c) = maxIt > iter ? maxIt - iter : 0;
-#pragma unroll
-        for (int i = 0; i < NC; i++) S.D(F_::Ks + i, c) = K[i];
-        c = a.L.take(list, n);
-        if (c >= 0) load();
-    };
-    if (c >= 0) load();
-    while (__any_sync(0xffffffffu, c >= 0)) {
-        if (c >= 0) {
-            v = rr_mixed<NC>(z, K, v, F.rr_tol, F.rr_maxit, itrr);
-            float  x0[NC], x1[NC];
-            double Kr[NC];
-#pragma unroll
-            for (int i = 0; i < NC; i++) {
-                Kr[i]            = K[i];
-                const double xi1 = z[i] / (1 + v * (K[i] - 1));
-                x1[i]            = (float)xi1;
-                x0[i]            = (float)(K[i] * xi1);
-            }
-            float l0[NC], l1[NC];
-            ln_phi32<NC>(F, sA, Bi, x0, l0);
-            ln_phi32<NC>(F, sA, Bi, x1, l1);
-            double Se = 0;
-#pragma unroll
-            for (int i = 0; i < NC; i++) {
-                K[i]           = (double)__expf(l1[i] - l0[i]);
-                const double q = K[i] / Kr[i] - 1;
-                Se += q * q;
-            }
-            iter++;
-            if (iter > maxIt || !(Se > Stol)) finish();
         }
     }
 }

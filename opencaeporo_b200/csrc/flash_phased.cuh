@@ -12,10 +12,10 @@
 //                 prep -> persistent SSM -> end-of-trial logic
 //   strict round k (StableSSM trial k + StableNR), k = 0..3:
 //                 prep -> persistent SSM -> verdict -> Newton
-//   split round r (SplitSSM2 + SplitNR; r = 0 first try, r >= 1 restarts):
-//                 prep -> persistent SSM -> Newton start -> Newton
-//   slow path     cells still restarting after the last split round: the
-//                 rest of PhaseSplit on one thread each
+//   split         (SplitSSM2 + SplitNR, first try):
+//                 prep -> persistent SSM -> Newton start -> persistent Newton
+//   restarts      cells whose split restarts: the rest of PhaseSplit, one
+//                 warp per cell (flash_warp.cuh)
 //   finalize      every cell: properties, derivatives, copy-out
 //
 // The persistent SSM kernels are where the time goes. Their loop body is one
@@ -78,15 +78,16 @@ struct StateBuf {
 };
 
 // ------------------------------------------------------------------ lists
-// Split rounds 0..3 are PhaseSplit's first try and three restarts; round
-// LEARN_ROUND is the learned initialiser's split of fresh cells (before any
-// stability test), whose failures fall back to the stability test.
+// Split round 0 is PhaseSplit's first try; the cells that restart go on to
+// the warp-per-cell path (L_SLOW). Round LEARN_ROUND is the learned
+// initialiser's split of fresh cells (before any stability test), whose
+// failures fall back to the stability test.
 enum ListId : int {
     L_S01_0 = 0, L_S01_1,
     L_STA_0, L_STA_1, L_STA_2, L_STA_3,
     L_NRSTA_0, L_NRSTA_1, L_NRSTA_2, L_NRSTA_3,
-    L_SP_0, L_SP_1, L_SP_2, L_SP_3, L_SP_LEARN,
-    L_SPNR_0, L_SPNR_1, L_SPNR_2, L_SPNR_3, L_SPNR_LEARN,
+    L_SP_0, L_SP_LEARN,
+    L_SPNR_0, L_SPNR_LEARN,
     L_SLOW,
     L_FRESH,  // fresh cells awaiting the learned initialiser
     // mixed form: stability trials whose Newton polish failed from the FP32
@@ -95,7 +96,10 @@ enum ListId : int {
     L_NRSTC_0, L_NRSTC_1, L_NRSTC_2, L_NRSTC_3,
     L_COUNT
 };
-constexpr int SPLIT_ROUNDS = 4;  // first try + 3 restarts on the fast path
+// A restart runs 200 or 400 substitution steps on one cell: on the
+// thread-per-cell kernels that is a single busy lane per warp, so every
+// restart takes the warp-per-cell path.
+constexpr int SPLIT_ROUNDS = 1;
 constexpr int LEARN_ROUND  = SPLIT_ROUNDS;
 static_assert(L_SP_0 + LEARN_ROUND == L_SP_LEARN && L_SPNR_0 + LEARN_ROUND == L_SPNR_LEARN, "list order");
 

@@ -267,13 +267,16 @@ __device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k, int
 {
     using F_ = SF<NC>;
     const StateBuf& S = a.S;
-    OCPF_FOR_ITEMS(a, list, c)
-    {
-        CellFlash<NC> f(F);
-        uint32_t      meta;
+    const uint32_t  n = a.L.len(list);
+    CellFlash<NC>   f(F);
+    uint32_t        meta = 0;
+    double          fugId[NC], Y[NC], fugSta[NC], res[NC];
+    double          Asta = 0, Bsta = 0, Zsta = 0, Se = 0;
+    int             iter = 0;
+    int64_t         c    = a.L.take(list, n);
+    auto load = [&]() {
         load_book(f, S, c, meta);
         f.P = a.in.P[c];
-        double fugId[NC], Y[NC], fugSta[NC], res[NC];
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             f.sA[i]   = S.D(F_::sA + i, c);
@@ -283,14 +286,39 @@ __device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k, int
             fugSta[i] = S.D(F_::phiS + i, c) * Y[i] * f.P;
             res[i]    = log(fugId[i] / (fugSta[i] * f.Yt));
         }
-        double Asta = S.D(F_::Asta, c), Bsta = S.D(F_::Bsta, c), Zsta = S.D(F_::Zsta, c);
-        double Se = 0;
+        Asta = S.D(F_::Asta, c), Bsta = S.D(F_::Bsta, c), Zsta = S.D(F_::Zsta, c);
+        Se   = 0;
 #pragma unroll
         for (int i = 0; i < NC; i++) Se += res[i] * res[i];
-        Se        = sqrt(Se);
-        int  iter = 0;
-        bool flag = true;
-        while (Se > F.nrsta_tol) {
+        Se   = sqrt(Se);
+        iter = 0;
+    };
+    // the end of StableNR for the lane's cell: verdict, or (mixed form) the
+    // FP64 continuation of a trial whose Newton step failed from FP32
+    auto finish = [&](bool flag) {
+        f.it_nrsta += iter;
+        if (!flag && fallback >= 0) {
+            f.status &= (uint16_t)~ST_NRSTA_FAIL;
+            f.Yt = S.D(F_::Yt, c);
+            store_book(f, S, c, meta | M_STC);
+            a.L.push(fallback, (int32_t)c);
+        } else {
+            f.nrsta_conflag = flag;
+            f.nrsta_realTol = Se;
+            sta_decide(f, a, c, meta & ~M_STC, k, flag);
+        }
+        c = a.L.take(list, n);
+        if (c >= 0) load();
+    };
+    if (c >= 0) load();
+    // StableNR iterations (src/MixtureComp.cpp:1600-1635) on a persistent
+    // grid: one Newton step per loop turn for every active lane
+    while (__any_sync(0xffffffffu, c >= 0)) {
+        if (c >= 0) {
+            if (!(Se > F.nrsta_tol)) {
+                finish(true);
+                continue;
+            }
             f.sta_nr_update(Y, f.Yt, res, Asta, Bsta, Zsta);
             f.fug_phi(Y, nullptr, fugSta, Asta, Bsta, Zsta);
             Se = 0;
@@ -303,24 +331,11 @@ __device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k, int
             iter++;
             if (iter > F.nrsta_maxit) {
                 f.status |= ST_NRSTA_FAIL;
-                flag = false;
-                break;
+                finish(false);
+            } else if (!(Se > F.nrsta_tol)) {
+                finish(true);
             }
         }
-        f.it_nrsta += iter;
-        if (!flag && fallback >= 0) {
-            // mixed form: Newton did not converge from the FP32 end point;
-            // continue the substitution there in FP64 to the reference's
-            // tolerance, then Newton again
-            f.status &= (uint16_t)~ST_NRSTA_FAIL;
-            f.Yt = S.D(F_::Yt, c);
-            store_book(f, S, c, meta | M_STC);
-            a.L.push(fallback, (int32_t)c);
-            continue;
-        }
-        f.nrsta_conflag = flag;
-        f.nrsta_realTol = Se;
-        sta_decide(f, a, c, meta & ~M_STC, k, flag);
     }
 }
 
@@ -774,47 +789,69 @@ __device__ void sp_nrinit_body(const FluidConst& F, const PhasedArgs& a, int r)
     }
 }
 
-// SplitNR iterations (src/MixtureComp.cpp:2071-2152), one thread per cell.
+// SplitNR iterations (src/MixtureComp.cpp:2071-2152) on a persistent grid:
+// each loop turn is one Newton step (Jacobian, solve, fugacities, residual)
+// for every active lane; a lane whose cell ends its Newton loop finishes it
+// (sp_after_nr) and takes the next cell, so lanes stay busy however
+// unequal the cells' step counts are.
 template <int NC>
 __device__ void sp_nr_body(const FluidConst& F, const PhasedArgs& a, int r)
 {
     using F_ = SF<NC>;
-    const StateBuf& S = a.S;
-    OCPF_FOR_ITEMS(a, L_SPNR_0 + r, c)
-    {
-        CellFlash<NC> f(F);
-        uint32_t      meta;
+    const StateBuf& S    = a.S;
+    const int       list = L_SPNR_0 + r;
+    const uint32_t  n    = a.L.len(list);
+    CellFlash<NC>   f(F);
+    uint32_t        meta = 0;
+    double          res[NC];
+    double          eNR0 = 0, eNR = 0;
+    int             iter = 0;
+    int64_t         c    = a.L.take(list, n);
+    auto load = [&]() {
         load_split_cell(f, a, c, meta);
-        const double eNR0 = S.D(F_::eNR0, c);
-        double       res[NC];
+        eNR0 = S.D(F_::eNR0, c);
+        eNR  = eNR0;
+        iter = 0;
 #pragma unroll
         for (int i = 0; i < NC; i++) res[i] = log(f.fug[1][i] / f.fug[0][i]);
-        double eNR  = eNR0;
-        int    iter = 0;
-        while (eNR > F.nrsp_tol) {
-            const double en = f.sp_nr_update(res);
-            f.fug_phi_all();
-            eNR = 0;
+    };
+    if (c >= 0) load();
+    while (__any_sync(0xffffffffu, c >= 0)) {
+        if (c >= 0) {
+            bool done = !(eNR > F.nrsp_tol);
+            if (!done) {
+                const double en = f.sp_nr_update(res);
+                f.fug_phi_all();
+                eNR = 0;
 #pragma unroll
-            for (int i = 0; i < NC; i++) {
-                res[i] = log(f.fug[1][i] / f.fug[0][i]);
-                eNR += res[i] * res[i];
+                for (int i = 0; i < NC; i++) {
+                    res[i] = log(f.fug[1][i] / f.fug[0][i]);
+                    eNR += res[i] * res[i];
+                }
+                eNR = sqrt(eNR);
+                iter++;
+                if (eNR > eNR0 || iter > F.nrsp_maxit) {
+                    done = true;
+                } else if (en / (2 * NC) < 1e-8) {
+                    f.nrsp_conflag = true;
+                    done           = true;
+                } else {
+                    done = !(eNR > F.nrsp_tol);
+                }
             }
-            eNR = sqrt(eNR);
-            iter++;
-            if (eNR > eNR0 || iter > F.nrsp_maxit) break;
-            if (en / (2 * NC) < 1e-8) {
-                f.nrsp_conflag = true;
-                break;
+            if (done) {
+                sp_after_nr(f, a, c, meta, r, eNR, iter);
+                c = a.L.take(list, n);
+                if (c >= 0) load();
             }
         }
-        sp_after_nr(f, a, c, meta, r, eNR, iter);
     }
 }
 
-// The rest of PhaseSplit's restart loop (src/MixtureComp.cpp:1750-1758) for
-// the cells still restarting after the last split round (rare), one warp per
-// cell (flash_warp.cuh); lane 0 stores the result.
+// PhaseSplit's restart loop (src/MixtureComp.cpp:1750-1758) for the cells
+// whose first split did not converge (rare: a few hundred per million
+// states, some needing tens of thousands of steps), one warp per cell
+// (flash_warp.cuh); lane 0 stores the result.
 template <int NC>
 __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
 {

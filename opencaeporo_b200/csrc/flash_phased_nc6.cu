@@ -26,7 +26,6 @@ K128 kp_sta_nr_6(const __grid_constant__ FluidConst F, const PhasedArgs a, int k
 }
 K128 kp_sp_prep_6(const __grid_constant__ FluidConst F, const PhasedArgs a, int r) { sp_prep_body<6>(F, a, r); }
 K128 kp_sp_ssm_6(const __grid_constant__ FluidConst F, const PhasedArgs a, int r) { sp_ssm_body<6>(F, a, r); }
-K128 kp_sp_ssm32_6(const __grid_constant__ FluidConst F, const PhasedArgs a, int r) { sp_ssm32_body<6>(F, a, r); }
 K128 kp_sp_nrinit_6(const __grid_constant__ FluidConst F, const PhasedArgs a, int r) { sp_nrinit_body<6>(F, a, r); }
 K128 kp_sp_nr_6(const __grid_constant__ FluidConst F, const PhasedArgs a, int r) { sp_nr_body<6>(F, a, r); }
 K128 kp_slow_6(const __grid_constant__ FluidConst F, const PhasedArgs a) { slow_body<6>(F, a); }
@@ -45,27 +44,19 @@ static int persistent_grid(const void* k, int sms)
     return sms * (per_sm > 0 ? per_sm : 1);
 }
 
-// One split round: set-up, successive substitution (in the mixed form's
-// first try and learned round FP32 first, then FP64 to the reference's
-// tolerance), Newton start, Newton.
+// One split round: set-up, successive substitution, Newton start, Newton.
 static void split_round_6(const FluidConst& F, const PhasedArgs& a, cudaStream_t st, int r, int gp, int gs,
-                            int gs32, bool fp32)
+                            int gnr)
 {
     kp_sp_prep_6<<<gp, 128, 0, st>>>(F, a, r);
-    if (fp32) {
-        kp_sp_ssm32_6<<<gs32, 128, 0, st>>>(F, a, r);
-        // the FP64 kernel continues every cell from where FP32 ended: its
-        // persistent consumers take the same list again from the start
-        cudaMemsetAsync(a.L.ctr + 2 * (L_SP_0 + r) + 1, 0, sizeof(uint32_t), st);
-    }
     kp_sp_ssm_6<<<gs, 128, 0, st>>>(F, a, r);
     kp_sp_nrinit_6<<<gp, 128, 0, st>>>(F, a, r);
-    kp_sp_nr_6<<<gp, 128, 0, st>>>(F, a, r);
+    kp_sp_nr_6<<<gnr, 128, 0, st>>>(F, a, r);
 }
 
 cudaError_t launch_phased_nc6(const FluidConst& F, const PhasedArgs& a, cudaStream_t st)
 {
-    static int g_s01 = 0, g_sta = 0, g_sp = 0, g_sta32 = 0, g_sp32 = 0, sms = 0;
+    static int g_s01 = 0, g_sta = 0, g_sp = 0, g_sta32 = 0, g_spnr = 0, g_stnr = 0, sms = 0;
     if (!sms) {
         int dev = 0;
         cudaGetDevice(&dev);
@@ -74,7 +65,8 @@ cudaError_t launch_phased_nc6(const FluidConst& F, const PhasedArgs& a, cudaStre
         g_sta = persistent_grid((const void*)kp_sta_ssm_6, sms);
         g_sp  = persistent_grid((const void*)kp_sp_ssm_6, sms);
         g_sta32 = persistent_grid((const void*)kp_sta_ssm32_6, sms);
-        g_sp32  = persistent_grid((const void*)kp_sp_ssm32_6, sms);
+        g_spnr  = persistent_grid((const void*)kp_sp_nr_6, sms);
+        g_stnr  = persistent_grid((const void*)kp_sta_nr_6, sms);
         cudaFuncSetAttribute(kp_learn_6, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(LearnSmem));
     }
     const int64_t need  = (a.count + 127) / 128;
@@ -87,7 +79,7 @@ cudaError_t launch_phased_nc6(const FluidConst& F, const PhasedArgs& a, cudaStre
         // learned initialiser: predicted-unstable fresh cells split first
         const int gl = (int)std::min<int64_t>((a.count + 63) / 64, (int64_t)sms * 4);
         kp_learn_6<<<gl, 128, sizeof(LearnSmem), st>>>(F, a);
-        split_round_6(F, a, st, LEARN_ROUND, gp, g_sp, g_sp32, mixed);
+        split_round_6(F, a, st, LEARN_ROUND, gp, g_sp, g_spnr);
     }
     for (int k = 0; k < 2; k++) {
         kp_s01_prep_6<<<gp, 128, 0, st>>>(F, a, k);
@@ -101,18 +93,18 @@ cudaError_t launch_phased_nc6(const FluidConst& F, const PhasedArgs& a, cudaStre
             // Newton fails continue in FP64, then Newton again
             kp_sta_ssm32_6<<<g_sta32, 128, 0, st>>>(F, a, k);
             kp_sta_verdict_6<<<gp, 128, 0, st>>>(F, a, k, L_STA_0 + k, L_NRSTA_0 + k, true);
-            kp_sta_nr_6<<<gp, 128, 0, st>>>(F, a, k, L_NRSTA_0 + k, L_STC_0 + k);
+            kp_sta_nr_6<<<g_stnr, 128, 0, st>>>(F, a, k, L_NRSTA_0 + k, L_STC_0 + k);
             kp_sta_ssm_6<<<g_sta, 128, 0, st>>>(F, a, L_STC_0 + k);
             kp_sta_verdict_6<<<gp, 128, 0, st>>>(F, a, k, L_STC_0 + k, L_NRSTC_0 + k, false);
-            kp_sta_nr_6<<<gp, 128, 0, st>>>(F, a, k, L_NRSTC_0 + k, -1);
+            kp_sta_nr_6<<<g_stnr, 128, 0, st>>>(F, a, k, L_NRSTC_0 + k, -1);
         } else {
             kp_sta_ssm_6<<<g_sta, 128, 0, st>>>(F, a, L_STA_0 + k);
             kp_sta_verdict_6<<<gp, 128, 0, st>>>(F, a, k, L_STA_0 + k, L_NRSTA_0 + k, false);
-            kp_sta_nr_6<<<gp, 128, 0, st>>>(F, a, k, L_NRSTA_0 + k, -1);
+            kp_sta_nr_6<<<g_stnr, 128, 0, st>>>(F, a, k, L_NRSTA_0 + k, -1);
         }
     }
     for (int r = 0; r < SPLIT_ROUNDS; r++)
-        split_round_6(F, a, st, r, gp, g_sp, g_sp32, mixed && r == 0);
+        split_round_6(F, a, st, r, gp, g_sp, g_spnr);
     kp_slow_6<<<gp, 128, 0, st>>>(F, a);
     kp_finalize_6<<<gcell, 128, 0, st>>>(F, a);
     return cudaGetLastError();

@@ -195,3 +195,25 @@ class MixtureCompBatch:
         rc = lib().ocpf_flash_fim_host(self._h, ncell, C.byref(fin), C.byref(sk), C.byref(fo),
                                        FORMS[form])
         check(rc, "ocpf_flash_fim_host")
+
+
+def flash_fim_regions(regions, form: str = "batched", stream=None, fresh: bool = False, diagnostics: bool = True):
+    """Flashes several PVT regions in one call (``ocpf_flash_fim_regions``):
+    ``regions`` is a list of (MixtureCompBatch, CellState) pairs, one per
+    region, on one device; fluids may have different component counts. The
+    regions run concurrently on their contexts' streams, joined back into
+    ``stream`` (default: torch's current stream)."""
+    torch = _torch()
+    n = len(regions)
+    if n == 0:
+        return
+    dev = regions[0][0].device
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    ctx = (C.c_void_p * n)(*[m._h.value for m, _ in regions])
+    cnt = (C.c_int64 * n)(*[st.ncell for _, st in regions])
+    ins, sks, outs = (_lib.FimIn * n)(), (_lib.Skip * n)(), (_lib.FimOut * n)()
+    for r, (m, st) in enumerate(regions):
+        ins[r], sks[r], outs[r] = m._structs(st, optional=diagnostics, fresh=fresh)
+    rc = lib().ocpf_flash_fim_regions(n, ctx, cnt, ins, sks, outs, FORMS[form], C.c_void_p(stream.cuda_stream))
+    check(rc, "ocpf_flash_fim_regions")

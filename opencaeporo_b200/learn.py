@@ -45,8 +45,8 @@ def raw_features(P, T, Ni):
     Ni = np.asarray(Ni, dtype=np.float64)
     nc = Ni.shape[1] - 1
     z = Ni[:, :nc] / np.sum(np.abs(Ni[:, :nc]), axis=1, keepdims=True)
-    return np.vstack([np.log(np.asarray(P, dtype=np.float64))[None, :],
-                      np.asarray(T, dtype=np.float64)[None, :], z.T])
+    return np.ascontiguousarray(np.vstack([np.log(np.asarray(P, dtype=np.float64))[None, :],
+                                           np.asarray(T, dtype=np.float64)[None, :], z.T]))
 
 
 def targets_from_flash(out: dict, nc: int):
@@ -113,12 +113,13 @@ class Initializer:
               "ocpf_set_initializer")
 
     def normalise(self, raw):
-        return ((raw - self.in_mean[:, None]) / self.in_scale[:, None]).astype(np.float32)
+        return np.ascontiguousarray((raw - self.in_mean[:, None]) / self.in_scale[:, None], dtype=np.float32)
 
 
 def forward(params_dev, x_dev, nout):
     """Network outputs [nout, n] for normalised features x [nin, n] (device tensors)."""
     torch = _torch()
+    x_dev = x_dev.contiguous()  # the kernel reads x[f * n + s]
     nin, n = x_dev.shape
     y = torch.empty((nout, n), dtype=torch.float32, device=x_dev.device)
     check(lib().ocpf_mlp_forward(nin, nout, n, params_dev.data_ptr(), x_dev.data_ptr(), y.data_ptr(), None),
@@ -127,6 +128,7 @@ def forward(params_dev, x_dev, nout):
 
 
 def grad(params_dev, x_dev, t_dev, w_dev, lnk_weight, grad_dev, loss_dev):
+    x_dev, t_dev, w_dev = x_dev.contiguous(), t_dev.contiguous(), w_dev.contiguous()
     nin, n = x_dev.shape
     nout = t_dev.shape[0]
     check(lib().ocpf_mlp_grad(nin, nout, n, params_dev.data_ptr(), x_dev.data_ptr(), t_dev.data_ptr(),

@@ -19,7 +19,7 @@ def bench_fluid():
     return synthetic_fluid(6, 1234)
 
 
-def gpu_phase_counter(fluid, device, chunk=1 << 18):
+def gpu_phase_counter(fluid, device, chunk=1 << 20):
     """Hydrocarbon phase count of (P, T, Ni) batches with the batched GPU
     flash (used only to place the near-envelope states)."""
     from .flash import MixtureCompBatch

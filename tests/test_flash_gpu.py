@@ -39,10 +39,12 @@ def test_matches_reference_goldens(case, form):
     same = got["phaseNum"] == ref["phaseNum"]
     assert np.array_equal(got["ftype"][same], ref["ftype"][same])
     # the work done follows the reference's: iteration counts are noise-
-    # sensitive near tol^2 = 1e-24, so the flop-weighted total is held to 5 %
+    # sensitive near tol^2 = 1e-24, so the flop-weighted total over the
+    # cells that are not knife-edge is held to 5 %
     from opencaeporo_b200 import roofline
-    wa = roofline.flops(fl.nc, got["iters"], got["phaseNum"] - 1)
-    wb = roofline.flops(fl.nc, ref["iters"], ref["NPhc"])
+    k = same & ~fragile
+    wa = roofline.flops(fl.nc, got["iters"][k], got["phaseNum"][k] - 1)
+    wb = roofline.flops(fl.nc, ref["iters"][k], ref["NPhc"][k])
     assert abs(wa - wb) <= 0.05 * wb, (got["iters"].sum(axis=0), ref["iters"].sum(axis=0))
 
 
@@ -212,3 +214,33 @@ def test_batched_host_path_and_reserve():
         np.testing.assert_array_equal(np.nan_to_num(a.astype(np.float64)),
                                       np.nan_to_num(dev[k].astype(np.float64)), err_msg=k)
     m.close()
+
+
+def test_regions_call_equals_one_call_per_region():
+    """Four PVT regions of 3, 6, 9 and 12 components in one
+    ocpf_flash_fim_regions call (each on its own stream) give exactly the
+    outputs of one ocpf_flash_fim per region."""
+    torch = _torch()
+    from opencaeporo_b200 import synth
+    from opencaeporo_b200.flash import MixtureCompBatch, flash_fim_regions
+    from opencaeporo_b200.fluid import synthetic_fluid
+    regs, sts, alone = [], [], []
+    for nc, seed in ((3, 31), (6, 61), (9, 91), (12, 121)):
+        fl = synthetic_fluid(nc, seed)
+        w = synth.uniform_states(fl, 3000 + 500 * nc, seed, p_mpa=(2.0, 60.0), t_k=(300.0, 450.0), alpha=0.5)
+        m = MixtureCompBatch(fl)
+        a = m.new_state(len(w["P"]))
+        b = m.new_state(len(w["P"]))
+        for st in (a, b):
+            st.load(w["P"], w["T"], w["Ni"])
+        m.flash_fim(a, form="batched", fresh=True)
+        regs.append((m, b))
+        alone.append(a)
+    flash_fim_regions(regs, form="batched", fresh=True)
+    torch.cuda.synchronize()
+    for (m, b), a in zip(regs, alone):
+        ha, hb = a.to_host(), b.to_host()
+        for k, v in ha.items():
+            if isinstance(v, np.ndarray):
+                np.testing.assert_array_equal(v, hb[k], err_msg=f"nc={m.nc} {k}")
+        m.close()

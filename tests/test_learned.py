@@ -113,7 +113,7 @@ def test_training_fits_a_known_function():
     t[1:] = A @ x
     w = np.ones(n, np.float32)
     logs = []
-    params = learn.train(x, t, w, epochs=6, batch=4096, lr=3e-3, log=logs.append)
+    params = learn.train(x, t, w, epochs=12, batch=4096, lr=3e-3, log=logs.append)
     import torch
     y = learn.forward(torch.as_tensor(params, device="cuda"), torch.as_tensor(x, device="cuda"), nout).cpu().numpy()
     acc = np.mean((y[0] > 0) == (t[0] > 0.5))
