@@ -138,6 +138,13 @@ struct ocpf_ctx {
     // ocpf_flash_fim_regions: this region's stream and its fork/join events
     cudaStream_t rs;
     cudaEvent_t  evf, evj;
+    // the batched forms' launch sequence as a CUDA graph, replayed while the
+    // call's arguments stay the same (captured on a private stream)
+    int64_t         launches;  // batched-form calls so far
+    cudaStream_t    gs;
+    cudaGraphExec_t gexec;
+    PhasedArgs      gkey;
+    bool            gvalid;
 };
 
 static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
@@ -185,6 +192,10 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->mlp       = nullptr;
     c->rs        = nullptr;
     c->evf = c->evj = nullptr;
+    c->launches  = 0;
+    c->gs        = nullptr;
+    c->gexec     = nullptr;
+    c->gvalid    = false;
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         cudaSetDevice(prev);
@@ -207,6 +218,8 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     if (c->eq) cudaFree(c->eq);
     if (c->mlp) cudaFree(c->mlp);
     if (c->rs) cudaStreamDestroy(c->rs);
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->gs) cudaStreamDestroy(c->gs);
     if (c->evf) cudaEventDestroy(c->evf);
     if (c->evj) cudaEventDestroy(c->evj);
     for (auto& s : c->hs)
@@ -271,6 +284,55 @@ static void scratch_view(const ocpf_ctx* c, int part, int64_t cap, StateBuf& S, 
     L.ctr      = (uint32_t*)(L.items + (size_t)L_COUNT * cap);
 }
 
+// The batched forms launch ~40-60 kernels per call. From the second call of
+// a context on (the first one also sets up each kernel's launch shape), the
+// sequence is captured once into a CUDA graph on the context's private
+// stream and replayed with one cudaGraphLaunch on the caller's stream while
+// the arguments (sizes, device pointers, form) stay the same; a change
+// re-captures (cudaGraphExecUpdate keeps the executable when only parameters
+// differ). Work already captured by the caller's own stream capture, and the
+// host path's alternating parts, launch directly.
+static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs& args, cudaStream_t st,
+                                 bool graph_ok)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusInvalidated;
+    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, st);
+    if (!(c->gvalid && std::memcmp(&c->gkey, &args, sizeof(args)) == 0)) {
+        c->gvalid = false;
+        if (!c->gs && cudaStreamCreateWithFlags(&c->gs, cudaStreamNonBlocking) != cudaSuccess) return k(c->fc, args, st);
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(c->gs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return k(c->fc, args, st);
+        const cudaError_t le = k(c->fc, args, c->gs);
+        const cudaError_t ce = cudaStreamEndCapture(c->gs, &g);
+        if (le != cudaSuccess || ce != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return k(c->fc, args, st);
+        }
+        bool ok = false;
+        if (c->gexec) {
+            cudaGraphExecUpdateResultInfo info;
+            ok = cudaGraphExecUpdate(c->gexec, g, &info) == cudaSuccess;
+            if (!ok) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(c->gexec);
+                c->gexec = nullptr;
+            }
+        }
+        if (!ok) ok = cudaGraphInstantiate(&c->gexec, g, 0) == cudaSuccess;
+        cudaGraphDestroy(g);
+        if (!ok) {
+            c->gexec = nullptr;
+            cudaGetLastError();
+            return k(c->fc, args, st);
+        }
+        c->gkey   = args;
+        c->gvalid = true;
+    }
+    return cudaGraphLaunch(c->gexec, st);
+}
+
 static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, const ocpf_fim_in& in,
                        const ocpf_skip& sk, const ocpf_fim_out& out, cudaStream_t st, bool timed,
                        int part = -1)
@@ -291,6 +353,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         PhasedLauncher k  = phased_kernel(c->fc.nc, &nd);
         if (!k) return OCPF_EUNSUPPORTED;
         PhasedArgs args;
+        std::memset(&args, 0, sizeof(args));  // compared bytewise as the graph's key
         args.count  = count;
         args.stride = stride;
         args.in     = in;
@@ -308,7 +371,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
             scratch_view(c, part, stride, args.S, args.L);
         }
         if (timed) cudaEventRecord(c->ev0, st);
-        e = k(c->fc, args, st);
+        e = launch_phased(c, k, args, st, part < 0);
         if (timed) cudaEventRecord(c->ev1, st);
     }
     return e == cudaSuccess ? OCPF_OK : OCPF_ECUDA;
@@ -653,6 +716,7 @@ extern "C" int ocpf_set_initializer(ocpf_ctx* c, const float* params, const floa
         }
         c->fc.learn_conf = confidence;
         c->fc.learn_on   = 1;
+        c->gvalid        = false;  // the constants a captured graph holds changed
     }
     if (prev != c->device) cudaSetDevice(prev);
     return rc;

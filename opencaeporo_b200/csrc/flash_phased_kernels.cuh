@@ -626,26 +626,32 @@ __device__ void sp_ssm_body(const FluidConst& F, const PhasedArgs& a, int r)
 }
 
 // End of the learned initialiser's split (no reference counterpart). The
-// split is kept when SplitNR converged to two phases (CheckSplit's accept
-// branch, src/MixtureComp.cpp:1790-1797) that differ (sum ln^2 K > 1e-4,
+// split is kept when SplitNR converged to its tolerance with two phases
+// (CheckSplit's accept branch, src/MixtureComp.cpp:1790-1797) whose
+// compositions each sum to one, that differ (sum ln^2 K > 1e-4,
 // StableSSM01's trivial-solution bound) and whose Gibbs energy is below the
 // feed's: sum_i z_i (ln f_i - ln f_i(z)) < 0, so the feed is unstable and the
-// stability test would send it to this split. Otherwise the cell returns,
-// as a fresh single-phase cell, to the strict stability test.
+// stability test would send it to a split. Otherwise the cell returns, as a
+// fresh single-phase cell, to the strict stability test.
 template <int NC>
 __device__ __forceinline__ void learned_after_nr(CellFlash<NC>& f, const PhasedArgs& a, int64_t c, uint32_t meta)
 {
     using F_ = SF<NC>;
     const StateBuf& S     = a.S;
     const double    nuMax = f.nu[0] < f.nu[1] ? f.nu[1] : f.nu[0];
-    double          eX = 0, tk = 0, dg = 0;
+    double          eX = 0, tk = 0, dg = 0, s0 = 0, s1 = 0;
 #pragma unroll
     for (int i = 0; i < NC; i++) {
         eX += sq(f.x[0][i] - f.x[1][i]);
         tk += sq(log(f.x[0][i] / f.x[1][i]));
         dg += f.zi[i] * log(f.fug[0][i] / (S.D(F_::phiZ + i, c) * f.zi[i] * f.P));
+        s0 += f.x[0][i];
+        s1 += f.x[1][i];
     }
-    const bool keep = f.nrsp_conflag && f.NP == 2 && nuMax < 1 && 1 - nuMax >= 1e-3 && isfinite(eX) &&
+    // converged to the tolerance (not SplitNR's small-step exit), both
+    // compositions summing to one (no phase-1 moles folded by |n / nu|)
+    const bool keep = f.nrsp_conflag && f.nrsp_realTol < f.F.nrsp_tol && fabs(s0 - 1) < 1e-10 &&
+                      fabs(s1 - 1) < 1e-10 && f.NP == 2 && nuMax < 1 && 1 - nuMax >= 1e-3 && isfinite(eX) &&
                       tk > 1e-4 && dg < 0;
     if (keep) {
         f.check_split();

@@ -244,3 +244,27 @@ def test_regions_call_equals_one_call_per_region():
             if isinstance(v, np.ndarray):
                 np.testing.assert_array_equal(v, hb[k], err_msg=f"nc={m.nc} {k}")
         m.close()
+
+
+def test_graph_replay_equals_direct_launch():
+    """From the second call on, the batched sequence is replayed from a
+    captured CUDA graph; replays (also after the arguments change, which
+    re-captures) give exactly the direct launch's outputs."""
+    torch = _torch()
+    from opencaeporo_b200.flash import MixtureCompBatch
+    fl, inp, ref, _ = load_golden("uniform_nc6")
+    m = MixtureCompBatch(fl)
+    n = len(inp["P"])
+    sts = [m.new_state(n), m.new_state(n)]
+    outs = []
+    for call in range(4):
+        st = sts[call % 2 if call > 1 else 0]
+        st.load(inp["P"], inp["T"], inp["Ni"])
+        m.flash_fim(st, form="mixed", fresh=True)
+        torch.cuda.synchronize()
+        outs.append(st.to_host())
+    m.close()
+    for o in outs[1:]:
+        for k, v in outs[0].items():
+            if isinstance(v, np.ndarray):
+                np.testing.assert_array_equal(v, o[k], err_msg=k)

@@ -129,19 +129,57 @@ def _model():
     return Initializer.load(MODEL)
 
 
+def _sub(d, mask):
+    n = len(mask)
+    out = {}
+    for k, v in d.items():
+        if isinstance(v, dict):
+            out[k] = _sub(v, mask)
+        elif isinstance(v, np.ndarray) and v.ndim and v.shape[0] == n:
+            out[k] = v[mask]
+        else:
+            out[k] = v
+    return out
+
+
+def _clean_equilibrium(res, nc):
+    """Cells whose result is a converged equilibrium: residual at or below
+    1e-9 and every present hydrocarbon phase's composition summing to one."""
+    n = len(res["phaseNum"])
+    x = np.nan_to_num(np.asarray(res["xij"]).reshape(n, 3, nc + 1)[:, :2, :nc])
+    ex = np.asarray(res["phaseExist"])[:, :2].astype(bool)
+    sums_ok = np.all(~ex | (np.abs(x.sum(axis=2) - 1) < 1e-9), axis=1)
+    return (np.asarray(res["ePEC"]) <= 1e-9) & sums_ok
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["uniform_nc6", "near_nc6"])
+@pytest.mark.parametrize("case", ["uniform_nc6", "near_nc6", "warm_nc6", "restart_nc6"])
 def test_fast_matches_reference_goldens(case):
-    """Fast form (mixed + trained initialiser) against the reference: the
-    same bar as every other form (identical phase counts except knife-edge
-    cells; outputs within 1e-8 relative or 10x the reference's own 1-ulp
-    sensitivity)."""
+    """Fast form (mixed + trained initialiser) against the reference. Where
+    the reference converged (ePEC <= 1e-9: its answer is an equilibrium),
+    the bar of every other form: identical phase counts except knife-edge
+    cells, outputs within 1e-8 relative or 10x the reference's own 1-ulp
+    sensitivity. Where it did not -- SplitNR stopped on its small-step test
+    short of its tolerance, with compositions no longer summing to one --
+    the fast form may have found the converged equilibrium instead; every
+    such cell it does not reproduce must be one."""
     from conftest import load_golden, run_gpu
     from oracle import compare as CMP
     fl, inp, ref, fragile = load_golden(case)
     got = run_gpu(fl, inp, form="fast", init=_model())
-    chk = CMP.check(got, ref, fl.nc, noise=ref["noise"], fragile=fragile)
+    det = np.asarray(ref["ePEC"]) <= 1e-9
+    chk = CMP.check(_sub(got, det), _sub(ref, det), fl.nc, noise=_sub(ref["noise"], det), fragile=fragile[det])
     assert chk["ok"], f"{case}: {CMP.check_summary(chk)}"
+    if (~det).any():
+        c2 = CMP.check(_sub(got, ~det), _sub(ref, ~det), fl.nc, noise=_sub(ref["noise"], ~det),
+                       fragile=fragile[~det])
+        worst = np.zeros(int((~det).sum()))
+        for k in CMP.FLOAT_KEYS:
+            allowed = np.maximum(1e-8, 10 * np.nan_to_num(_sub(ref["noise"], ~det)[k], nan=0.0))
+            worst = np.fmax(worst, np.nan_to_num(c2["errors"][k], nan=0.0) / allowed)
+        differs = (worst > 1) | ~c2["errors"]["same"]
+        clean = _clean_equilibrium(_sub(got, ~det), fl.nc)
+        assert np.all(clean[differs]), np.nonzero(~det)[0][differs & ~clean]
 
 
 @pytest.mark.gpu
@@ -178,8 +216,14 @@ def test_initialiser_gain_over_mixed():
         res[form], ms[form] = st.to_host(), best
         m.close()
     mix, fast = res["mixed"], res["fast"]
-    mism = np.count_nonzero(mix["phaseNum"] != fast["phaseNum"])
-    assert mism <= max(3, n // 10000), mism
+    # where the mixed form's answer is a converged equilibrium the fast form
+    # ends with the same phase count (a few knife-edge cells aside); where it
+    # is not, a differing fast answer must be one
+    det = _clean_equilibrium(mix, fl.nc)
+    diff = mix["phaseNum"] != fast["phaseNum"]
+    mism = int(np.count_nonzero(diff & det))
+    assert mism <= max(3, n // 20000), mism
+    assert np.all(_clean_equilibrium(fast, fl.nc)[diff & ~det])
     it_m, it_f = mix["iters"].sum(axis=0), fast["iters"].sum(axis=0)
     work_m = roofline.flops(fl.nc, mix["iters"], mix["phaseNum"] - 1)
     work_f = roofline.flops(fl.nc, fast["iters"], fast["phaseNum"] - 1)
