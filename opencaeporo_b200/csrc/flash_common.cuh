@@ -61,8 +61,12 @@ constexpr uint16_t ST_NONFINITE  = OCPF_CELL_NONFINITE;
 constexpr uint16_t ST_SPLIT_CAP  = OCPF_CELL_SPLIT_CAP;
 constexpr uint16_t ST_GUARD      = OCPF_CELL_GUARD;
 
-// Bound on PhaseSplit's restart loop (src/MixtureComp.cpp:1752-1757 has none).
-constexpr int SPLIT_RESTART_CAP = 1000;
+// Bound on PhaseSplit's restart loop (src/MixtureComp.cpp:1752-1757 has none:
+// a cell whose restarts never converge loops there for ever). Converging
+// cells need few restarts (at most 78 in the 1M-state workload, at most 4 in
+// 262,144 states of wider P, T and composition ranges); cells that do not
+// converge within the bound are reported with OCPF_CELL_SPLIT_CAP.
+constexpr int SPLIT_RESTART_CAP = 200;
 
 __device__ __forceinline__ double sq(double v) { return v * v; }
 __device__ __forceinline__ double dlt(int i, int k) { return i == k ? 1.0 : 0.0; }

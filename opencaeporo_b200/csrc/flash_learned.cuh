@@ -1,11 +1,14 @@
 // flash_learned.cuh -- the learned initialiser inside the fast form
 // (OCPF_FORM_FAST): fresh cells (no last phase count) are run through the
 // MLP of learned.cuh on the tensor cores, 16 cells per warp. A cell whose
-// predicted probability of being unstable reaches the confidence goes
-// straight to a split (round LEARN_ROUND) started from the predicted K; the
+// predicted probability of ending two-phase reaches the confidence skips the
+// stability test and goes straight to a split (round LEARN_ROUND); the
 // rest, and every cell whose learned split fails its checks
 // (learned_after_nr), take the strict stability test as in the other forms.
-// No counterpart in the reference.
+// The split starts from Wilson's K, not from the network's ln K: a different
+// start can lead the substitution to a different solution where the
+// mixture has more than one, and it shortens a linearly converging
+// substitution by only a step or two. No counterpart in the reference.
 #pragma once
 
 #include "flash_phased.cuh"
@@ -66,19 +69,13 @@ __device__ void learn_body(const FluidConst& F, const PhasedArgs& a, LearnSmem& 
                 const int64_t c  = a.L.item(L_FRESH, k);
                 const float*  o  = sm.out + threadIdx.x * MLP_IO;
                 const float   pu = 1.f / (1.f + __expf(-o[0]));
-                bool          go = pu >= F.learn_conf;
-                double        K[NC];
-#pragma unroll
-                for (int i = 0; i < NC; i++) {
-                    K[i] = exp((double)o[1 + i]);
-                    go   = go && K[i] > 0 && isfinite(K[i]);
-                }
-                if (go) {
+                if (pu >= F.learn_conf) {
                     // a two-phase start, as for a cell whose stability test
-                    // failed with Yt < 1.1 (the tighter split settings)
+                    // found it unstable with Yt < 1.1 (the tighter split
+                    // settings); the split starts from Wilson's K as the
+                    // reference's does (sp_prep), so it reaches the same
+                    // solution branch
                     const uint32_t meta = (uint32_t)S.I(IF_META, c);
-#pragma unroll
-                    for (int i = 0; i < NC; i++) S.D(F_::Ks + i, c) = K[i];
                     S.D(F_::Yt, c)    = 1.01;
                     S.I(IF_META, c)   = (int32_t)((meta & ~M_NP_MASK) | 2u | M_LEARNED);
                     a.L.push(L_SP_LEARN, (int32_t)c);

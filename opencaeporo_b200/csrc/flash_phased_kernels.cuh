@@ -521,8 +521,6 @@ __device__ void sp_prep_body(const FluidConst& F, const PhasedArgs& a, int r)
         if (!restart) {
             f.ssmsp_conflag = false;  // PhaseSplit, :1745-1749
             f.nrsp_conflag  = false;
-        }
-        if (!restart && r != LEARN_ROUND) {  // the learned round's K is the prediction
             const uint32_t lastNP = a.in.lastNP[c];
             const int      lNP    = lastNP > 0 ? (int)lastNP - 1 : 0;
             if (lNP == 2) {

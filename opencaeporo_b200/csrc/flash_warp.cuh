@@ -68,12 +68,15 @@ struct WarpSplit {
         const double numin = __shfl_sync(WARP_ALL, bound, 0);
         const double numax = __shfl_sync(WARP_ALL, bound, 16);
         double       v     = 0.5 * (numin + numax);
-        const double zq = pick(f.zi), Kq = pick(f.Ks);
+        // loop-invariant parts of component q's terms, formed as the
+        // one-thread form forms them: z km1 / tmp and z km1 km1 / (tmp tmp)
+        const double km1 = pick(f.Ks) - 1;
+        const double zk  = pick(f.zi) * km1;
+        const double num = half ? zk * km1 : zk;
         int          iter = 0;
         while (true) {
-            const double km1  = Kq - 1;
             const double tmp  = 1 + v * km1;
-            const double term = half ? zq * km1 * km1 / (tmp * tmp) : zq * km1 / tmp;
+            const double term = num / (half ? tmp * tmp : tmp);
             double       rj = 0, J = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {

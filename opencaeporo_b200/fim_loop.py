@@ -93,10 +93,26 @@ class SyntheticFIM:
         return P_t, T_t, N_t
 
 
-def run(forms=("plain", "fast"), steps=20, newton=4, device=0, log=print, grid=(60, 220, 85)):
+def _gather(st, idx):
+    """Host copies of a cell sample's inputs, warm-start state and outputs."""
+    o = st.out
+    return {"P": st.P[idx].cpu().numpy(), "T": st.T[idx].cpu().numpy(),
+            "Ni": st.Ni[:, idx].cpu().numpy().T.copy(),
+            "S": o["S"][:, idx].cpu().numpy().T.copy(), "lastNP": o["phaseNum"][idx].cpu().numpy().astype(np.int32),
+            "xij": o["xij"][:, idx].cpu().numpy().T.copy(),
+            "skip": {k: (v[idx] if v.dim() == 1 else v[:, idx].T).cpu().numpy().copy() for k, v in st.skip.items()},
+            "out": {k: (v[idx] if v.dim() == 1 else v[:, idx].T).cpu().numpy().copy() for k, v in o.items()}}
+
+
+def run(forms=("plain", "fast"), steps=20, newton=4, device=0, log=print, grid=(60, 220, 85), hook=None,
+        sample=4096, seed=5):
     """Runs the loop once per form in lockstep on identical inputs; returns
     per-iteration flash times and, for every form other than the first,
-    phase-count differences and output errors against the first."""
+    phase-count differences and output errors against the first. With
+    ``hook``, for a seeded sample of ``sample`` cells every iteration calls
+    hook(form, step, it, before, after): the sample's inputs and warm-start
+    state before the flash and its outputs after (host arrays, cell-major),
+    e.g. to check them against an oracle."""
     torch = _torch()
     from .flash import MixtureCompBatch
     from .workload import bench_fluid
@@ -111,17 +127,27 @@ def run(forms=("plain", "fast"), steps=20, newton=4, device=0, log=print, grid=(
         st = m.new_state(drv.n)
         ctx.append((form, m, st))
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in forms]
+    idx = None
+    if hook is not None:
+        idx = torch.as_tensor(np.sort(np.random.default_rng(seed).choice(drv.n, min(sample, drv.n), replace=False)),
+                              device=drv.dev)
     rec = {f: [] for f in forms}
     acc = {f: [] for f in forms[1:]}
     for step in range(steps):
         for it in range(newton):
             P, T, N = drv.inputs(step, it, newton)
+            before = {}
             for k, (form, m, st) in enumerate(ctx):
                 st.P.copy_(P); st.T.copy_(T); st.Ni.copy_(N)
+                if hook is not None:
+                    before[form] = _gather(st, idx)
                 ev[k][0].record()
                 m.flash_fim(st, form=form)
                 ev[k][1].record()
             torch.cuda.synchronize()
+            if hook is not None:
+                for form, m, st in ctx:
+                    hook(form, step, it, before[form], _gather(st, idx)["out"])
             for k, (form, m, st) in enumerate(ctx):
                 rec[form].append(ev[k][0].elapsed_time(ev[k][1]))
             base = ctx[0][2].out

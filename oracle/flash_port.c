@@ -946,7 +946,8 @@ static int check_split(Mix* m)
     return 1;
 }
 
-/* PhaseSplit, src/MixtureComp.cpp:1743-1782 (restart loop bounded at 1000) */
+/* PhaseSplit, src/MixtureComp.cpp:1743-1782 (restart loop bounded at 200,
+ * as the CUDA library bounds it; the reference's is unbounded) */
 static void phase_split(Mix* m)
 {
     m->ssmsp_conflag = 0;
@@ -954,7 +955,7 @@ static void phase_split(Mix* m)
     split_ssm2(m, 0);
     split_nr(m);
     int guard = 0;
-    while (!m->nrsp_conflag && guard++ < 1000) {
+    while (!m->nrsp_conflag && guard++ < 200) {
         split_ssm2(m, 1);
         split_nr(m);
         if (!check_split(m)) break;

@@ -260,6 +260,7 @@ def test_graph_replay_equals_direct_launch():
     for call in range(4):
         st = sts[call % 2 if call > 1 else 0]
         st.load(inp["P"], inp["T"], inp["Ni"])
+        st.skip["flag"].zero_()  # every call a fresh flash (no skip-cache hits)
         m.flash_fim(st, form="mixed", fresh=True)
         torch.cuda.synchronize()
         outs.append(st.to_host())
