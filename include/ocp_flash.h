@@ -150,6 +150,38 @@ typedef struct {
     uint16_t* status;       /* [ncell] OCPF_CELL_* bits */
 } ocpf_fim_out;
 
+/* FlashIMPEC's inputs (src/MixtureComp.cpp:444-450): no saturations. */
+typedef struct {
+    const double*   P;      /* [ncell] psia */
+    const double*   T;      /* [ncell] degF */
+    const double*   Ni;     /* [numCom][ncell] lbmol */
+    const uint32_t* lastNP; /* [ncell] phase count of the last step (0: fresh) */
+    const double*   xij;    /* [numPhase*numCom][ncell] last step's compositions */
+} ocpf_impec_in;
+
+/* The Bulk arrays IsoT_IMPEC::PassFlashValue fills (src/OCPFluidMethod.cpp:
+ * 275-305), same layouts as ocpf_fim_out, plus the phase volumes vj. Outputs
+ * of absent phases are left untouched, as there. The diagnostics may be
+ * null. */
+typedef struct {
+    uint32_t* phaseNum;
+    uint32_t* phaseExist;
+    double*   S;
+    double*   Nt;
+    double*   vf;
+    double*   vfP;
+    double*   vfi;
+    double*   vj;  /* [numPhase][ncell] ft3 */
+    double*   rho;
+    double*   xi;
+    double*   mu;
+    double*   xij;
+    double*   ePEC;
+    uint8_t*  ftype;
+    int32_t*  iters;
+    uint16_t* status;
+} ocpf_impec_out;
+
 typedef struct ocpf_ctx ocpf_ctx;
 
 /* Library version string. */
@@ -208,6 +240,15 @@ int ocpf_reserve(ocpf_ctx* ctx, int64_t ncell);
  * MixtureComp object on the host). */
 int ocpf_flash_fim_noalloc(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
                            ocpf_fim_out* out, void* stream);
+
+/* Batched MixtureComp::FlashIMPEC + IsoT_IMPEC::PassFlashValue over ncell
+ * cells (src/MixtureComp.cpp:444-492, src/OCPFluidMethod.cpp:264-305): the
+ * IMPEC flash type (skip or full; no two-phase warm type), the same phase
+ * equilibrium as the FIM call, then the volume derivatives vfi / vfP and the
+ * phase properties without dXsdXp or property partials. Forms and
+ * asynchrony as ocpf_flash_fim. */
+int ocpf_flash_impec(ocpf_ctx* ctx, int64_t ncell, const ocpf_impec_in* in, ocpf_skip* skip,
+                     ocpf_impec_out* out, int form, void* stream);
 
 /* Several PVT regions at once -- the batched counterpart of a Bulk whose
  * cells belong to different regions (flashCal[PVTNUM[n]] in

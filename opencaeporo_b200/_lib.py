@@ -34,7 +34,8 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_flash_fim", "ocpf_flash_fim_host", "ocpf_last_kernel_ms",
            "ocpf_measure_fma_peak", "ocpf_reserve", "ocpf_flash_fim_noalloc",
            "ocpf_mlp_param_count", "ocpf_mlp_forward", "ocpf_mlp_grad", "ocpf_mlp_adam",
-           "ocpf_set_initializer", "ocpf_flash_fim_regions", "ocpf_measure_fp64_latency")
+           "ocpf_set_initializer", "ocpf_flash_fim_regions", "ocpf_measure_fp64_latency",
+           "ocpf_flash_impec")
 
 _vp = C.c_void_p
 
@@ -72,6 +73,19 @@ class Skip(C.Structure):
 
 class FimOut(C.Structure):
     _fields_ = [(f, _vp) for f in OUT_FIELDS]
+
+
+IMPEC_IN_FIELDS = ("P", "T", "Ni", "lastNP", "xij")
+IMPEC_OUT_FIELDS = ("phaseNum", "phaseExist", "S", "Nt", "vf", "vfP", "vfi", "vj", "rho", "xi", "mu", "xij",
+                    "ePEC", "ftype", "iters", "status")
+
+
+class ImpecIn(C.Structure):
+    _fields_ = [(f, _vp) for f in IMPEC_IN_FIELDS]
+
+
+class ImpecOut(C.Structure):
+    _fields_ = [(f, _vp) for f in IMPEC_OUT_FIELDS]
 
 
 def out_shapes(nc: int) -> dict:
@@ -149,6 +163,9 @@ def lib():
     L.ocpf_flash_fim_regions.restype = C.c_int
     L.ocpf_measure_fp64_latency.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.ocpf_measure_fp64_latency.restype = C.c_int
+    L.ocpf_flash_impec.argtypes = [_vp, C.c_int64, C.POINTER(ImpecIn), C.POINTER(Skip), C.POINTER(ImpecOut),
+                                   C.c_int, _vp]
+    L.ocpf_flash_impec.restype = C.c_int
     _LIB = L
     return L
 

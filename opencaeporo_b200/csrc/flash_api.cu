@@ -15,14 +15,15 @@ namespace ocpf {
 #define OCPF_DECL_PLAIN(N)                                                                        \
     cudaError_t launch_plain_nc##N(const FluidConst& F, int64_t count, int64_t stride,            \
                                    const ocpf_fim_in& in, const ocpf_skip& sk,                     \
-                                   const ocpf_fim_out& out, unsigned blocks, int bs, cudaStream_t st);
+                                   const ocpf_fim_out& out, double* vj, bool impec, unsigned blocks, \
+                                   int bs, cudaStream_t st);
 OCPF_DECL_PLAIN(3)
 OCPF_DECL_PLAIN(6)
 OCPF_DECL_PLAIN(9)
 OCPF_DECL_PLAIN(12)
 
 using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const ocpf_fim_in&,
-                                      const ocpf_skip&, const ocpf_fim_out&, unsigned, int,
+                                      const ocpf_skip&, const ocpf_fim_out&, double*, bool, unsigned, int,
                                       cudaStream_t);
 
 // Batched-form launch sequences (flash_phased_ncN.cu).
@@ -335,7 +336,7 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
 
 static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, const ocpf_fim_in& in,
                        const ocpf_skip& sk, const ocpf_fim_out& out, cudaStream_t st, bool timed,
-                       int part = -1)
+                       int part = -1, double* vj = nullptr, bool impec = false)
 {
     if (count == 0) return OCPF_OK;
     cudaError_t e;
@@ -346,7 +347,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         const int64_t blocks = (count + bs - 1) / bs;
         if (blocks > 0x7fffffffLL) return OCPF_EINVAL;
         if (timed) cudaEventRecord(c->ev0, st);
-        e = k(c->fc, count, stride, in, sk, out, (unsigned)blocks, bs, st);
+        e = k(c->fc, count, stride, in, sk, out, vj, impec, (unsigned)blocks, bs, st);
         if (timed) cudaEventRecord(c->ev1, st);
     } else {
         int            nd = 0;
@@ -361,6 +362,8 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         args.out    = out;
         args.opts   = form >= OCPF_FORM_MIXED ? PH_MIXED : 0u;
         args.mlp    = c->mlp;
+        args.vj     = vj;
+        if (impec) args.opts |= PH_IMPEC;
         if (form == OCPF_FORM_FAST && c->mlp && c->fc.learn_on) args.opts |= PH_LEARN;
         if (part < 0) {
             const int rc = ensure_scratch(c, count);
@@ -391,6 +394,50 @@ extern "C" int ocpf_flash_fim(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in* in,
     if (sk) s = *sk;
     const int rc = launch_form(c, form, ncell, ncell, *in, s, *out, (cudaStream_t)stream, true);
     c->timed     = (rc == OCPF_OK && ncell > 0);
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+extern "C" int ocpf_flash_impec(ocpf_ctx* c, int64_t ncell, const ocpf_impec_in* in, ocpf_skip* sk,
+                                ocpf_impec_out* out, int form, void* stream)
+{
+    if (!c || ncell < 0) return OCPF_EINVAL;
+    if (ncell == 0) return OCPF_OK;
+    if (!in || !out || form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (!in->P || !in->T || !in->Ni || !in->lastNP || !in->xij) return OCPF_EINVAL;
+    if (!out->phaseNum || !out->phaseExist || !out->S || !out->Nt || !out->vf || !out->vfP || !out->vfi ||
+        !out->vj || !out->rho || !out->xi || !out->mu || !out->xij)
+        return OCPF_EINVAL;
+    if (c->fc.use_skip && (!sk || !sk->flag || !sk->minEig || !sk->P || !sk->T || !sk->z)) return OCPF_EINVAL;
+    ocpf_fim_in fin{};
+    fin.P      = in->P;
+    fin.T      = in->T;
+    fin.Ni     = in->Ni;
+    fin.lastNP = in->lastNP;
+    fin.xij    = in->xij;
+    ocpf_fim_out fo{};
+    fo.phaseNum   = out->phaseNum;
+    fo.phaseExist = out->phaseExist;
+    fo.S          = out->S;
+    fo.Nt         = out->Nt;
+    fo.vf         = out->vf;
+    fo.vfP        = out->vfP;
+    fo.vfi        = out->vfi;
+    fo.rho        = out->rho;
+    fo.xi         = out->xi;
+    fo.mu         = out->mu;
+    fo.xij        = out->xij;
+    fo.ePEC       = out->ePEC;
+    fo.ftype      = out->ftype;
+    fo.iters      = out->iters;
+    fo.status     = out->status;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    ocpf_skip s{};
+    if (sk) s = *sk;
+    const int rc = launch_form(c, form, ncell, ncell, fin, s, fo, (cudaStream_t)stream, true, -1, out->vj, true);
+    c->timed     = (rc == OCPF_OK);
     if (prev != c->device) cudaSetDevice(prev);
     return rc;
 }

@@ -37,9 +37,10 @@ struct FimCell : CellFlash<NC> {
 
     __device__ __forceinline__ explicit FimCell(const FluidConst& f) : Base(f) {}
 
-    // SkipStaAnaly::CalFtypeFIM / IfSkip, src/AcceleratePVT.cpp:54-120
+    // SkipStaAnaly::CalFtypeFIM / CalFtypeIMPEC / IfSkip,
+    // src/AcceleratePVT.cpp:54-120 (IMPEC has no two-phase warm type 2)
     __device__ __forceinline__ int cal_ftype(const double* Sin, bool skflag, double skEig, double skP,
-                                             double skT, const double* skz) const
+                                             double skT, const double* skz, bool impec = false) const
     {
         if (!F.use_skip) return 0;
         bool skip = false;
@@ -52,6 +53,7 @@ struct FimCell : CellFlash<NC> {
                 if (fabs(Ni[i] / Nh - skz[i]) >= skEig / 10) skip = false;
         }
         if (skip) return 1;
+        if (impec) return 0;
         if (lNP >= 2) {
             if (Sin[0] < 1e-4 || Sin[1] < 1e-4) return 0;
             return 2;
@@ -115,11 +117,12 @@ struct FimCell : CellFlash<NC> {
     }
 
     // Reads cell n_'s inputs (SoA with field stride `stride`) and decides the
-    // flash type: FlashFIM up to CalFtypeFIM (src/MixtureComp.cpp:501-515).
-    // Everything is read before any output is written, so the caller may pass
-    // the same xij and S arrays in and out.
+    // flash type: FlashFIM up to CalFtypeFIM (src/MixtureComp.cpp:501-515),
+    // or with `impec` FlashIMPEC up to CalFtypeIMPEC (:451-461; S is not
+    // read). Everything is read before any output is written, so the caller
+    // may pass the same xij and S arrays in and out.
     __device__ __forceinline__ void load_inputs(int64_t n_, int64_t stride, const ocpf_fim_in& in,
-                                                const ocpf_skip& sk)
+                                                const ocpf_skip& sk, bool impec = false)
     {
         const int64_t N = stride;
         auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
@@ -127,9 +130,11 @@ struct FimCell : CellFlash<NC> {
         const double Tin = in.T[n_];
 #pragma unroll
         for (int i = 0; i < NUMCOM; i++) Ni[i] = in.Ni[at(i)];
-        double Sin[2];
-        Sin[0]                = in.S[at(0)];
-        Sin[1]                = in.S[at(1)];
+        double Sin[2] = {0, 0};
+        if (!impec) {
+            Sin[0] = in.S[at(0)];
+            Sin[1] = in.S[at(1)];
+        }
         const uint32_t lastNP = in.lastNP[n_];
         lNP                   = lastNP > 0 ? (int)lastNP - 1 : 0;
         if (lNP == 2) {
@@ -162,16 +167,17 @@ struct FimCell : CellFlash<NC> {
 #pragma unroll
         for (int i = 0; i < NC; i++) zi[i] = Ni[i] / Nh;
 
-        ftype = cal_ftype(Sin, skflag, skEig, skP, skT, skz);
+        ftype = cal_ftype(Sin, skflag, skEig, skP, skT, skz, impec);
     }
 
-    // The whole FlashFIM of one cell on this thread.
+    // The whole FlashFIM (or, with `impec`, FlashIMPEC) of one cell on this
+    // thread.
     __device__ void run(int64_t n_, int64_t stride, const ocpf_fim_in& in, const ocpf_skip& sk,
-                        const ocpf_fim_out& out)
+                        const ocpf_fim_out& out, double* vjOut = nullptr, bool impec = false)
     {
-        load_inputs(n_, stride, in, sk);
+        load_inputs(n_, stride, in, sk, impec);
         this->phase_equilibrium();
-        finalize(n_, stride, sk, out);
+        finalize(n_, stride, sk, out, vjOut, impec);
     }
 
     // Everything after PhaseEquilibrium: CalFlash's property tail, the
@@ -179,7 +185,12 @@ struct FimCell : CellFlash<NC> {
     // the copy-out of PassFlashValue. Needs load_inputs' state, cal_ai_bi's
     // Ai/Bi and the equilibrium (NP, x, nu as phase fractions, Aj/Bj/Zj of
     // each phase, n from the split, flagSkip, ePEC, counters, status).
-    __device__ void finalize(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out)
+    // With `impec`, FlashIMPEC's tail instead (src/MixtureComp.cpp:462-491)
+    // and IsoT_IMPEC::PassFlashValue's outputs (src/OCPFluidMethod.cpp:
+    // 275-305): no dXsdXp and no property partials; the phase volumes vj go
+    // to vjOut.
+    __device__ void finalize(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out,
+                             double* vjOut = nullptr, bool impec = false)
     {
         const int64_t N = stride;
         auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
@@ -422,6 +433,15 @@ struct FimCell : CellFlash<NC> {
         out.vfP[n_]      = vfP;
 #pragma unroll
         for (int i = 0; i < NUMCOM; i++) out.vfi[at(i)] = vfi[i];
+        if (vjOut) {
+#pragma unroll
+            for (int j = 0; j < NPH; j++)
+                if (exist[j]) vjOut[at(j)] = vj[j];
+        }
+        if (impec) {
+            finalize_impec(n_, stride, sk, out, label, exist, xiC, rhoC, muC, bw, xiW, S, vf, vfP);
+            return;
+        }
 
         // ---- CaldXsdXpAPI02p, src/MixtureComp.cpp:4386-4493 (compact rows)
         const double vf2  = vf * vf;
@@ -606,6 +626,57 @@ struct FimCell : CellFlash<NC> {
         }
 
         // ---- diagnostics
+        if (!isfinite(vf) || !isfinite(vfP) || !isfinite(S[0]) || !isfinite(S[1])) status |= ST_NONFINITE;
+        if (out.ePEC) out.ePEC[n_] = this->ePEC;
+        if (out.ftype) out.ftype[n_] = (uint8_t)ftype;
+        if (out.iters) {
+            out.iters[at(0)] = this->it_ssmsta;
+            out.iters[at(1)] = this->it_nrsta;
+            out.iters[at(2)] = this->it_ssmsp;
+            out.iters[at(3)] = this->it_nrsp;
+            out.iters[at(4)] = this->it_rr;
+        }
+        if (out.status) out.status[n_] = status;
+    }
+
+    // FlashIMPEC's remaining outputs (IsoT_IMPEC::PassFlashValue): the
+    // per-phase properties of the existing phases, the water phase, the skip
+    // cache and the diagnostics.
+    __device__ void finalize_impec(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out,
+                                   const int* label, const bool* exist, const double* xiC, const double* rhoC,
+                                   const double* muC, double bw, double xiW, const double* S, double vf, double vfP)
+    {
+        const int64_t N = stride;
+        auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            if (j < NP) {
+                const int j1     = label[j];
+                out.rho[at(j1)]  = rhoC[j];
+                out.xi[at(j1)]   = xiC[j];
+                out.mu[at(j1)]   = muC[j];
+                if (out.nj) out.nj[at(j1)] = nu[j];
+#pragma unroll
+                for (int k = 0; k < NC; k++) out.xij[at(j1 * NUMCOM + k)] = x[j][k];
+                out.xij[at(j1 * NUMCOM + NC)] = 0.0;
+            }
+        }
+        out.rho[at(2)] = F.std_rho_w / bw;
+        out.xi[at(2)]  = xiW;
+        out.mu[at(2)]  = F.pvtw[3];
+        if (out.nj) out.nj[at(2)] = Ni[NC];
+#pragma unroll
+        for (int k = 0; k < NUMCOM; k++) out.xij[at(2 * NUMCOM + k)] = (k == NC) ? 1.0 : 0.0;
+        if (F.use_skip) {
+            if (flagSkip && ftype == 0) {
+                sk.minEig[n_] = skip_min_eig();
+                sk.P[n_]      = P;
+                sk.T[n_]      = T;
+#pragma unroll
+                for (int i = 0; i < NC; i++) sk.z[at(i)] = zi[i];
+            }
+            sk.flag[n_] = flagSkip ? 1u : 0u;
+        }
         if (!isfinite(vf) || !isfinite(vfP) || !isfinite(S[0]) || !isfinite(S[1])) status |= ST_NONFINITE;
         if (out.ePEC) out.ePEC[n_] = this->ePEC;
         if (out.ftype) out.ftype[n_] = (uint8_t)ftype;

@@ -125,11 +125,13 @@ struct Lists {
 // PhasedArgs::opts bits
 constexpr uint32_t PH_MIXED = 1u;  // FP32 successive substitution (flash_mixed.cuh)
 constexpr uint32_t PH_LEARN = 2u;  // learned initialiser for fresh cells (flash_learned.cuh)
+constexpr uint32_t PH_IMPEC = 4u;  // FlashIMPEC: IMPEC flash type and tail (FimCell::finalize)
 
 struct PhasedArgs {
     int64_t      count, stride;
     uint32_t     opts;
     const float* mlp;  // learned initialiser parameters (PH_LEARN)
+    double*      vj;   // phase volumes (PH_IMPEC), or null
     ocpf_fim_in  in;
     ocpf_skip    sk;
     ocpf_fim_out out;

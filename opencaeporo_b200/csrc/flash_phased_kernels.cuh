@@ -27,7 +27,7 @@ __device__ void init_body(const FluidConst& F, const PhasedArgs& a)
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
          c += (int64_t)gridDim.x * blockDim.x) {
         FimCell<NC> f(F);
-        f.load_inputs(c, a.stride, a.in, a.sk);
+        f.load_inputs(c, a.stride, a.in, a.sk, (a.opts & PH_IMPEC) != 0);
         f.cal_ai_bi();
         uint32_t meta = 0;
 #pragma unroll
@@ -911,7 +911,8 @@ __device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
          c += (int64_t)gridDim.x * blockDim.x) {
         FimCell<NC> f(F);
-        f.load_inputs(c, a.stride, a.in, a.sk);
+        const bool  impec = (a.opts & PH_IMPEC) != 0;
+        f.load_inputs(c, a.stride, a.in, a.sk, impec);
         uint32_t meta;
         load_book(f, S, c, meta);
 #pragma unroll
@@ -935,7 +936,7 @@ __device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
             f.n[0][i] = S.D(F_::n0 + i, c);
             f.n[1][i] = S.D(F_::n1 + i, c);
         }
-        f.finalize(c, a.stride, a.sk, a.out);
+        f.finalize(c, a.stride, a.sk, a.out, a.vj, impec);
     }
 }
 

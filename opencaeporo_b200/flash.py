@@ -156,6 +156,27 @@ class MixtureCompBatch:
                                   FORMS[form], C.c_void_p(stream.cuda_stream))
         check(rc, "ocpf_flash_fim")
 
+    def flash_impec(self, st: CellState, form: str = "plain", stream=None, diagnostics: bool = True,
+                    fresh: bool = False):
+        """Batched FlashIMPEC + IsoT_IMPEC::PassFlashValue (``ocpf_flash_impec``)
+        on device state: warm start from ``phaseNum`` and ``xij`` (or, with
+        ``fresh``, as new bulks); writes the IMPEC outputs into ``st.out``
+        and the phase volumes into ``st.out['vj']``."""
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        o = st.out
+        if "vj" not in o:
+            o["vj"] = torch.zeros((NPH, st.ncell), dtype=torch.float64, device=st.P.device)
+        fin_fim, sk, _ = self._structs(st, optional=diagnostics, fresh=fresh)
+        fin = _lib.ImpecIn(st.P.data_ptr(), st.T.data_ptr(), st.Ni.data_ptr(), fin_fim.lastNP, fin_fim.xij)
+        vals = []
+        for k in _lib.IMPEC_OUT_FIELDS:
+            vals.append(o[k].data_ptr() if (diagnostics or k not in _lib.OPTIONAL_OUT) else None)
+        rc = lib().ocpf_flash_impec(self._h, st.ncell, C.byref(fin), C.byref(sk), C.byref(_lib.ImpecOut(*vals)),
+                                    FORMS[form], C.c_void_p(stream.cuda_stream))
+        check(rc, "ocpf_flash_impec")
+
     def reserve(self, ncell: int):
         """Pre-allocates the batched forms' device scratch for ncell cells."""
         check(lib().ocpf_reserve(self._h, int(ncell)), "ocpf_reserve")

@@ -181,3 +181,63 @@ def summary(res: dict) -> str:
     parts += [f"{k}={res[k]:.1e}" for k in FLOAT_KEYS]
     parts += [f"{k}={res[k]}" for k in res if k.endswith("_mismatch") and k != "np_mismatch" and res[k]]
     return " ".join(parts)
+
+
+# ---------------------------------------------------------------- IMPEC flash
+IMPEC_CELL_FIELDS = ("S", "Nt", "vf", "vfP", "vfi")
+IMPEC_PHASE_FIELDS = ("rho", "xi", "mu", "vj")
+IMPEC_FLOAT_KEYS = IMPEC_CELL_FIELDS + IMPEC_PHASE_FIELDS + ("xij",)
+
+
+def impec_errors(gpu: dict, ref: dict, nc: int) -> dict:
+    """per_cell_errors for the outputs of IsoT_IMPEC::PassFlashValue (no
+    derivative blocks; the phase volumes vj)."""
+    ncom = nc + 1
+    n = len(ref["phaseNum"])
+    same = np.asarray(gpu["phaseNum"]).astype(np.int64) == np.asarray(ref["phaseNum"]).astype(np.int64)
+    same &= np.all(np.asarray(gpu["phaseExist"]).astype(np.int64) ==
+                   np.asarray(ref["phaseExist"]).astype(np.int64), axis=1)
+    exist = np.asarray(ref["phaseExist"]).astype(bool)
+    out = {"same": same}
+
+    def field_err(g, o, mask=None):
+        g = np.asarray(g, dtype=np.float64).reshape(n, -1)
+        o = np.asarray(o, dtype=np.float64).reshape(n, -1)
+        m = np.ones_like(o, dtype=bool) if mask is None else mask
+        fin = np.isfinite(o) & m
+        scale = np.max(np.abs(o[fin])) if fin.any() else 1.0
+        den = np.maximum(np.maximum(np.abs(o), 1e-12 * scale), 1e-300)
+        r = np.abs(g - o) / den
+        r[~np.isfinite(o) & ~np.isfinite(g)] = 0.0
+        r[~m] = 0.0
+        e = np.max(r, axis=1) if r.shape[1] else np.zeros(n)
+        e[~same] = np.nan
+        return e
+
+    for k in IMPEC_CELL_FIELDS:
+        out[k] = field_err(gpu[k], ref[k])
+    for k in IMPEC_PHASE_FIELDS:
+        out[k] = field_err(gpu[k], ref[k], exist)
+    out["xij"] = field_err(gpu["xij"], ref["xij"], np.repeat(exist, ncom, axis=1))
+    return out
+
+
+def check_impec(gpu: dict, ref: dict, nc: int, noise: dict = None, fragile=None, tol: float = 1e-8,
+                factor: float = 10.0) -> dict:
+    """check() for the IMPEC outputs."""
+    e = impec_errors(gpu, ref, nc)
+    n = len(e["same"])
+    frag = np.zeros(n, bool) if fragile is None else np.asarray(fragile, bool)
+    bad_np = np.nonzero(~e["same"] & ~frag)[0]
+    worst, ok = {}, len(bad_np) == 0
+    for k in IMPEC_FLOAT_KEYS:
+        allowed = np.full(n, tol)
+        if noise is not None and k in noise:
+            allowed = np.maximum(allowed, factor * np.nan_to_num(np.asarray(noise[k]), nan=0.0))
+        ratio = np.where(e["same"], e[k] / allowed, 0.0)
+        i = int(np.nanargmax(ratio)) if n else 0
+        worst[k] = (float(ratio[i]) if n else 0.0, i)
+        if n and ratio[i] > 1.0:
+            ok = False
+    return {"ok": ok, "np_mismatch": bad_np, "np_mismatch_all": np.nonzero(~e["same"])[0], "worst": worst,
+            "errors": e}

@@ -121,6 +121,33 @@ def load(kind: str = "reference"):
     return lib
 
 
+def flash_impec(fluid, P, T, Ni, lastNP=None, xij=None, skip=None, nthreads: int = 0):
+    """Runs one FlashIMPEC per cell through the compiled reference
+    (orc_flash_impec_batch; the restatement has no IMPEC entry). Arguments
+    as flash_fim without S; returns the IMPEC outputs (Bulk layout, absent
+    phases NaN) plus ``vj`` [n, 3]."""
+    lib = load("reference")
+    if not fluid.controls.use_skip:
+        fluid = fluid.with_controls(use_skip=True)  # see flash_fim
+        skip = None
+    n = int(np.asarray(P).shape[0])
+    vj = np.full((n, NP), np.nan)
+    b, f, arrays, skip, _keep = _prepare(fluid, P, T, Ni, None, lastNP, xij, skip)
+    secs = C.c_double(0.0)
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    lib.orc_flash_impec_batch.argtypes = [C.POINTER(OrcFluid), C.POINTER(OrcBatch), _dp, C.c_int,
+                                          C.POINTER(C.c_double)]
+    lib.orc_flash_impec_batch.restype = C.c_int
+    rc = lib.orc_flash_impec_batch(C.byref(f), C.byref(b), vj.ctypes.data_as(_dp), int(nthreads), C.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"orc_flash_impec_batch failed with {rc}")
+    arrays["vj"] = vj
+    arrays["seconds"] = secs.value
+    arrays["skip"] = skip
+    return arrays
+
+
 def _ptr(a, ct):
     return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
 
@@ -131,31 +158,12 @@ def new_skip(n: int, nc: int) -> dict:
             "T": np.zeros(n), "z": np.zeros((n, nc))}
 
 
-def flash_fim(kind: str, fluid, P, T, Ni, S=None, lastNP=None, xij=None, skip=None,
-              nthreads: int = 0):
-    """Runs one FlashFIM per cell through the chosen oracle.
-
-    P [n] psia, T [n] degF, Ni [n, numCom]; S [n,3], lastNP [n] and
-    xij [n,3,numCom] are the warm-start inputs (default: fresh cells,
-    lastNP = 0). ``skip`` (dict of arrays, updated in place) is the
-    SkipStaAnaly cache. Returns a dict of outputs in Bulk layout; entries of
-    absent phases are NaN. ``out["seconds"]`` is the flash-loop wall time.
-    """
-    lib = load(kind)
+def _prepare(fluid, P, T, Ni, S, lastNP, xij, skip):
+    """Batch struct, fluid struct, output arrays (NaN / -1 filled), skip cache
+    and the input arrays the struct points into (kept alive by the caller)."""
     nc = fluid.nc
     ncom = nc + 1
     n = int(np.asarray(P).shape[0])
-    if kind == "reference" and not fluid.controls.use_skip:
-        # The reference's FlashFIM sets SkipStaAnaly::flag[bulkId] after every
-        # flash (CalSkipForNextStep, src/MixtureComp.cpp:5253 ->
-        # include/AcceleratePVT.hpp:36) even when the skip option is off and
-        # the array was never allocated (src/MixtureComp.cpp:5130-5131): a
-        # write through an empty vector that crashes. Run it with the option
-        # on and a fresh cache (flag 0: no cell skips, every cell takes the
-        # full path), which gives the same flash; the cache it fills is
-        # discarded.
-        fluid = fluid.with_controls(use_skip=True)
-        skip = None
     P = np.ascontiguousarray(P, dtype=np.float64)
     T = np.ascontiguousarray(T, dtype=np.float64)
     Ni = np.ascontiguousarray(np.asarray(Ni, dtype=np.float64).reshape(n, ncom))
@@ -191,7 +199,32 @@ def flash_fim(kind: str, fluid, P, T, Ni, S=None, lastNP=None, xij=None, skip=No
     for name, ct in _BATCH_FIELDS[12:]:
         arr = out[name]
         setattr(b, name, arr.ctypes.data_as(ct))
-    f = make_orc_fluid(fluid)
+    return b, make_orc_fluid(fluid), out, skip, (P, T, Ni, S, lastNP, xij)
+
+
+def flash_fim(kind: str, fluid, P, T, Ni, S=None, lastNP=None, xij=None, skip=None,
+              nthreads: int = 0):
+    """Runs one FlashFIM per cell through the chosen oracle.
+
+    P [n] psia, T [n] degF, Ni [n, numCom]; S [n,3], lastNP [n] and
+    xij [n,3,numCom] are the warm-start inputs (default: fresh cells,
+    lastNP = 0). ``skip`` (dict of arrays, updated in place) is the
+    SkipStaAnaly cache. Returns a dict of outputs in Bulk layout; entries of
+    absent phases are NaN. ``out["seconds"]`` is the flash-loop wall time.
+    """
+    lib = load(kind)
+    if kind == "reference" and not fluid.controls.use_skip:
+        # The reference's FlashFIM sets SkipStaAnaly::flag[bulkId] after every
+        # flash (CalSkipForNextStep, src/MixtureComp.cpp:5253 ->
+        # include/AcceleratePVT.hpp:36) even when the skip option is off and
+        # the array was never allocated (src/MixtureComp.cpp:5130-5131): a
+        # write through an empty vector that crashes. Run it with the option
+        # on and a fresh cache (flag 0: no cell skips, every cell takes the
+        # full path), which gives the same flash; the cache it fills is
+        # discarded.
+        fluid = fluid.with_controls(use_skip=True)
+        skip = None
+    b, f, out, skip, _keep = _prepare(fluid, P, T, Ni, S, lastNP, xij, skip)
     secs = C.c_double(0.0)
     if nthreads <= 0:
         nthreads = os.cpu_count() or 1

@@ -111,6 +111,14 @@ typedef struct {
 int orc_flash_fim_batch(const orc_fluid* fluid, const orc_batch* batch,
                         int nthreads, double* seconds);
 
+/* Runs FlashIMPEC over the batch (src/MixtureComp.cpp:444-492) with the
+ * copy-out of IsoT_IMPEC::PassFlashValue (src/OCPFluidMethod.cpp:275-305):
+ * phaseNum, phaseExist, S, Nt, vf, vfP, vfi, rho, xi, mu, xij of the batch
+ * plus vj [n*3] (phase volumes); S_in is not read. The reference oracle
+ * only. */
+int orc_flash_impec_batch(const orc_fluid* fluid, const orc_batch* batch, double* vj,
+                          int nthreads, double* seconds);
+
 /* Identifies the implementation: "reference" or "port". */
 const char* orc_kind(void);
 

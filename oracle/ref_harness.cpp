@@ -193,6 +193,88 @@ void run_chunk(const orc_fluid& f, const orc_batch& b, int64_t lo, int64_t hi,
 
 } // namespace
 
+// FlashIMPEC over cells [lo, hi) with IsoT_IMPEC::PassFlashValue's copy-out
+// (src/OCPFluidMethod.cpp:264-305).
+void run_chunk_impec(const orc_fluid& f, const orc_batch& b, double* vjout, int64_t lo, int64_t hi,
+                     double* secs)
+{
+    const int nc      = f.nc;
+    const int numCom  = nc + 1;
+    const int np      = 3;
+    const int64_t cnt = hi - lo;
+    if (cnt <= 0) {
+        *secs = 0;
+        return;
+    }
+    ParamReservoir rs;
+    make_param(f, rs);
+    MixtureComp mc(rs, 0);
+    mc.std_RhoW = f.std_rho_w;
+    OptionalFeatures of;
+    of.skipStaAnaly.SetUseSkip(f.use_skip ? OCP_TRUE : OCP_FALSE);
+    mc.SetupOptionalFeatures(of, static_cast<OCP_USI>(cnt));
+    SkipStaAnaly& sk = of.skipStaAnaly;
+    if (f.use_skip) {
+        for (int64_t c = 0; c < cnt; c++) {
+            const int64_t n = lo + c;
+            sk.flag[c]      = b.skip_flag[n] ? OCP_TRUE : OCP_FALSE;
+            sk.minEigen[c]  = b.skip_minEig[n];
+            sk.P[c]         = b.skip_P[n];
+            sk.T[c]         = b.skip_T[n];
+            for (int i = 0; i < nc; i++) sk.zi[c * nc + i] = b.skip_z[n * nc + i];
+        }
+    }
+    std::vector<double> xin(np * numCom), Nin(numCom);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int64_t c = 0; c < cnt; c++) {
+        const int64_t n = lo + c;
+        std::copy(b.xij_in + n * np * numCom, b.xij_in + (n + 1) * np * numCom, xin.begin());
+        std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, Nin.begin());
+        const OCP_ULL it0[5] = {mc.itersSSMSTA, mc.itersNRSTA, mc.itersSSMSP, mc.itersNRSP, mc.itersRR};
+        mc.FlashIMPEC(b.P[n], b.T[n], Nin.data(), static_cast<USI>(b.lastNP[n]), xin.data(),
+                      static_cast<OCP_USI>(c));
+        int pn = 0;
+        for (int j = 0; j < np; j++) {
+            b.S[n * np + j]          = mc.GetS(j);
+            const int ex             = mc.GetPhaseExist(j) ? 1 : 0;
+            b.phaseExist[n * np + j] = ex;
+            if (ex) {
+                pn++;
+                for (int i = 0; i < numCom; i++) b.xij[(n * np + j) * numCom + i] = mc.GetXij(j, i);
+                vjout[n * np + j]  = mc.GetVj(j);
+                b.rho[n * np + j]  = mc.GetRho(j);
+                b.xi[n * np + j]   = mc.GetXi(j);
+                b.mu[n * np + j]   = mc.GetMu(j);
+            }
+        }
+        b.phaseNum[n] = pn;
+        b.Nt[n]       = mc.GetNt();
+        b.vf[n]       = mc.GetVf();
+        b.vfP[n]      = mc.GetVfP();
+        for (int i = 0; i < numCom; i++) b.vfi[n * numCom + i] = mc.GetVfi(i);
+        b.ePEC[n]          = mc.GetErrorPEC();
+        b.ftype[n]         = static_cast<int32_t>(mc.ftype);
+        b.NPhc[n]          = static_cast<int32_t>(mc.NP);
+        b.iters[n * 5 + 0] = static_cast<int32_t>(mc.itersSSMSTA - it0[0]);
+        b.iters[n * 5 + 1] = static_cast<int32_t>(mc.itersNRSTA - it0[1]);
+        b.iters[n * 5 + 2] = static_cast<int32_t>(mc.itersSSMSP - it0[2]);
+        b.iters[n * 5 + 3] = static_cast<int32_t>(mc.itersNRSP - it0[3]);
+        b.iters[n * 5 + 4] = static_cast<int32_t>(mc.itersRR - it0[4]);
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    *secs   = std::chrono::duration<double>(t1 - t0).count();
+    if (f.use_skip) {
+        for (int64_t c = 0; c < cnt; c++) {
+            const int64_t n  = lo + c;
+            b.skip_flag[n]   = sk.flag[c] ? 1 : 0;
+            b.skip_minEig[n] = sk.minEigen[c];
+            b.skip_P[n]      = sk.P[c];
+            b.skip_T[n]      = sk.T[c];
+            for (int i = 0; i < nc; i++) b.skip_z[n * nc + i] = sk.zi[c * nc + i];
+        }
+    }
+}
+
 extern "C" int orc_flash_fim_batch(const orc_fluid* fluid, const orc_batch* batch,
                                    int nthreads, double* seconds)
 {
@@ -226,6 +308,31 @@ extern "C" int orc_flash_fim_batch(const orc_fluid* fluid, const orc_batch* batc
         (void)wall0;
         (void)wall1;
     }
+    return 0;
+}
+
+extern "C" int orc_flash_impec_batch(const orc_fluid* fluid, const orc_batch* batch, double* vj, int nthreads,
+                                     double* seconds)
+{
+    if (!fluid || !batch || !vj || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
+    if (nthreads < 1) nthreads = 1;
+    const int64_t n = batch->n;
+    if (n <= 0) {
+        if (seconds) *seconds = 0;
+        return 0;
+    }
+    if (nthreads > n) nthreads = static_cast<int>(n);
+    std::ios::iostate st = std::cout.rdstate();
+    std::cout.setstate(std::ios::failbit);
+    std::vector<double>      secs(nthreads, 0.0);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++) {
+        const int64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
+        th.emplace_back(run_chunk_impec, std::cref(*fluid), std::cref(*batch), vj, lo, hi, &secs[t]);
+    }
+    for (auto& x : th) x.join();
+    std::cout.clear(st);
+    if (seconds) *seconds = *std::max_element(secs.begin(), secs.end());
     return 0;
 }
 

@@ -49,6 +49,59 @@ def golden():
     return load_golden
 
 
+def load_golden_impec(name="impec_nc6"):
+    """(fluid, inputs, reference IMPEC outputs with their self-noise, fragile
+    mask) of the FlashIMPEC fixture."""
+    d = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    fl, _, _, _ = _fluid_only(d)
+    inp = {"P": d["in_P"], "T": d["in_T"], "Ni": d["in_Ni"], "lastNP": d["in_lastNP"].astype(np.int32),
+           "xij": d["in_xij"], "skip": {k: d[f"skipin_{k}"] for k in ("flag", "minEig", "P", "T", "z")}}
+    out = {k[4:]: d[k] for k in d.files if k.startswith("out_")}
+    out["skip"] = {k: d[f"skipout_{k}"] for k in ("flag", "minEig", "P", "T", "z")}
+    out["noise"] = {k[6:]: d[k].astype(np.float64) for k in d.files if k.startswith("noise_")}
+    return fl, inp, out, d["fragile"]
+
+
+def _fluid_only(d):
+    from opencaeporo_b200.fluid import Controls, Fluid
+    c = d["controls"]
+    ctl = Controls(rr_maxit=int(c[0]), rr_tol=c[1], ssmsta_maxit=int(c[2]), ssmsta_tol=c[3],
+                   ssmsta_eyt=c[4], nrsta_maxit=int(c[5]), nrsta_tol=c[6], ssmsp_maxit=int(c[7]),
+                   ssmsp_tol=c[8], nrsp_maxit=int(c[9]), nrsp_tol=c[10], use_skip=bool(c[11]))
+    nc = len(d["fluid_Tc"])
+    fl = Fluid(nc=nc, Tc=d["fluid_Tc"], Pc=d["fluid_Pc"], Vc=d["fluid_Vc"], MW=d["fluid_MW"],
+               Acf=d["fluid_Acf"], BIC=d["fluid_BIC"], OmegaA=d["fluid_OmegaA"],
+               OmegaB=d["fluid_OmegaB"], Vshift=d["fluid_Vshift"], LBCcoef=d["fluid_LBCcoef"],
+               pvtw=d["fluid_pvtw"], std_rho_w=float(d["fluid_std_rho_w"]), controls=ctl,
+               name=str(d["fluid_name"]))
+    return fl, None, None, None
+
+
+def run_gpu_impec(fl, inp, form="plain"):
+    """One FlashIMPEC of a fixture's inputs through ocpf_flash_impec on cuda:0."""
+    import torch
+    from opencaeporo_b200.flash import MixtureCompBatch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    m = MixtureCompBatch(fl)
+    n = len(inp["P"])
+    st = m.new_state(n)
+    st.load(inp["P"], inp["T"], inp["Ni"])
+    st.out["phaseNum"].copy_(torch.as_tensor(inp["lastNP"].astype(np.int32)))
+    ncom = fl.nc + 1
+    st.out["xij"].copy_(torch.as_tensor(np.ascontiguousarray(inp["xij"].reshape(n, 3 * ncom).T)))
+    sk = inp["skip"]
+    st.skip["flag"].copy_(torch.as_tensor(sk["flag"].astype(np.int32)))
+    for k in ("minEig", "P", "T"):
+        st.skip[k].copy_(torch.as_tensor(np.asarray(sk[k], dtype=np.float64)))
+    st.skip["z"].copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(sk["z"]).T)))
+    m.flash_impec(st, form=form)
+    torch.cuda.synchronize()
+    res = st.to_host()
+    m.close()
+    return res
+
+
 def run_gpu(fl, inp, form="plain", init=None):
     """One flash of a fixture's inputs through the C ABI on cuda:0 (warm-start
     state and skip cache from the fixture); ``init``: a learned initialiser

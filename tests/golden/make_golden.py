@@ -122,12 +122,83 @@ def restart_case():
     run_case("restart_nc6", fl, inp, note="synthetic nc=6: bench-workload states with the most split restarts")
 
 
+def impec_case():
+    """FlashIMPEC on the 6-component fluid: a fresh step on 512 uniform states
+    (the first 256) and near-envelope states (the rest), then a warm second
+    step from the first step's phase counts, compositions and skip cache with
+    P and Ni perturbed (skip hits, warm two-phase starts, relaxed stability);
+    the fixture holds the second step, its warm-start inputs and the
+    reference's IMPEC outputs, with the fragile mask and self-noise of
+    run_case."""
+    from oracle import compare as CMP
+    fl = synthetic_fluid(6, 1234)
+
+    def pc(P, T, Ni):
+        return O.flash_fim("reference", fl, P, T, Ni, nthreads=8)["NPhc"]
+
+    a = synth.uniform_states(fl, 256, 77)
+    b = synth.near_envelope_states(fl, 256, 78, pc)
+    inp = {k: np.concatenate([a[k], b[k]]) for k in ("P", "T", "Ni")}
+    n = 512
+    skip = O.new_skip(n, fl.nc)
+    s1 = O.flash_impec(fl, inp["P"], inp["T"], inp["Ni"], skip=skip, nthreads=8)
+    rng = np.random.default_rng(11)
+    scale = np.where(rng.uniform(size=n) < 0.5, 1e-4, 3e-2)
+    P2 = inp["P"] * (1 + scale * rng.uniform(-1, 1, n))
+    N2 = inp["Ni"] * (1 + scale[:, None] * rng.uniform(-1, 1, inp["Ni"].shape))
+    lastNP = s1["phaseNum"].astype(np.int32)
+    xij = np.nan_to_num(s1["xij"], nan=0.0)
+    skip_in = {k: v.copy() for k, v in skip.items()}
+
+    def run(P, T, Ni):
+        sk = {k: v.copy() for k, v in skip_in.items()}
+        return O.flash_impec(fl, P, T, Ni, lastNP=lastNP, xij=xij, skip=sk, nthreads=8), sk
+
+    r, skip_out = run(P2, inp["T"], N2)
+    frag = np.zeros(n, bool)
+    noise = {k: np.zeros(n) for k in CMP.IMPEC_FLOAT_KEYS}
+    eps = 2.0 ** -50
+    prng = np.random.default_rng(7)
+    for trial in range(6):
+        P, T, Ni = P2.copy(), inp["T"].copy(), N2.copy()
+        sgn = 1 if trial % 2 == 0 else -1
+        if trial < 2:
+            P *= 1 + sgn * eps
+        elif trial < 4:
+            T = T + sgn * eps * np.maximum(np.abs(T), 1.0)
+        else:
+            Ni = Ni * (1 + eps * prng.choice([-1.0, 1.0], size=Ni.shape))
+        rr, _ = run(P, T, Ni)
+        frag |= rr["phaseNum"] != r["phaseNum"]
+        e = CMP.impec_errors(rr, r, fl.nc)
+        for k in CMP.IMPEC_FLOAT_KEYS:
+            noise[k] = np.fmax(noise[k], np.nan_to_num(e[k], nan=0.0))
+    d = fluid_arrays(fl)
+    d["note"] = np.array("FlashIMPEC, second step: warm start from a first step, P and Ni perturbed")
+    d["in_P"], d["in_T"], d["in_Ni"] = P2, inp["T"], N2
+    d["in_lastNP"], d["in_xij"] = lastNP, xij
+    for k, v in skip_in.items():
+        d[f"skipin_{k}"] = v
+    for k, v in skip_out.items():
+        d[f"skipout_{k}"] = v
+    for k in ("phaseNum", "phaseExist", "S", "Nt", "vf", "vfP", "vfi", "vj", "rho", "xi", "mu", "xij",
+              "ePEC", "ftype", "NPhc", "iters"):
+        d[f"out_{k}"] = r[k]
+    d["fragile"] = frag
+    for k, v in noise.items():
+        d[f"noise_{k}"] = v.astype(np.float32)
+    path = os.path.join(HERE, "impec_nc6.npz")
+    np.savez_compressed(path, **d)
+    print(f"impec_nc6: n={n} two-phase={np.mean(r['NPhc'] == 2):.3f} ftype={np.bincount(r['ftype'], minlength=3)} "
+          f"fragile={frag.sum()} size={os.path.getsize(path) / 1e6:.2f} MB")
+
+
 def main(only=()):
     if not O.available("reference"):
         raise SystemExit("oracle/_ref/libocpref.so missing: run `make -C oracle ref` first")
     if only:
         for name in only:
-            {"restart_nc6": restart_case}[name]()
+            {"restart_nc6": restart_case, "impec_nc6": impec_case}[name]()
         return
 
     # 1) SPE5 fluid (examples/spe5/EGOIL.in) at 160 degF, the deck's initial composition
@@ -179,6 +250,9 @@ def main(only=()):
 
     # 6) cells with long split-restart chains
     restart_case()
+
+    # 7) the IMPEC flash, warm-started
+    impec_case()
 
 
 if __name__ == "__main__":

@@ -269,3 +269,22 @@ def test_graph_replay_equals_direct_launch():
         for k, v in outs[0].items():
             if isinstance(v, np.ndarray):
                 np.testing.assert_array_equal(v, o[k], err_msg=k)
+
+
+@pytest.mark.parametrize("form", ["plain", "batched", "mixed"])
+def test_impec_matches_reference_golden(form):
+    """ocpf_flash_impec (FlashIMPEC + IsoT_IMPEC::PassFlashValue) on a
+    warm-started second step against the reference's outputs: identical
+    phase counts except knife-edge cells, flash types and skip cache, every
+    output (S, Nt, vf, vfP, vfi, vj, rho, xi, mu, xij) within 1e-8 relative
+    or 10x the reference's own 1-ulp sensitivity."""
+    from conftest import load_golden_impec, run_gpu_impec
+    fl, inp, ref, fragile = load_golden_impec()
+    got = run_gpu_impec(fl, inp, form=form)
+    chk = CMP.check_impec(got, ref, fl.nc, noise=ref["noise"], fragile=fragile)
+    assert chk["ok"], f"{form}: np_mismatch={list(chk['np_mismatch'])} worst={chk['worst']}"
+    same = (got["phaseNum"] == ref["phaseNum"]) & ~fragile
+    assert np.array_equal(got["ftype"][same], ref["ftype"][same])
+    assert set(np.unique(ref["ftype"])) == {0, 1}
+    sg, sr = got["skip"], ref["skip"]
+    assert np.array_equal(sg["flag"][same].astype(int), sr["flag"][same].astype(int))

@@ -114,3 +114,20 @@ def test_reference_with_skip_option_off():
     b = O.flash_fim("port", fl, P, T, Ni, nthreads=2)
     assert np.array_equal(a["NPhc"], b["NPhc"])
     assert np.array_equal(a["ftype"], np.zeros(64, np.int32))
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SRC), reason="reference sources not present")
+def test_reference_reproduces_impec_golden():
+    """The compiled reference's FlashIMPEC, rebuilt here, reproduces the
+    IMPEC fixture (guards the fixture and the IMPEC harness)."""
+    import subprocess
+    from conftest import load_golden_impec
+    subprocess.check_call(["make", "-s", "-C", os.path.join(os.path.dirname(O.__file__)), "ref"])
+    fl, inp, ref, _ = load_golden_impec()
+    skip = {k: np.array(v, copy=True) for k, v in inp["skip"].items()}
+    got = O.flash_impec(fl, inp["P"], inp["T"], inp["Ni"], lastNP=inp["lastNP"], xij=inp["xij"], skip=skip,
+                        nthreads=4)
+    e = CMP.impec_errors(got, ref, fl.nc)
+    assert e["same"].all()
+    for k in CMP.IMPEC_FLOAT_KEYS:
+        assert np.nanmax(e[k]) == 0.0, k
