@@ -182,6 +182,19 @@ typedef struct {
     uint16_t* status;
 } ocpf_impec_out;
 
+/* The initial state InitFlashFIM / InitFlashIMPEC take per cell
+ * (src/MixtureComp.cpp:261-267, :195-201, as IsoT_FIM::InitFlash and
+ * IsoT_IMPEC::InitFlash pass the Bulk arrays, src/OCPFluidMethod.cpp:
+ * 1095-1106, 251-262). The bubble-point pressure Pb the reference passes is
+ * not used by the compositional flash and has no field. */
+typedef struct {
+    const double* P;     /* [ncell] psia */
+    const double* T;     /* [ncell] degF */
+    const double* S;     /* [numPhase][ncell] initial saturations; S_w (the last) is read */
+    const double* Vpore; /* [ncell] pore volume (Bulk::rockVp), ft3 */
+    const double* zi;    /* [numCom][ncell] initial mole fractions; the water entry is not read */
+} ocpf_init_in;
+
 typedef struct ocpf_ctx ocpf_ctx;
 
 /* Library version string. */
@@ -249,6 +262,26 @@ int ocpf_flash_fim_noalloc(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, 
  * asynchrony as ocpf_flash_fim. */
 int ocpf_flash_impec(ocpf_ctx* ctx, int64_t ncell, const ocpf_impec_in* in, ocpf_skip* skip,
                      ocpf_impec_out* out, int form, void* stream);
+
+/* Batched MixtureComp::InitFlashFIM + IsoT_FIM::PassFlashValue over ncell
+ * cells (src/MixtureComp.cpp:261-353, src/OCPFluidMethod.cpp:1095-1106): a
+ * full flash of z (strict stability, no skip test, no warm start), the
+ * hydrocarbon moles Nh = Vpore (1 - S_w) / vf and the water moles
+ * Vpore S_w xi_w that fill the pore volume, then FlashFIM's derivatives and
+ * outputs. Ni [numCom][ncell] receives the moles (what IsoT_FIM::InitFlash
+ * copies back into Bulk::Ni); it may alias in->zi, and out->S may alias
+ * in->S. The skip cache is written as FlashFIM writes it. Forms and
+ * asynchrony as ocpf_flash_fim. As in the reference, out->nj of a
+ * hydrocarbon phase holds its mole fraction (CopyPhase runs before the
+ * moles are scaled); the other outputs are per cell as after FlashFIM. */
+int ocpf_init_flash_fim(ocpf_ctx* ctx, int64_t ncell, const ocpf_init_in* in, ocpf_skip* skip, double* Ni,
+                        ocpf_fim_out* out, int form, void* stream);
+
+/* Batched MixtureComp::InitFlashIMPEC + IsoT_IMPEC::PassFlashValue
+ * (src/MixtureComp.cpp:195-259, src/OCPFluidMethod.cpp:251-262): as
+ * ocpf_init_flash_fim with the IMPEC outputs of ocpf_flash_impec. */
+int ocpf_init_flash_impec(ocpf_ctx* ctx, int64_t ncell, const ocpf_init_in* in, ocpf_skip* skip, double* Ni,
+                          ocpf_impec_out* out, int form, void* stream);
 
 /* Several PVT regions at once -- the batched counterpart of a Bulk whose
  * cells belong to different regions (flashCal[PVTNUM[n]] in

@@ -35,7 +35,7 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_measure_fma_peak", "ocpf_reserve", "ocpf_flash_fim_noalloc",
            "ocpf_mlp_param_count", "ocpf_mlp_forward", "ocpf_mlp_grad", "ocpf_mlp_adam",
            "ocpf_set_initializer", "ocpf_flash_fim_regions", "ocpf_measure_fp64_latency",
-           "ocpf_flash_impec")
+           "ocpf_flash_impec", "ocpf_init_flash_fim", "ocpf_init_flash_impec")
 
 _vp = C.c_void_p
 
@@ -86,6 +86,13 @@ class ImpecIn(C.Structure):
 
 class ImpecOut(C.Structure):
     _fields_ = [(f, _vp) for f in IMPEC_OUT_FIELDS]
+
+
+INIT_IN_FIELDS = ("P", "T", "S", "Vpore", "zi")
+
+
+class InitIn(C.Structure):
+    _fields_ = [(f, _vp) for f in INIT_IN_FIELDS]
 
 
 def out_shapes(nc: int) -> dict:
@@ -166,6 +173,12 @@ def lib():
     L.ocpf_flash_impec.argtypes = [_vp, C.c_int64, C.POINTER(ImpecIn), C.POINTER(Skip), C.POINTER(ImpecOut),
                                    C.c_int, _vp]
     L.ocpf_flash_impec.restype = C.c_int
+    L.ocpf_init_flash_fim.argtypes = [_vp, C.c_int64, C.POINTER(InitIn), C.POINTER(Skip), _vp, C.POINTER(FimOut),
+                                      C.c_int, _vp]
+    L.ocpf_init_flash_fim.restype = C.c_int
+    L.ocpf_init_flash_impec.argtypes = [_vp, C.c_int64, C.POINTER(InitIn), C.POINTER(Skip), _vp,
+                                        C.POINTER(ImpecOut), C.c_int, _vp]
+    L.ocpf_init_flash_impec.restype = C.c_int
     _LIB = L
     return L
 

@@ -15,7 +15,7 @@ namespace ocpf {
 #define OCPF_DECL_PLAIN(N)                                                                        \
     cudaError_t launch_plain_nc##N(const FluidConst& F, int64_t count, int64_t stride,            \
                                    const ocpf_fim_in& in, const ocpf_skip& sk,                     \
-                                   const ocpf_fim_out& out, double* vj, bool impec, unsigned blocks, \
+                                   const ocpf_fim_out& out, const FlashTail& tail, unsigned blocks, \
                                    int bs, cudaStream_t st);
 OCPF_DECL_PLAIN(3)
 OCPF_DECL_PLAIN(6)
@@ -23,7 +23,7 @@ OCPF_DECL_PLAIN(9)
 OCPF_DECL_PLAIN(12)
 
 using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const ocpf_fim_in&,
-                                      const ocpf_skip&, const ocpf_fim_out&, double*, bool, unsigned, int,
+                                      const ocpf_skip&, const ocpf_fim_out&, const FlashTail&, unsigned, int,
                                       cudaStream_t);
 
 // Batched-form launch sequences (flash_phased_ncN.cu).
@@ -230,17 +230,53 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     return OCPF_OK;
 }
 
+// The outputs every FIM-tail entry point writes (IsoT_FIM::PassFlashValue's).
+static bool fim_out_ok(const ocpf_fim_out* o)
+{
+    return o && o->phaseNum && o->phaseExist && o->S && o->Nt && o->vf && o->vfP && o->vfi && o->rho && o->xi &&
+           o->mu && o->rhoP && o->xiP && o->muP && o->xij && o->rhox && o->xix && o->mux && o->dSec_dPri &&
+           o->bRowSizedSdP && o->pSderExist && o->pVnumCom;
+}
+
+// The outputs every IMPEC-tail entry point writes (IsoT_IMPEC::PassFlashValue's).
+static bool impec_out_ok(const ocpf_impec_out* o)
+{
+    return o && o->phaseNum && o->phaseExist && o->S && o->Nt && o->vf && o->vfP && o->vfi && o->vj && o->rho &&
+           o->xi && o->mu && o->xij;
+}
+
+static bool skip_ok(const ocpf_ctx* c, const ocpf_skip* sk)
+{
+    return !c->fc.use_skip || (sk && sk->flag && sk->minEig && sk->P && sk->T && sk->z);
+}
+
+// The IMPEC outputs as the FIM output record the kernels write through.
+static ocpf_fim_out impec_as_fim(const ocpf_impec_out& o)
+{
+    ocpf_fim_out fo{};
+    fo.phaseNum   = o.phaseNum;
+    fo.phaseExist = o.phaseExist;
+    fo.S          = o.S;
+    fo.Nt         = o.Nt;
+    fo.vf         = o.vf;
+    fo.vfP        = o.vfP;
+    fo.vfi        = o.vfi;
+    fo.rho        = o.rho;
+    fo.xi         = o.xi;
+    fo.mu         = o.mu;
+    fo.xij        = o.xij;
+    fo.ePEC       = o.ePEC;
+    fo.ftype      = o.ftype;
+    fo.iters      = o.iters;
+    fo.status     = o.status;
+    return fo;
+}
+
 static bool fim_args_ok(const ocpf_ctx* c, const ocpf_fim_in* in, const ocpf_skip* sk,
                         const ocpf_fim_out* o)
 {
-    if (!in || !o) return false;
-    if (!in->P || !in->T || !in->Ni || !in->S || !in->lastNP || !in->xij) return false;
-    if (!o->phaseNum || !o->phaseExist || !o->S || !o->Nt || !o->vf || !o->vfP || !o->vfi ||
-        !o->rho || !o->xi || !o->mu || !o->rhoP || !o->xiP || !o->muP || !o->xij || !o->rhox ||
-        !o->xix || !o->mux || !o->dSec_dPri || !o->bRowSizedSdP || !o->pSderExist || !o->pVnumCom)
-        return false;
-    if (c->fc.use_skip && (!sk || !sk->flag || !sk->minEig || !sk->P || !sk->T || !sk->z)) return false;
-    return true;
+    if (!in || !in->P || !in->T || !in->Ni || !in->S || !in->lastNP || !in->xij) return false;
+    return fim_out_ok(o) && skip_ok(c, sk);
 }
 
 static size_t scratch_bytes_per_cell(int nc)
@@ -336,7 +372,7 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
 
 static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, const ocpf_fim_in& in,
                        const ocpf_skip& sk, const ocpf_fim_out& out, cudaStream_t st, bool timed,
-                       int part = -1, double* vj = nullptr, bool impec = false)
+                       int part = -1, FlashTail tail = FlashTail{FM_FIM, nullptr, nullptr, nullptr})
 {
     if (count == 0) return OCPF_OK;
     cudaError_t e;
@@ -347,7 +383,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         const int64_t blocks = (count + bs - 1) / bs;
         if (blocks > 0x7fffffffLL) return OCPF_EINVAL;
         if (timed) cudaEventRecord(c->ev0, st);
-        e = k(c->fc, count, stride, in, sk, out, vj, impec, (unsigned)blocks, bs, st);
+        e = k(c->fc, count, stride, in, sk, out, tail, (unsigned)blocks, bs, st);
         if (timed) cudaEventRecord(c->ev1, st);
     } else {
         int            nd = 0;
@@ -362,8 +398,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         args.out    = out;
         args.opts   = form >= OCPF_FORM_MIXED ? PH_MIXED : 0u;
         args.mlp    = c->mlp;
-        args.vj     = vj;
-        if (impec) args.opts |= PH_IMPEC;
+        args.tail   = tail;
         if (form == OCPF_FORM_FAST && c->mlp && c->fc.learn_on) args.opts |= PH_LEARN;
         if (part < 0) {
             const int rc = ensure_scratch(c, count);
@@ -403,43 +438,73 @@ extern "C" int ocpf_flash_impec(ocpf_ctx* c, int64_t ncell, const ocpf_impec_in*
 {
     if (!c || ncell < 0) return OCPF_EINVAL;
     if (ncell == 0) return OCPF_OK;
-    if (!in || !out || form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (!in || form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
     if (!in->P || !in->T || !in->Ni || !in->lastNP || !in->xij) return OCPF_EINVAL;
-    if (!out->phaseNum || !out->phaseExist || !out->S || !out->Nt || !out->vf || !out->vfP || !out->vfi ||
-        !out->vj || !out->rho || !out->xi || !out->mu || !out->xij)
-        return OCPF_EINVAL;
-    if (c->fc.use_skip && (!sk || !sk->flag || !sk->minEig || !sk->P || !sk->T || !sk->z)) return OCPF_EINVAL;
+    if (!impec_out_ok(out) || !skip_ok(c, sk)) return OCPF_EINVAL;
     ocpf_fim_in fin{};
     fin.P      = in->P;
     fin.T      = in->T;
     fin.Ni     = in->Ni;
     fin.lastNP = in->lastNP;
     fin.xij    = in->xij;
-    ocpf_fim_out fo{};
-    fo.phaseNum   = out->phaseNum;
-    fo.phaseExist = out->phaseExist;
-    fo.S          = out->S;
-    fo.Nt         = out->Nt;
-    fo.vf         = out->vf;
-    fo.vfP        = out->vfP;
-    fo.vfi        = out->vfi;
-    fo.rho        = out->rho;
-    fo.xi         = out->xi;
-    fo.mu         = out->mu;
-    fo.xij        = out->xij;
-    fo.ePEC       = out->ePEC;
-    fo.ftype      = out->ftype;
-    fo.iters      = out->iters;
-    fo.status     = out->status;
+    const ocpf_fim_out fo = impec_as_fim(*out);
     int prev = 0;
     cudaGetDevice(&prev);
     if (prev != c->device) cudaSetDevice(c->device);
     ocpf_skip s{};
     if (sk) s = *sk;
-    const int rc = launch_form(c, form, ncell, ncell, fin, s, fo, (cudaStream_t)stream, true, -1, out->vj, true);
+    const FlashTail tail{FM_IMPEC, out->vj, nullptr, nullptr};
+    const int rc = launch_form(c, form, ncell, ncell, fin, s, fo, (cudaStream_t)stream, true, -1, tail);
     c->timed     = (rc == OCPF_OK);
     if (prev != c->device) cudaSetDevice(prev);
     return rc;
+}
+
+// InitFlashFIM / InitFlashIMPEC: the initial-state inputs as the FIM input
+// record (z in place of Ni, S for the water saturation) and the launch.
+static int launch_init(ocpf_ctx* c, int64_t ncell, const ocpf_init_in* in, ocpf_skip* sk, double* Ni,
+                       const ocpf_fim_out& fo, double* vj, int form, void* stream)
+{
+    ocpf_fim_in fin{};
+    fin.P  = in->P;
+    fin.T  = in->T;
+    fin.Ni = in->zi;
+    fin.S  = in->S;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    ocpf_skip s{};
+    if (sk) s = *sk;
+    const FlashTail tail{vj ? (FM_INIT | FM_IMPEC) : FM_INIT, vj, in->Vpore, Ni};
+    const int rc = launch_form(c, form, ncell, ncell, fin, s, fo, (cudaStream_t)stream, true, -1, tail);
+    c->timed     = (rc == OCPF_OK);
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+static bool init_in_ok(const ocpf_init_in* in)
+{
+    return in && in->P && in->T && in->S && in->Vpore && in->zi;
+}
+
+extern "C" int ocpf_init_flash_fim(ocpf_ctx* c, int64_t ncell, const ocpf_init_in* in, ocpf_skip* sk, double* Ni,
+                                   ocpf_fim_out* out, int form, void* stream)
+{
+    if (!c || ncell < 0) return OCPF_EINVAL;
+    if (ncell == 0) return OCPF_OK;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (!init_in_ok(in) || !Ni || !fim_out_ok(out) || !skip_ok(c, sk)) return OCPF_EINVAL;
+    return launch_init(c, ncell, in, sk, Ni, *out, nullptr, form, stream);
+}
+
+extern "C" int ocpf_init_flash_impec(ocpf_ctx* c, int64_t ncell, const ocpf_init_in* in, ocpf_skip* sk,
+                                     double* Ni, ocpf_impec_out* out, int form, void* stream)
+{
+    if (!c || ncell < 0) return OCPF_EINVAL;
+    if (ncell == 0) return OCPF_OK;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (!init_in_ok(in) || !Ni || !impec_out_ok(out) || !skip_ok(c, sk)) return OCPF_EINVAL;
+    return launch_init(c, ncell, in, sk, Ni, impec_as_fim(*out), out->vj, form, stream);
 }
 
 extern "C" int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,

@@ -7,6 +7,21 @@
 
 namespace ocpf {
 
+// Which of the reference's flash entry points a launch runs (bit flags):
+// FlashFIM, FlashIMPEC, InitFlashFIM (FM_INIT) or InitFlashIMPEC
+// (FM_INIT | FM_IMPEC).
+enum : int { FM_FIM = 0, FM_IMPEC = 1, FM_INIT = 2 };
+
+// The entry point of a launch and the arrays beyond ocpf_fim_in/out that it
+// reads or writes. With FM_INIT, ocpf_fim_in.Ni holds the mole fractions z
+// and ocpf_fim_in.S the initial saturations; lastNP and xij are not read.
+struct FlashTail {
+    int           mode;
+    double*       vj;     // [3][n] phase volumes (FM_IMPEC), or null
+    const double* vpore;  // [n] pore volumes, ft3 (FM_INIT)
+    double*       ni;     // [numCom][n] moles after the flash (FM_INIT); may alias in.Ni
+};
+
 template <int NC>
 struct FimCell : CellFlash<NC> {
     using Base = CellFlash<NC>;
@@ -34,6 +49,8 @@ struct FimCell : CellFlash<NC> {
     using Base::n;
     using Base::status;
     using Base::omb;
+
+    double Sw0 = 0, Vp0 = 0;  // initial water saturation and pore volume (FM_INIT)
 
     __device__ __forceinline__ explicit FimCell(const FluidConst& f) : Base(f) {}
 
@@ -118,16 +135,37 @@ struct FimCell : CellFlash<NC> {
 
     // Reads cell n_'s inputs (SoA with field stride `stride`) and decides the
     // flash type: FlashFIM up to CalFtypeFIM (src/MixtureComp.cpp:501-515),
-    // or with `impec` FlashIMPEC up to CalFtypeIMPEC (:451-461; S is not
-    // read). Everything is read before any output is written, so the caller
-    // may pass the same xij and S arrays in and out.
+    // with FM_IMPEC FlashIMPEC up to CalFtypeIMPEC (:451-461; S is not
+    // read), with FM_INIT InitFlashFIM / InitFlashIMPEC up to InitPTZ
+    // (:261-275, :195-209: flash type 0, no last phase count, z read as
+    // given). Everything is read before any output is written, so the caller
+    // may pass the same xij, S (and, with FM_INIT, z and Ni) arrays in and out.
     __device__ __forceinline__ void load_inputs(int64_t n_, int64_t stride, const ocpf_fim_in& in,
-                                                const ocpf_skip& sk, bool impec = false)
+                                                const ocpf_skip& sk, const FlashTail& tl)
     {
         const int64_t N = stride;
         auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
         const double Pin = in.P[n_];
         const double Tin = in.T[n_];
+        this->it_ssmsta = this->it_nrsta = this->it_ssmsp = this->it_nrsp = this->it_rr = 0;
+        status                                                                        = 0;
+        this->ssmsta_conflag = this->nrsta_conflag = this->ssmsp_conflag = this->nrsp_conflag = false;
+        this->ssmsta_realTol = this->nrsta_realTol = this->ssmsp_realTol = this->nrsp_realTol = 0;
+        this->Yt                                                                      = 0;
+        if (tl.mode & FM_INIT) {
+            // InitPTZ, include/MixtureComp.hpp:171-176; Nh is set by the tail
+            P  = Pin;
+            T  = Tin + CONV5;
+            Nh = 1;
+#pragma unroll
+            for (int i = 0; i < NC; i++) zi[i] = in.Ni[at(i)];
+            Sw0   = in.S[at(2)];
+            Vp0   = tl.vpore[n_];
+            lNP   = 0;
+            ftype = 0;
+            return;
+        }
+        const bool impec = (tl.mode & FM_IMPEC) != 0;
 #pragma unroll
         for (int i = 0; i < NUMCOM; i++) Ni[i] = in.Ni[at(i)];
         double Sin[2] = {0, 0};
@@ -152,11 +190,6 @@ struct FimCell : CellFlash<NC> {
             for (int i = 0; i < NC; i++) skz[i] = sk.z[at(i)];
         }
 
-        this->it_ssmsta = this->it_nrsta = this->it_ssmsp = this->it_nrsp = this->it_rr = 0;
-        status                                                                        = 0;
-        this->ssmsta_conflag = this->nrsta_conflag = this->ssmsp_conflag = this->nrsp_conflag = false;
-        this->ssmsta_realTol = this->nrsta_realTol = this->ssmsp_realTol = this->nrsp_realTol = 0;
-        this->Yt                                                                      = 0;
 
         // InitPTN, include/MixtureComp.hpp:177-184
         P  = Pin;
@@ -170,14 +203,14 @@ struct FimCell : CellFlash<NC> {
         ftype = cal_ftype(Sin, skflag, skEig, skP, skT, skz, impec);
     }
 
-    // The whole FlashFIM (or, with `impec`, FlashIMPEC) of one cell on this
-    // thread.
+    // The whole flash of one cell on this thread (FlashFIM, FlashIMPEC,
+    // InitFlashFIM or InitFlashIMPEC by tl.mode).
     __device__ void run(int64_t n_, int64_t stride, const ocpf_fim_in& in, const ocpf_skip& sk,
-                        const ocpf_fim_out& out, double* vjOut = nullptr, bool impec = false)
+                        const ocpf_fim_out& out, const FlashTail& tl)
     {
-        load_inputs(n_, stride, in, sk, impec);
+        load_inputs(n_, stride, in, sk, tl);
         this->phase_equilibrium();
-        finalize(n_, stride, sk, out, vjOut, impec);
+        finalize(n_, stride, sk, out, tl);
     }
 
     // Everything after PhaseEquilibrium: CalFlash's property tail, the
@@ -185,20 +218,28 @@ struct FimCell : CellFlash<NC> {
     // the copy-out of PassFlashValue. Needs load_inputs' state, cal_ai_bi's
     // Ai/Bi and the equilibrium (NP, x, nu as phase fractions, Aj/Bj/Zj of
     // each phase, n from the split, flagSkip, ePEC, counters, status).
-    // With `impec`, FlashIMPEC's tail instead (src/MixtureComp.cpp:462-491)
+    // With FM_IMPEC, FlashIMPEC's tail instead (src/MixtureComp.cpp:462-491)
     // and IsoT_IMPEC::PassFlashValue's outputs (src/OCPFluidMethod.cpp:
     // 275-305): no dXsdXp and no property partials; the phase volumes vj go
-    // to vjOut.
+    // to tl.vj. With FM_INIT, the tails of InitFlashFIM / InitFlashIMPEC
+    // (:276-353, :210-258): the properties are formed per mole of
+    // hydrocarbon, then Nh = Vpore (1 - S_w) / vf scales the phase moles and
+    // volumes, Ni = z Nh and N_w = Vpore S_w xi_w, and Ni goes to tl.ni.
     __device__ void finalize(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out,
-                             double* vjOut = nullptr, bool impec = false)
+                             const FlashTail& tl)
     {
         const int64_t N = stride;
         auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
+        const bool impec = (tl.mode & FM_IMPEC) != 0;
+        const bool init  = (tl.mode & FM_INIT) != 0;
 
-        // ---- CalFlash, src/MixtureComp.cpp:697-708 (after PhaseEquilibrium)
+        // ---- CalFlash, src/MixtureComp.cpp:697-708 (after PhaseEquilibrium);
+        // the initialisation keeps nu as phase fractions here
+        if (!init) {
 #pragma unroll
-        for (int j = 0; j < 2; j++)
-            if (j < NP) nu[j] *= Nh;
+            for (int j = 0; j < 2; j++)
+                if (j < NP) nu[j] *= Nh;
+        }
 
         double MW[2], vC[2], xiC[2], rhoC[2], muC[2], muA[2][5];
         // CalMW, src/MixtureComp.cpp:1147-1156
@@ -283,6 +324,23 @@ struct FimCell : CellFlash<NC> {
                 label[1] = 0;
             }
             exist[0] = exist[1] = true;
+        }
+        // CopyPhase's nj (src/MixtureComp.cpp:2386-2398): the phase moles, or
+        // in the initialisation the phase fractions (nu is rescaled after it)
+        const double njC[2] = {nu[0], nu[1]};
+        if (init) {
+            // InitFlashFIM, src/MixtureComp.cpp:282-297 (InitFlashIMPEC :216-229)
+            Nh = Vp0 * (1 - Sw0) / vf;
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                if (j < NP) {
+                    nu[j] *= Nh;
+                    vC[j] *= Nh;
+                }
+            }
+            vf *= Nh;
+#pragma unroll
+            for (int i = 0; i < NC; i++) Ni[i] = zi[i] * Nh;
         }
 
         // ---- CalVfiVfp_full02, src/MixtureComp.cpp:3911-3989
@@ -399,12 +457,14 @@ struct FimCell : CellFlash<NC> {
             }
         }
 
-        // ---- water, src/MixtureComp.cpp:517-546 (single-row PVTW: zero slopes)
-        const double Nw  = Ni[NC];
-        const double Nt  = Nh + Nw;
+        // ---- water, src/MixtureComp.cpp:517-546 (single-row PVTW: zero slopes);
+        // the initialisation fills the water from the pore volume (:314)
         const double bw  = F.pvtw[1] * (1 - F.pvtw[2] * (P - F.pvtw[0]));
         const double bwp = -F.pvtw[2] * F.pvtw[1];
         const double xiW = 1 / (CONV1 * bw);
+        if (init) Ni[NC] = Vp0 * Sw0 * xiW;
+        const double Nw  = Ni[NC];
+        const double Nt  = Nh + Nw;
         const double xiPW = -bwp / (bw * bw * CONV1);
         const double vw  = CONV1 * Nw * bw;
         vfi[NC]          = CONV1 * bw;
@@ -433,13 +493,17 @@ struct FimCell : CellFlash<NC> {
         out.vfP[n_]      = vfP;
 #pragma unroll
         for (int i = 0; i < NUMCOM; i++) out.vfi[at(i)] = vfi[i];
-        if (vjOut) {
+        if (tl.vj) {
 #pragma unroll
             for (int j = 0; j < NPH; j++)
-                if (exist[j]) vjOut[at(j)] = vj[j];
+                if (exist[j]) tl.vj[at(j)] = vj[j];
+        }
+        if (init && tl.ni) {
+#pragma unroll
+            for (int i = 0; i < NUMCOM; i++) tl.ni[at(i)] = Ni[i];
         }
         if (impec) {
-            finalize_impec(n_, stride, sk, out, label, exist, xiC, rhoC, muC, bw, xiW, S, vf, vfP);
+            finalize_impec(n_, stride, sk, out, label, exist, xiC, rhoC, muC, njC, bw, xiW, S, vf, vfP);
             return;
         }
 
@@ -560,7 +624,7 @@ struct FimCell : CellFlash<NC> {
                 out.xiP[at(j1)]  = xiP;
                 out.rhoP[at(j1)] = xiP * MW[j];
                 out.muP[at(j1)]  = muP;
-                if (out.nj) out.nj[at(j1)] = nu[j];
+                if (out.nj) out.nj[at(j1)] = njC[j];
 #pragma unroll
                 for (int k = 0; k < NC; k++) {
                     const int    o     = j1 * NUMCOM + k;
@@ -644,7 +708,8 @@ struct FimCell : CellFlash<NC> {
     // cache and the diagnostics.
     __device__ void finalize_impec(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out,
                                    const int* label, const bool* exist, const double* xiC, const double* rhoC,
-                                   const double* muC, double bw, double xiW, const double* S, double vf, double vfP)
+                                   const double* muC, const double* njC, double bw, double xiW, const double* S,
+                                   double vf, double vfP)
     {
         const int64_t N = stride;
         auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
@@ -655,7 +720,7 @@ struct FimCell : CellFlash<NC> {
                 out.rho[at(j1)]  = rhoC[j];
                 out.xi[at(j1)]   = xiC[j];
                 out.mu[at(j1)]   = muC[j];
-                if (out.nj) out.nj[at(j1)] = nu[j];
+                if (out.nj) out.nj[at(j1)] = njC[j];
 #pragma unroll
                 for (int k = 0; k < NC; k++) out.xij[at(j1 * NUMCOM + k)] = x[j][k];
                 out.xij[at(j1 * NUMCOM + NC)] = 0.0;

@@ -44,16 +44,12 @@ __device__ void learn_body(const FluidConst& F, const PhasedArgs& a, LearnSmem& 
             for (int j = 0; j < MLP_IO; j++) f[j] = 0.f;
             if (k < n) {
                 const int64_t c = a.L.item(L_FRESH, k);
-                double        Ni[NC], Nh = 0;
-#pragma unroll
-                for (int i = 0; i < NC; i++) {
-                    Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
-                    Nh += fabs(Ni[i]);
-                }
+                double        z[NC];
+                load_z<NC>(a, c, z);
                 f[0] = (float)log(a.in.P[c]);
                 f[1] = (float)a.in.T[c];
 #pragma unroll
-                for (int i = 0; i < NC; i++) f[2 + i] = (float)(Ni[i] / Nh);
+                for (int i = 0; i < NC; i++) f[2 + i] = (float)z[i];
 #pragma unroll
                 for (int j = 0; j < NC + 2; j++) f[j] = (f[j] - F.lin_mean[j]) / F.lin_scale[j];
             }

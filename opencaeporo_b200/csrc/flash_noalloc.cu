@@ -1,6 +1,7 @@
 // flash_noalloc.cu -- ocpf_flash_fim_noalloc: the batched flash with its
 // scratch in an array compiled into the library, for callers that cannot
 // allocate device memory (see include/ocp_flash.h).
+#include <cstring>
 #include <mutex>
 
 #include "flash_phased.cuh"
@@ -77,6 +78,8 @@ extern "C" int ocpf_flash_fim_noalloc(ocpf_ctx* ctx, int64_t ncell, const ocpf_f
     if (rc == OCPF_OK) {
         // same layout as the context scratch of ocpf_flash_fim, stride kMaxCells
         PhasedArgs a;
+        std::memset(&a, 0, sizeof(a));  // every field not set below is zero / null
+        a.tail   = FlashTail{FM_FIM, nullptr, nullptr, nullptr};
         a.count  = ncell;
         a.stride = ncell;
         a.in     = *in;

@@ -125,13 +125,12 @@ struct Lists {
 // PhasedArgs::opts bits
 constexpr uint32_t PH_MIXED = 1u;  // FP32 successive substitution (flash_mixed.cuh)
 constexpr uint32_t PH_LEARN = 2u;  // learned initialiser for fresh cells (flash_learned.cuh)
-constexpr uint32_t PH_IMPEC = 4u;  // FlashIMPEC: IMPEC flash type and tail (FimCell::finalize)
 
 struct PhasedArgs {
     int64_t      count, stride;
     uint32_t     opts;
     const float* mlp;  // learned initialiser parameters (PH_LEARN)
-    double*      vj;   // phase volumes (PH_IMPEC), or null
+    FlashTail    tail; // entry point (FlashFIM, FlashIMPEC, InitFlash*) and its extra arrays
     ocpf_fim_in  in;
     ocpf_skip    sk;
     ocpf_fim_out out;
@@ -139,23 +138,45 @@ struct PhasedArgs {
     Lists        L;
 };
 
-// Reads P, T and z of cell c into a CellFlash (InitPTN, bit for bit as
-// load_inputs forms them) and computes Ai, Bi.
+// z of cell c, bit for bit as FimCell::load_inputs forms it: Ni / Nh
+// (InitPTN), or in the initialisation the given mole fractions (InitPTZ).
+// Returns Nh (1 in the initialisation, where the tail sets it).
+template <int NC>
+__device__ __forceinline__ double load_z(const PhasedArgs& a, int64_t c, double* z)
+{
+    const int64_t N = a.stride;
+    if (a.tail.mode & FM_INIT) {
+#pragma unroll
+        for (int i = 0; i < NC; i++) z[i] = a.in.Ni[(int64_t)i * N + c];
+        return 1;
+    }
+    double Ni[NC], Nh = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        Ni[i] = a.in.Ni[(int64_t)i * N + c];
+        Nh += fabs(Ni[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < NC; i++) z[i] = Ni[i] / Nh;
+    return Nh;
+}
+
+// lNP of cell c: the last step's hydrocarbon phase count (none in the
+// initialisation).
+__device__ __forceinline__ int last_hc_np(const PhasedArgs& a, int64_t c)
+{
+    if (a.tail.mode & FM_INIT) return 0;
+    const uint32_t lastNP = a.in.lastNP[c];
+    return lastNP > 0 ? (int)lastNP - 1 : 0;
+}
+
+// Reads P, T and z of cell c into a CellFlash and computes Ai, Bi.
 template <int NC>
 __device__ __forceinline__ void load_ptz(CellFlash<NC>& f, const PhasedArgs& a, int64_t c)
 {
-    const int64_t N = a.stride;
-    f.P             = a.in.P[c];
-    f.T             = a.in.T[c] + CONV5;
-    double Ni[NC];
-#pragma unroll
-    for (int i = 0; i < NC; i++) Ni[i] = a.in.Ni[(int64_t)i * N + c];
-    double Nh = 0;
-#pragma unroll
-    for (int i = 0; i < NC; i++) Nh += fabs(Ni[i]);
-    f.Nh = Nh;
-#pragma unroll
-    for (int i = 0; i < NC; i++) f.zi[i] = Ni[i] / Nh;
+    f.P  = a.in.P[c];
+    f.T  = a.in.T[c] + CONV5;
+    f.Nh = load_z<NC>(a, c, f.zi);
     f.cal_ai_bi();
 }
 

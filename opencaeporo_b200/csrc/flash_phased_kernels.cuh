@@ -27,7 +27,7 @@ __device__ void init_body(const FluidConst& F, const PhasedArgs& a)
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
          c += (int64_t)gridDim.x * blockDim.x) {
         FimCell<NC> f(F);
-        f.load_inputs(c, a.stride, a.in, a.sk, (a.opts & PH_IMPEC) != 0);
+        f.load_inputs(c, a.stride, a.in, a.sk, a.tail);
         f.cal_ai_bi();
         uint32_t meta = 0;
 #pragma unroll
@@ -372,15 +372,9 @@ __device__ void s01_ssm_body(const FluidConst& F, const PhasedArgs& a, int k)
     int64_t         c    = a.L.take(list, n);
     auto load = [&]() {
         P = a.in.P[c];
-        double Ni[NC], Nh = 0;
+        load_z<NC>(a, c, z);
 #pragma unroll
         for (int i = 0; i < NC; i++) {
-            Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
-            Nh += fabs(Ni[i]);
-        }
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            z[i]   = Ni[i] / Nh;
             ks[i]  = S.D(F_::Ks + i, c);
             sA[i]  = S.D(F_::sA + i, c);
             Bi[i]  = S.D(F_::Bi + i, c);
@@ -484,9 +478,8 @@ __device__ void s01_end_body(const FluidConst& F, const PhasedArgs& a, int k)
             continue;
         }
         // lNP of the cell (the last phase count, water excluded)
-        const uint32_t lastNP = a.in.lastNP[c];
-        const int      lNP    = lastNP > 0 ? (int)lastNP - 1 : 0;
-        const int      tmpNP  = f.NP + (verdict ? 0 : 1);
+        const int lNP   = last_hc_np(a, c);
+        const int tmpNP = f.NP + (verdict ? 0 : 1);
         if (tmpNP != lNP) {
             f.flagSkip = false;
             store_book(f, S, c, meta);
@@ -521,8 +514,7 @@ __device__ void sp_prep_body(const FluidConst& F, const PhasedArgs& a, int r)
         if (!restart) {
             f.ssmsp_conflag = false;  // PhaseSplit, :1745-1749
             f.nrsp_conflag  = false;
-            const uint32_t lastNP = a.in.lastNP[c];
-            const int      lNP    = lastNP > 0 ? (int)lastNP - 1 : 0;
+            const int lNP = last_hc_np(a, c);
             if (lNP == 2) {
                 const int64_t N = a.stride;
 #pragma unroll
@@ -568,15 +560,9 @@ __device__ void sp_ssm_body(const FluidConst& F, const PhasedArgs& a, int r)
     int64_t         c     = a.L.take(list, n);
     auto load = [&]() {
         f.P = a.in.P[c];
-        double Ni[NC], Nh = 0;
+        load_z<NC>(a, c, f.zi);
 #pragma unroll
         for (int i = 0; i < NC; i++) {
-            Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
-            Nh += fabs(Ni[i]);
-        }
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            f.zi[i] = Ni[i] / Nh;
             f.Ks[i] = S.D(F_::Ks + i, c);
             f.sA[i] = S.D(F_::sA + i, c);
             f.Bi[i] = S.D(F_::Bi + i, c);
@@ -743,16 +729,9 @@ __device__ __forceinline__ void load_split_cell(CellFlash<NC>& f, const PhasedAr
     const StateBuf& S = a.S;
     load_book(f, S, c, meta);
     f.P      = a.in.P[c];
-    double Ni[NC], Nh = 0;
+    f.Nh     = load_z<NC>(a, c, f.zi);
 #pragma unroll
     for (int i = 0; i < NC; i++) {
-        Ni[i] = a.in.Ni[(int64_t)i * a.stride + c];
-        Nh += fabs(Ni[i]);
-    }
-    f.Nh = Nh;
-#pragma unroll
-    for (int i = 0; i < NC; i++) {
-        f.zi[i] = Ni[i] / Nh;
         f.sA[i] = S.D(F_::sA + i, c);
         f.Bi[i] = S.D(F_::Bi + i, c);
     }
@@ -911,8 +890,7 @@ __device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
     for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
          c += (int64_t)gridDim.x * blockDim.x) {
         FimCell<NC> f(F);
-        const bool  impec = (a.opts & PH_IMPEC) != 0;
-        f.load_inputs(c, a.stride, a.in, a.sk, impec);
+        f.load_inputs(c, a.stride, a.in, a.sk, a.tail);
         uint32_t meta;
         load_book(f, S, c, meta);
 #pragma unroll
@@ -936,7 +914,7 @@ __device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
             f.n[0][i] = S.D(F_::n0 + i, c);
             f.n[1][i] = S.D(F_::n1 + i, c);
         }
-        f.finalize(c, a.stride, a.sk, a.out, a.vj, impec);
+        f.finalize(c, a.stride, a.sk, a.out, a.tail);
     }
 }
 

@@ -9,19 +9,19 @@ namespace ocpf {
 __global__ void __launch_bounds__(128) k_flash_fim_plain_nc3(const __grid_constant__ FluidConst F,
                                                              int64_t count, int64_t stride,
                                                              const ocpf_fim_in in, const ocpf_skip sk,
-                                                             const ocpf_fim_out out, double* vj, bool impec)
+                                                             const ocpf_fim_out out, const FlashTail tail)
 {
     const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (n >= count) return;
     FimCell<3> c(F);
-    c.run(n, stride, in, sk, out, vj, impec);
+    c.run(n, stride, in, sk, out, tail);
 }
 
 cudaError_t launch_plain_nc3(const FluidConst& F, int64_t count, int64_t stride, const ocpf_fim_in& in,
-                              const ocpf_skip& sk, const ocpf_fim_out& out, double* vj, bool impec,
+                              const ocpf_skip& sk, const ocpf_fim_out& out, const FlashTail& tail,
                               unsigned blocks, int bs, cudaStream_t st)
 {
-    k_flash_fim_plain_nc3<<<blocks, bs, 0, st>>>(F, count, stride, in, sk, out, vj, impec);
+    k_flash_fim_plain_nc3<<<blocks, bs, 0, st>>>(F, count, stride, in, sk, out, tail);
     return cudaGetLastError();
 }
 

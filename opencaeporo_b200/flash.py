@@ -177,6 +177,43 @@ class MixtureCompBatch:
                                     FORMS[form], C.c_void_p(stream.cuda_stream))
         check(rc, "ocpf_flash_impec")
 
+    def init_flash(self, st: CellState, Vpore, S=None, impec: bool = False, form: str = "plain", stream=None,
+                   diagnostics: bool = True):
+        """IsoT_FIM::InitFlash (``ocpf_init_flash_fim``) or, with ``impec``,
+        IsoT_IMPEC::InitFlash (``ocpf_init_flash_impec``) on device state.
+        On entry ``st.Ni`` holds the initial mole fractions z and
+        ``st.out['S']`` (or ``S`` [n, 3], copied in first) the initial
+        saturations, of which S_w is read; ``Vpore`` [n] are the pore volumes
+        in ft3. On return ``st.Ni`` holds the moles that fill the pore
+        volume and ``st.out`` the FIM (or IMPEC, with ``vj``) outputs, as the
+        reference leaves Bulk::Ni and the Bulk arrays."""
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        o = st.out
+        dev = st.P.device
+        if S is not None:
+            o["S"].copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(S, dtype=np.float64).T)))
+        vp = torch.as_tensor(Vpore, dtype=torch.float64).to(dev).reshape(st.ncell).contiguous()
+        st.__dict__["_vpore"] = vp  # alive until the next call on this state
+        sk = _lib.Skip(*[st.skip[k].data_ptr() for k in _lib.SKIP_FIELDS])
+        fin = _lib.InitIn(st.P.data_ptr(), st.T.data_ptr(), o["S"].data_ptr(), vp.data_ptr(), st.Ni.data_ptr())
+        h, s = self._h, C.c_void_p(stream.cuda_stream)
+        if impec:
+            if "vj" not in o:
+                o["vj"] = torch.zeros((NPH, st.ncell), dtype=torch.float64, device=dev)
+            vals = [o[k].data_ptr() if (diagnostics or k not in _lib.OPTIONAL_OUT) else None
+                    for k in _lib.IMPEC_OUT_FIELDS]
+            rc = lib().ocpf_init_flash_impec(h, st.ncell, C.byref(fin), C.byref(sk), st.Ni.data_ptr(),
+                                             C.byref(_lib.ImpecOut(*vals)), FORMS[form], s)
+            check(rc, "ocpf_init_flash_impec")
+        else:
+            vals = [o[k].data_ptr() if (diagnostics or k not in _lib.OPTIONAL_OUT) else None
+                    for k in _lib.OUT_FIELDS]
+            rc = lib().ocpf_init_flash_fim(h, st.ncell, C.byref(fin), C.byref(sk), st.Ni.data_ptr(),
+                                           C.byref(_lib.FimOut(*vals)), FORMS[form], s)
+            check(rc, "ocpf_init_flash_fim")
+
     def reserve(self, ncell: int):
         """Pre-allocates the batched forms' device scratch for ncell cells."""
         check(lib().ocpf_reserve(self._h, int(ncell)), "ocpf_reserve")

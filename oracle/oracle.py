@@ -148,6 +148,43 @@ def flash_impec(fluid, P, T, Ni, lastNP=None, xij=None, skip=None, nthreads: int
     return arrays
 
 
+def init_flash(fluid, P, T, z, S, Vpore, impec: bool = False, skip=None, nthreads: int = 0):
+    """Runs one InitFlashFIM (or, with ``impec``, InitFlashIMPEC) per cell
+    through the compiled reference (orc_init_flash_batch; the restatement
+    has no initialisation entry). z [n, numCom] are the initial mole
+    fractions (water entry ignored), S [n, 3] the initial saturations (S_w
+    read), Vpore [n] the pore volumes in ft3. Returns the FIM outputs (or
+    the IMPEC ones plus ``vj``) and ``Ni`` [n, numCom], the moles the flash
+    object holds afterwards."""
+    lib = load("reference")
+    if not fluid.controls.use_skip:
+        fluid = fluid.with_controls(use_skip=True)  # see flash_fim
+        skip = None
+    n = int(np.asarray(P).shape[0])
+    ncom = fluid.nc + 1
+    vj = np.full((n, NP), np.nan)
+    Niout = np.full((n, ncom), np.nan)
+    Vp = np.ascontiguousarray(Vpore, dtype=np.float64).reshape(n)
+    b, f, arrays, skip, _keep = _prepare(fluid, P, T, z, S, None, None, skip)
+    secs = C.c_double(0.0)
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    lib.orc_init_flash_batch.argtypes = [C.POINTER(OrcFluid), C.POINTER(OrcBatch), _dp, C.c_int, _dp, _dp,
+                                         C.c_int, C.POINTER(C.c_double)]
+    lib.orc_init_flash_batch.restype = C.c_int
+    rc = lib.orc_init_flash_batch(C.byref(f), C.byref(b), Vp.ctypes.data_as(_dp), 1 if impec else 0,
+                                  Niout.ctypes.data_as(_dp), vj.ctypes.data_as(_dp), int(nthreads),
+                                  C.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"orc_init_flash_batch failed with {rc}")
+    if impec:
+        arrays["vj"] = vj
+    arrays["Ni"] = Niout
+    arrays["seconds"] = secs.value
+    arrays["skip"] = skip
+    return arrays
+
+
 def _ptr(a, ct):
     return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
 

@@ -119,6 +119,18 @@ int orc_flash_fim_batch(const orc_fluid* fluid, const orc_batch* batch,
 int orc_flash_impec_batch(const orc_fluid* fluid, const orc_batch* batch, double* vj,
                           int nthreads, double* seconds);
 
+/* Runs InitFlashFIM (impec == 0, src/MixtureComp.cpp:261-353) or
+ * InitFlashIMPEC (impec != 0, :195-259) over the batch, as IsoT_FIM::InitFlash
+ * (src/OCPFluidMethod.cpp:1095-1106) and IsoT_IMPEC::InitFlash (:251-262)
+ * make them: batch->Ni holds the initial mole fractions z [n*numCom] (water
+ * entry ignored), batch->S_in the initial saturations (only S_w is read),
+ * Vpore [n] the pore volumes (ft3); lastNP and xij_in are not read. Ni [n*numCom]
+ * receives the flash object's Ni afterwards (may alias batch->Ni). The
+ * copy-out is the FIM one (orc_flash_fim_batch's outputs) or, with impec, the
+ * IMPEC one with the phase volumes in vj [n*3]. The reference oracle only. */
+int orc_init_flash_batch(const orc_fluid* fluid, const orc_batch* batch, const double* Vpore, int impec,
+                         double* Ni, double* vj, int nthreads, double* seconds);
+
 /* Identifies the implementation: "reference" or "port". */
 const char* orc_kind(void);
 

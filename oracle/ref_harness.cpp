@@ -82,125 +82,111 @@ void make_param(const orc_fluid& f, ParamReservoir& rs)
     rs.density.activity = OCP_TRUE; // std_RhoW = RHOW_STD, overwritten below
 }
 
-void run_chunk(const orc_fluid& f, const orc_batch& b, int64_t lo, int64_t hi,
-               double* secs)
+// The per-bulk SkipStaAnaly cache of cells [lo, lo + cnt) in and out of the
+// flash object's own copy (src/AcceleratePVT.cpp).
+void skip_in(const orc_fluid& f, const orc_batch& b, SkipStaAnaly& sk, int64_t lo, int64_t cnt)
 {
-    const int nc      = f.nc;
-    const int numCom  = nc + 1;
-    const int np      = 3;
-    const int ncol    = numCom + 1;
-    const int maxLen  = ncol * ncol * np;
-    const int64_t cnt = hi - lo;
-    if (cnt <= 0) {
-        *secs = 0;
-        return;
-    }
-
-    ParamReservoir rs;
-    make_param(f, rs);
-    MixtureComp mc(rs, 0);
-    mc.std_RhoW = f.std_rho_w;
-    OptionalFeatures of;
-    of.skipStaAnaly.SetUseSkip(f.use_skip ? OCP_TRUE : OCP_FALSE);
-    mc.SetupOptionalFeatures(of, static_cast<OCP_USI>(cnt));
-    SkipStaAnaly& sk = of.skipStaAnaly;
-
-    if (f.use_skip) {
-        for (int64_t c = 0; c < cnt; c++) {
-            const int64_t n = lo + c;
-            sk.flag[c]      = b.skip_flag[n] ? OCP_TRUE : OCP_FALSE;
-            sk.minEigen[c]  = b.skip_minEig[n];
-            sk.P[c]         = b.skip_P[n];
-            sk.T[c]         = b.skip_T[n];
-            for (int i = 0; i < nc; i++) sk.zi[c * nc + i] = b.skip_z[n * nc + i];
-        }
-    }
-
-    std::vector<double> Sin(np), xin(np * numCom), Nin(numCom);
-    auto t0 = std::chrono::steady_clock::now();
+    if (!f.use_skip) return;
     for (int64_t c = 0; c < cnt; c++) {
         const int64_t n = lo + c;
-        std::copy(b.S_in + n * np, b.S_in + (n + 1) * np, Sin.begin());
-        std::copy(b.xij_in + n * np * numCom, b.xij_in + (n + 1) * np * numCom,
-                  xin.begin());
-        std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, Nin.begin());
-        const OCP_ULL it0[5] = {mc.itersSSMSTA, mc.itersNRSTA, mc.itersSSMSP,
-                                mc.itersNRSP, mc.itersRR};
-
-        mc.FlashFIM(b.P[n], b.T[n], Nin.data(), Sin.data(),
-                    static_cast<USI>(b.lastNP[n]), xin.data(),
-                    static_cast<OCP_USI>(c));
-
-        // copy-out, as IsoT_FIM::PassFlashValue does
-        int pn = 0, len = 0;
-        for (int j = 0; j < np; j++) {
-            b.S[n * np + j]          = mc.GetS(j);
-            const int ex             = mc.GetPhaseExist(j) ? 1 : 0;
-            b.phaseExist[n * np + j] = ex;
-            if (ex) {
-                pn++;
-                b.rho[n * np + j]  = mc.GetRho(j);
-                b.xi[n * np + j]   = mc.GetXi(j);
-                b.mu[n * np + j]   = mc.GetMu(j);
-                b.rhoP[n * np + j] = mc.GetRhoP(j);
-                b.xiP[n * np + j]  = mc.GetXiP(j);
-                b.muP[n * np + j]  = mc.GetMuP(j);
-                b.nj[n * np + j]   = mc.GetNj(j);
-                for (int i = 0; i < numCom; i++) {
-                    const int64_t o = (n * np + j) * numCom + i;
-                    b.xij[o]        = mc.GetXij(j, i);
-                    b.rhox[o]       = mc.GetRhoX(j, i);
-                    b.xix[o]        = mc.GetXiX(j, i);
-                    b.mux[o]        = mc.GetMuX(j, i);
-                }
-            }
-            b.pSderExist[n * np + j] = mc.GetPSderExist(j) ? 1 : 0;
-            b.pVnumCom[n * np + j]   = static_cast<int32_t>(mc.GetPVnumCom(j));
-            if (b.pSderExist[n * np + j]) len++;
-            len += b.pVnumCom[n * np + j];
-        }
-        b.phaseNum[n] = pn;
-        b.Nt[n]       = mc.GetNt();
-        b.vf[n]       = mc.GetVf();
-        b.vfP[n]      = mc.GetVfP();
-        for (int i = 0; i < numCom; i++) b.vfi[n * numCom + i] = mc.GetVfi(i);
-        b.bRowSizedSdP[n]              = len;
-        const std::vector<OCP_DBL>& dd = mc.GetDXsDXp();
-        std::copy(dd.begin(), dd.begin() + len * ncol, b.dSec_dPri + n * maxLen);
-        b.ePEC[n]          = mc.GetErrorPEC();
-        b.ftype[n]         = static_cast<int32_t>(mc.ftype);
-        b.NPhc[n]          = static_cast<int32_t>(mc.NP);
-        b.iters[n * 5 + 0] = static_cast<int32_t>(mc.itersSSMSTA - it0[0]);
-        b.iters[n * 5 + 1] = static_cast<int32_t>(mc.itersNRSTA - it0[1]);
-        b.iters[n * 5 + 2] = static_cast<int32_t>(mc.itersSSMSP - it0[2]);
-        b.iters[n * 5 + 3] = static_cast<int32_t>(mc.itersNRSP - it0[3]);
-        b.iters[n * 5 + 4] = static_cast<int32_t>(mc.itersRR - it0[4]);
-    }
-    auto t1 = std::chrono::steady_clock::now();
-    *secs   = std::chrono::duration<double>(t1 - t0).count();
-
-    if (f.use_skip) {
-        for (int64_t c = 0; c < cnt; c++) {
-            const int64_t n  = lo + c;
-            b.skip_flag[n]   = sk.flag[c] ? 1 : 0;
-            b.skip_minEig[n] = sk.minEigen[c];
-            b.skip_P[n]      = sk.P[c];
-            b.skip_T[n]      = sk.T[c];
-            for (int i = 0; i < nc; i++) b.skip_z[n * nc + i] = sk.zi[c * nc + i];
-        }
+        sk.flag[c]      = b.skip_flag[n] ? OCP_TRUE : OCP_FALSE;
+        sk.minEigen[c]  = b.skip_minEig[n];
+        sk.P[c]         = b.skip_P[n];
+        sk.T[c]         = b.skip_T[n];
+        for (int i = 0; i < f.nc; i++) sk.zi[c * f.nc + i] = b.skip_z[n * f.nc + i];
     }
 }
 
-} // namespace
-
-// FlashIMPEC over cells [lo, hi) with IsoT_IMPEC::PassFlashValue's copy-out
-// (src/OCPFluidMethod.cpp:264-305).
-void run_chunk_impec(const orc_fluid& f, const orc_batch& b, double* vjout, int64_t lo, int64_t hi,
-                     double* secs)
+void skip_out(const orc_fluid& f, const orc_batch& b, const SkipStaAnaly& sk, int64_t lo, int64_t cnt)
 {
-    const int nc      = f.nc;
-    const int numCom  = nc + 1;
-    const int np      = 3;
+    if (!f.use_skip) return;
+    for (int64_t c = 0; c < cnt; c++) {
+        const int64_t n  = lo + c;
+        b.skip_flag[n]   = sk.flag[c] ? 1 : 0;
+        b.skip_minEig[n] = sk.minEigen[c];
+        b.skip_P[n]      = sk.P[c];
+        b.skip_T[n]      = sk.T[c];
+        for (int i = 0; i < f.nc; i++) b.skip_z[n * f.nc + i] = sk.zi[c * f.nc + i];
+    }
+}
+
+// Copy-out of IsoT_FIM::PassFlashValue (src/OCPFluidMethod.cpp:1122-1187)
+// for cell n, plus nj.
+void copy_fim(const MixtureComp& mc, const orc_batch& b, int numCom, int64_t n)
+{
+    const int np     = 3;
+    const int ncol   = numCom + 1;
+    const int maxLen = ncol * ncol * np;
+    int       pn = 0, len = 0;
+    for (int j = 0; j < np; j++) {
+        b.S[n * np + j]          = mc.GetS(j);
+        const int ex             = mc.GetPhaseExist(j) ? 1 : 0;
+        b.phaseExist[n * np + j] = ex;
+        if (ex) {
+            pn++;
+            b.rho[n * np + j]  = mc.GetRho(j);
+            b.xi[n * np + j]   = mc.GetXi(j);
+            b.mu[n * np + j]   = mc.GetMu(j);
+            b.rhoP[n * np + j] = mc.GetRhoP(j);
+            b.xiP[n * np + j]  = mc.GetXiP(j);
+            b.muP[n * np + j]  = mc.GetMuP(j);
+            b.nj[n * np + j]   = mc.GetNj(j);
+            for (int i = 0; i < numCom; i++) {
+                const int64_t o = (n * np + j) * numCom + i;
+                b.xij[o]        = mc.GetXij(j, i);
+                b.rhox[o]       = mc.GetRhoX(j, i);
+                b.xix[o]        = mc.GetXiX(j, i);
+                b.mux[o]        = mc.GetMuX(j, i);
+            }
+        }
+        b.pSderExist[n * np + j] = mc.GetPSderExist(j) ? 1 : 0;
+        b.pVnumCom[n * np + j]   = static_cast<int32_t>(mc.GetPVnumCom(j));
+        if (b.pSderExist[n * np + j]) len++;
+        len += b.pVnumCom[n * np + j];
+    }
+    b.phaseNum[n] = pn;
+    b.Nt[n]       = mc.GetNt();
+    b.vf[n]       = mc.GetVf();
+    b.vfP[n]      = mc.GetVfP();
+    for (int i = 0; i < numCom; i++) b.vfi[n * numCom + i] = mc.GetVfi(i);
+    b.bRowSizedSdP[n]              = len;
+    const std::vector<OCP_DBL>& dd = mc.GetDXsDXp();
+    std::copy(dd.begin(), dd.begin() + len * ncol, b.dSec_dPri + n * maxLen);
+}
+
+// Copy-out of IsoT_IMPEC::PassFlashValue (src/OCPFluidMethod.cpp:275-305)
+// for cell n, the phase volumes into vjout.
+void copy_impec(const MixtureComp& mc, const orc_batch& b, double* vjout, int numCom, int64_t n)
+{
+    const int np = 3;
+    int       pn = 0;
+    for (int j = 0; j < np; j++) {
+        b.S[n * np + j]          = mc.GetS(j);
+        const int ex             = mc.GetPhaseExist(j) ? 1 : 0;
+        b.phaseExist[n * np + j] = ex;
+        if (ex) {
+            pn++;
+            for (int i = 0; i < numCom; i++) b.xij[(n * np + j) * numCom + i] = mc.GetXij(j, i);
+            vjout[n * np + j] = mc.GetVj(j);
+            b.rho[n * np + j] = mc.GetRho(j);
+            b.xi[n * np + j]  = mc.GetXi(j);
+            b.mu[n * np + j]  = mc.GetMu(j);
+        }
+    }
+    b.phaseNum[n] = pn;
+    b.Nt[n]       = mc.GetNt();
+    b.vf[n]       = mc.GetVf();
+    b.vfP[n]      = mc.GetVfP();
+    for (int i = 0; i < numCom; i++) b.vfi[n * numCom + i] = mc.GetVfi(i);
+}
+
+// Runs cells [lo, hi) of a batch on one flash object of its own: for each
+// cell `call(mc, n, c)` makes the reference's flash call (c: the cell's bulk
+// id within the object) and `copy(mc, n)` its copy-out; the diagnostics
+// (ePEC, flash type, hydrocarbon phase count, iteration counts) follow.
+template <class Call, class Copy>
+void run_cells(const orc_fluid& f, const orc_batch& b, int64_t lo, int64_t hi, double* secs, Call call, Copy copy)
+{
     const int64_t cnt = hi - lo;
     if (cnt <= 0) {
         *secs = 0;
@@ -214,44 +200,13 @@ void run_chunk_impec(const orc_fluid& f, const orc_batch& b, double* vjout, int6
     of.skipStaAnaly.SetUseSkip(f.use_skip ? OCP_TRUE : OCP_FALSE);
     mc.SetupOptionalFeatures(of, static_cast<OCP_USI>(cnt));
     SkipStaAnaly& sk = of.skipStaAnaly;
-    if (f.use_skip) {
-        for (int64_t c = 0; c < cnt; c++) {
-            const int64_t n = lo + c;
-            sk.flag[c]      = b.skip_flag[n] ? OCP_TRUE : OCP_FALSE;
-            sk.minEigen[c]  = b.skip_minEig[n];
-            sk.P[c]         = b.skip_P[n];
-            sk.T[c]         = b.skip_T[n];
-            for (int i = 0; i < nc; i++) sk.zi[c * nc + i] = b.skip_z[n * nc + i];
-        }
-    }
-    std::vector<double> xin(np * numCom), Nin(numCom);
+    skip_in(f, b, sk, lo, cnt);
     auto t0 = std::chrono::steady_clock::now();
     for (int64_t c = 0; c < cnt; c++) {
-        const int64_t n = lo + c;
-        std::copy(b.xij_in + n * np * numCom, b.xij_in + (n + 1) * np * numCom, xin.begin());
-        std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, Nin.begin());
+        const int64_t n      = lo + c;
         const OCP_ULL it0[5] = {mc.itersSSMSTA, mc.itersNRSTA, mc.itersSSMSP, mc.itersNRSP, mc.itersRR};
-        mc.FlashIMPEC(b.P[n], b.T[n], Nin.data(), static_cast<USI>(b.lastNP[n]), xin.data(),
-                      static_cast<OCP_USI>(c));
-        int pn = 0;
-        for (int j = 0; j < np; j++) {
-            b.S[n * np + j]          = mc.GetS(j);
-            const int ex             = mc.GetPhaseExist(j) ? 1 : 0;
-            b.phaseExist[n * np + j] = ex;
-            if (ex) {
-                pn++;
-                for (int i = 0; i < numCom; i++) b.xij[(n * np + j) * numCom + i] = mc.GetXij(j, i);
-                vjout[n * np + j]  = mc.GetVj(j);
-                b.rho[n * np + j]  = mc.GetRho(j);
-                b.xi[n * np + j]   = mc.GetXi(j);
-                b.mu[n * np + j]   = mc.GetMu(j);
-            }
-        }
-        b.phaseNum[n] = pn;
-        b.Nt[n]       = mc.GetNt();
-        b.vf[n]       = mc.GetVf();
-        b.vfP[n]      = mc.GetVfP();
-        for (int i = 0; i < numCom; i++) b.vfi[n * numCom + i] = mc.GetVfi(i);
+        call(mc, n, static_cast<OCP_USI>(c));
+        copy(mc, n);
         b.ePEC[n]          = mc.GetErrorPEC();
         b.ftype[n]         = static_cast<int32_t>(mc.ftype);
         b.NPhc[n]          = static_cast<int32_t>(mc.NP);
@@ -263,77 +218,125 @@ void run_chunk_impec(const orc_fluid& f, const orc_batch& b, double* vjout, int6
     }
     auto t1 = std::chrono::steady_clock::now();
     *secs   = std::chrono::duration<double>(t1 - t0).count();
-    if (f.use_skip) {
-        for (int64_t c = 0; c < cnt; c++) {
-            const int64_t n  = lo + c;
-            b.skip_flag[n]   = sk.flag[c] ? 1 : 0;
-            b.skip_minEig[n] = sk.minEigen[c];
-            b.skip_P[n]      = sk.P[c];
-            b.skip_T[n]      = sk.T[c];
-            for (int i = 0; i < nc; i++) b.skip_z[n * nc + i] = sk.zi[c * nc + i];
-        }
-    }
+    skip_out(f, b, sk, lo, cnt);
 }
 
-extern "C" int orc_flash_fim_batch(const orc_fluid* fluid, const orc_batch* batch,
-                                   int nthreads, double* seconds)
+// FlashFIM over cells [lo, hi): the calls of IsoT_FIM::CalFlash
+// (src/OCPFluidMethod.cpp:1108-1120).
+void run_chunk(const orc_fluid& f, const orc_batch& b, int64_t lo, int64_t hi, double* secs)
 {
-    if (!fluid || !batch || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
+    const int           numCom = f.nc + 1, np = 3;
+    std::vector<double> Sin(np), xin(np * numCom), Nin(numCom);
+    run_cells(
+        f, b, lo, hi, secs,
+        [&](MixtureComp& mc, int64_t n, OCP_USI c) {
+            std::copy(b.S_in + n * np, b.S_in + (n + 1) * np, Sin.begin());
+            std::copy(b.xij_in + n * np * numCom, b.xij_in + (n + 1) * np * numCom, xin.begin());
+            std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, Nin.begin());
+            mc.FlashFIM(b.P[n], b.T[n], Nin.data(), Sin.data(), static_cast<USI>(b.lastNP[n]), xin.data(), c);
+        },
+        [&](const MixtureComp& mc, int64_t n) { copy_fim(mc, b, numCom, n); });
+}
+
+// FlashIMPEC over cells [lo, hi): the calls of IsoT_IMPEC::CalFlash
+// (src/OCPFluidMethod.cpp:264-273).
+void run_chunk_impec(const orc_fluid& f, const orc_batch& b, double* vjout, int64_t lo, int64_t hi, double* secs)
+{
+    const int           numCom = f.nc + 1, np = 3;
+    std::vector<double> xin(np * numCom), Nin(numCom);
+    run_cells(
+        f, b, lo, hi, secs,
+        [&](MixtureComp& mc, int64_t n, OCP_USI c) {
+            std::copy(b.xij_in + n * np * numCom, b.xij_in + (n + 1) * np * numCom, xin.begin());
+            std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, Nin.begin());
+            mc.FlashIMPEC(b.P[n], b.T[n], Nin.data(), static_cast<USI>(b.lastNP[n]), xin.data(), c);
+        },
+        [&](const MixtureComp& mc, int64_t n) { copy_impec(mc, b, vjout, numCom, n); });
+}
+
+// InitFlashFIM or InitFlashIMPEC over cells [lo, hi): the calls of
+// IsoT_FIM::InitFlash (src/OCPFluidMethod.cpp:1095-1106) or
+// IsoT_IMPEC::InitFlash (:251-262). b.Ni holds the mole fractions z, S_in
+// the initial saturations; Ni receives the flash object's Ni afterwards.
+void run_chunk_init(const orc_fluid& f, const orc_batch& b, const double* Vpore, int impec, double* Niout,
+                    double* vjout, int64_t lo, int64_t hi, double* secs)
+{
+    const int           numCom = f.nc + 1, np = 3;
+    std::vector<double> Sin(np), zin(numCom);
+    run_cells(
+        f, b, lo, hi, secs,
+        [&](MixtureComp& mc, int64_t n, OCP_USI c) {
+            std::copy(b.S_in + n * np, b.S_in + (n + 1) * np, Sin.begin());
+            std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, zin.begin());
+            const OCP_DBL Pbb = 0;  // unused by MixtureComp
+            if (impec)
+                mc.InitFlashIMPEC(b.P[n], Pbb, b.T[n], Sin.data(), Vpore[n], zin.data(), c);
+            else
+                mc.InitFlashFIM(b.P[n], Pbb, b.T[n], Sin.data(), Vpore[n], zin.data(), c);
+            for (int i = 0; i < numCom; i++) Niout[n * numCom + i] = mc.GetNi(i);
+        },
+        [&](const MixtureComp& mc, int64_t n) {
+            if (impec)
+                copy_impec(mc, b, vjout, numCom, n);
+            else
+                copy_fim(mc, b, numCom, n);
+        });
+}
+
+// Runs `chunk(lo, hi, &secs)` over nthreads host threads with the
+// reference's console output muted; *seconds: the slowest thread's loop.
+template <class Chunk>
+int run_threads(int64_t n, int nthreads, double* seconds, Chunk chunk)
+{
     if (nthreads < 1) nthreads = 1;
-    const int64_t n = batch->n;
     if (n <= 0) {
         if (seconds) *seconds = 0;
         return 0;
     }
     if (nthreads > n) nthreads = static_cast<int>(n);
-
     // The reference prints from its constructor and from CheckSplit; mute it.
-    std::ios::iostate st = std::cout.rdstate();
-    std::cout.setstate(std::ios::failbit);
-
-    std::vector<double> secs(nthreads, 0.0);
-    std::vector<std::thread> th;
-    auto wall0 = std::chrono::steady_clock::now();
-    for (int t = 0; t < nthreads; t++) {
-        const int64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
-        th.emplace_back(run_chunk, std::cref(*fluid), std::cref(*batch), lo, hi,
-                        &secs[t]);
-    }
-    for (auto& x : th) x.join();
-    auto wall1 = std::chrono::steady_clock::now();
-    std::cout.clear(st);
-    if (seconds) {
-        // wall time of the slowest thread's flash loop
-        *seconds = *std::max_element(secs.begin(), secs.end());
-        (void)wall0;
-        (void)wall1;
-    }
-    return 0;
-}
-
-extern "C" int orc_flash_impec_batch(const orc_fluid* fluid, const orc_batch* batch, double* vj, int nthreads,
-                                     double* seconds)
-{
-    if (!fluid || !batch || !vj || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
-    if (nthreads < 1) nthreads = 1;
-    const int64_t n = batch->n;
-    if (n <= 0) {
-        if (seconds) *seconds = 0;
-        return 0;
-    }
-    if (nthreads > n) nthreads = static_cast<int>(n);
     std::ios::iostate st = std::cout.rdstate();
     std::cout.setstate(std::ios::failbit);
     std::vector<double>      secs(nthreads, 0.0);
     std::vector<std::thread> th;
     for (int t = 0; t < nthreads; t++) {
         const int64_t lo = n * t / nthreads, hi = n * (t + 1) / nthreads;
-        th.emplace_back(run_chunk_impec, std::cref(*fluid), std::cref(*batch), vj, lo, hi, &secs[t]);
+        th.emplace_back([&chunk, lo, hi, &secs, t]() { chunk(lo, hi, &secs[t]); });
     }
     for (auto& x : th) x.join();
     std::cout.clear(st);
     if (seconds) *seconds = *std::max_element(secs.begin(), secs.end());
     return 0;
+}
+
+} // namespace
+
+extern "C" int orc_flash_fim_batch(const orc_fluid* fluid, const orc_batch* batch, int nthreads, double* seconds)
+{
+    if (!fluid || !batch || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
+    return run_threads(batch->n, nthreads, seconds, [fluid, batch](int64_t lo, int64_t hi, double* s) {
+        run_chunk(*fluid, *batch, lo, hi, s);
+    });
+}
+
+extern "C" int orc_flash_impec_batch(const orc_fluid* fluid, const orc_batch* batch, double* vj, int nthreads,
+                                     double* seconds)
+{
+    if (!fluid || !batch || !vj || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
+    return run_threads(batch->n, nthreads, seconds, [fluid, batch, vj](int64_t lo, int64_t hi, double* s) {
+        run_chunk_impec(*fluid, *batch, vj, lo, hi, s);
+    });
+}
+
+extern "C" int orc_init_flash_batch(const orc_fluid* fluid, const orc_batch* batch, const double* Vpore, int impec,
+                                    double* Ni, double* vj, int nthreads, double* seconds)
+{
+    if (!fluid || !batch || !Vpore || !Ni || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
+    if (impec && !vj) return 1;
+    return run_threads(batch->n, nthreads, seconds,
+                       [fluid, batch, Vpore, impec, Ni, vj](int64_t lo, int64_t hi, double* s) {
+                           run_chunk_init(*fluid, *batch, Vpore, impec, Ni, vj, lo, hi, s);
+                       });
 }
 
 extern "C" const char* orc_kind(void) { return "reference"; }

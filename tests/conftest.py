@@ -102,6 +102,42 @@ def run_gpu_impec(fl, inp, form="plain"):
     return res
 
 
+def load_golden_init(name="init_nc6"):
+    """(fluid, inputs, reference outputs of InitFlashFIM, of InitFlashIMPEC,
+    fragile mask) of the initialisation fixture; each output dict carries
+    its self-noise under ``noise``."""
+    d = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    fl, _, _, _ = _fluid_only(d)
+    inp = {"P": d["in_P"], "T": d["in_T"], "z": d["in_z"], "S": d["in_S"], "Vpore": d["in_Vpore"]}
+    out = {k[4:]: d[k] for k in d.files if k.startswith("out_")}
+    out["skip"] = {k: d[f"skipout_{k}"] for k in ("flag", "minEig", "P", "T", "z")}
+    out["noise"] = {k[6:]: d[k].astype(np.float64) for k in d.files if k.startswith("noise_")}
+    outi = {k[5:]: d[k] for k in d.files if k.startswith("outi_")}
+    outi["noise"] = {k[7:]: d[k].astype(np.float64) for k in d.files if k.startswith("noisei_")}
+    return fl, inp, out, outi, d["fragile"]
+
+
+def run_gpu_init(fl, inp, impec=False, form="plain", init=None):
+    """One InitFlashFIM (or InitFlashIMPEC) of a fixture's initial states
+    through the C ABI on cuda:0; the host outputs carry ``Ni``."""
+    import torch
+    from opencaeporo_b200.flash import MixtureCompBatch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    m = MixtureCompBatch(fl)
+    if init is not None:
+        init.attach(m)
+    n = len(inp["P"])
+    st = m.new_state(n)
+    st.load(inp["P"], inp["T"], inp["z"])
+    m.init_flash(st, inp["Vpore"], S=inp["S"], impec=impec, form=form)
+    torch.cuda.synchronize()
+    res = st.to_host()
+    res["Ni"] = st.Ni.cpu().numpy().T.copy()
+    m.close()
+    return res
+
+
 def run_gpu(fl, inp, form="plain", init=None):
     """One flash of a fixture's inputs through the C ABI on cuda:0 (warm-start
     state and skip cache from the fixture); ``init``: a learned initialiser

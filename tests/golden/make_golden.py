@@ -11,7 +11,7 @@ edge of an iteration cap or a stability threshold; any implementation whose
 rounding differs from the reference's may legitimately land on either side.
 
     python tests/golden/make_golden.py            # writes tests/golden/*.npz
-    python tests/golden/make_golden.py restart_nc6   # one case only
+    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6)
 """
 from __future__ import annotations
 
@@ -122,14 +122,37 @@ def restart_case():
     run_case("restart_nc6", fl, inp, note="synthetic nc=6: bench-workload states with the most split restarts")
 
 
+NOISE_TRIALS = 32
+
+
+def perturbed(P, T, X, trial, prng, eps=2.0 ** -50):
+    """Inputs of noise trial `trial`: P, T or each entry of X (Ni or z)
+    moved by a few units in the last place -- the first six trials one
+    input at a time with both signs, the rest all together with random
+    signs and sizes."""
+    P, T, X = P.copy(), T.copy(), X.copy()
+    sgn = 1 if trial % 2 == 0 else -1
+    if trial < 2:
+        P *= 1 + sgn * eps
+    elif trial < 4:
+        T = T + sgn * eps * np.maximum(np.abs(T), 1.0)
+    elif trial < 6:
+        X = X * (1 + eps * prng.choice([-1.0, 1.0], size=X.shape))
+    else:
+        P *= 1 + eps * prng.choice([-2.0, -1.0, 1.0, 2.0], size=P.shape)
+        T = T * (1 + eps * prng.choice([-1.0, 1.0], size=T.shape))
+        X = X * (1 + eps * prng.choice([-1.0, 1.0], size=X.shape))
+    return P, T, X
+
+
 def impec_case():
     """FlashIMPEC on the 6-component fluid: a fresh step on 512 uniform states
     (the first 256) and near-envelope states (the rest), then a warm second
     step from the first step's phase counts, compositions and skip cache with
     P and Ni perturbed (skip hits, warm two-phase starts, relaxed stability);
     the fixture holds the second step, its warm-start inputs and the
-    reference's IMPEC outputs, with the fragile mask and self-noise of
-    run_case."""
+    reference's IMPEC outputs, with the fragile mask and the self-noise over
+    NOISE_TRIALS perturbations (``perturbed``)."""
     from oracle import compare as CMP
     fl = synthetic_fluid(6, 1234)
 
@@ -157,17 +180,9 @@ def impec_case():
     r, skip_out = run(P2, inp["T"], N2)
     frag = np.zeros(n, bool)
     noise = {k: np.zeros(n) for k in CMP.IMPEC_FLOAT_KEYS}
-    eps = 2.0 ** -50
     prng = np.random.default_rng(7)
-    for trial in range(6):
-        P, T, Ni = P2.copy(), inp["T"].copy(), N2.copy()
-        sgn = 1 if trial % 2 == 0 else -1
-        if trial < 2:
-            P *= 1 + sgn * eps
-        elif trial < 4:
-            T = T + sgn * eps * np.maximum(np.abs(T), 1.0)
-        else:
-            Ni = Ni * (1 + eps * prng.choice([-1.0, 1.0], size=Ni.shape))
+    for trial in range(NOISE_TRIALS):
+        P, T, Ni = perturbed(P2, inp["T"], N2, trial, prng)
         rr, _ = run(P, T, Ni)
         frag |= rr["phaseNum"] != r["phaseNum"]
         e = CMP.impec_errors(rr, r, fl.nc)
@@ -193,12 +208,82 @@ def impec_case():
           f"fragile={frag.sum()} size={os.path.getsize(path) / 1e6:.2f} MB")
 
 
+def init_case():
+    """InitFlashFIM and InitFlashIMPEC on the 6-component fluid: 512 initial
+    states (256 uniform, 256 near the envelope) given as mole fractions z,
+    with water saturations S_w ~ U(0.05, 0.5) and pore volumes
+    Vpore ~ U(50, 5000) ft3. The fixture holds the inputs, the reference's
+    FIM outputs (out_*) and IMPEC outputs (outi_*), each with the moles Ni
+    the flash object holds afterwards, the fragile mask and the self-noise
+    of both (``perturbed``)."""
+    from oracle import compare as CMP
+    fl = synthetic_fluid(6, 1234)
+
+    def pc(P, T, Ni):
+        return O.flash_fim("reference", fl, P, T, Ni, nthreads=8)["NPhc"]
+
+    a = synth.uniform_states(fl, 256, 91)
+    # (seed 92's bisection reaches a state whose split restarts without end
+    # in the reference)
+    b = synth.near_envelope_states(fl, 256, 94, pc)
+    P = np.concatenate([a["P"], b["P"]])
+    T = np.concatenate([a["T"], b["T"]])
+    Ni = np.concatenate([a["Ni"], b["Ni"]])
+    n = len(P)
+    z = Ni / Ni[:, :fl.nc].sum(axis=1, keepdims=True)
+    z[:, fl.nc] = 0.0
+    rng = np.random.default_rng(93)
+    S = np.zeros((n, 3))
+    S[:, 2] = rng.uniform(0.05, 0.5, n)
+    S[:, 0] = 1 - S[:, 2]
+    Vp = rng.uniform(50.0, 5000.0, n)
+
+    def run(P, T, z, impec):
+        return O.init_flash(fl, P, T, z, S, Vp, impec=impec, skip=O.new_skip(n, fl.nc), nthreads=8)
+
+    r, ri = run(P, T, z, False), run(P, T, z, True)
+    frag = np.zeros(n, bool)
+    noise = {k: np.zeros(n) for k in CMP.FLOAT_KEYS + ("Ni",)}
+    noisei = {k: np.zeros(n) for k in CMP.IMPEC_FLOAT_KEYS + ("Ni",)}
+    prng = np.random.default_rng(7)
+    for trial in range(NOISE_TRIALS):
+        Pp, Tp, zp = perturbed(P, T, z, trial, prng)
+        rr, rri = run(Pp, Tp, zp, False), run(Pp, Tp, zp, True)
+        frag |= (rr["phaseNum"] != r["phaseNum"]) | (rri["phaseNum"] != ri["phaseNum"])
+        e, ei = CMP.per_cell_errors(rr, r, fl.nc), CMP.impec_errors(rri, ri, fl.nc)
+        e["Ni"] = CMP._rel(rr["Ni"], r["Ni"]).max(axis=1)
+        ei["Ni"] = CMP._rel(rri["Ni"], ri["Ni"]).max(axis=1)
+        for k in noise:
+            noise[k] = np.fmax(noise[k], np.nan_to_num(e[k], nan=0.0))
+        for k in noisei:
+            noisei[k] = np.fmax(noisei[k], np.nan_to_num(ei[k], nan=0.0))
+    d = fluid_arrays(fl)
+    d["note"] = np.array("InitFlashFIM / InitFlashIMPEC of initial states z, S_w, Vpore")
+    d["in_P"], d["in_T"], d["in_z"], d["in_S"], d["in_Vpore"] = P, T, z, S, Vp
+    for k in OUT_KEYS + ("Ni",):
+        d[f"out_{k}"] = r[k]
+    for k in ("phaseNum", "phaseExist", "S", "Nt", "vf", "vfP", "vfi", "vj", "rho", "xi", "mu", "xij",
+              "ePEC", "ftype", "NPhc", "iters", "Ni"):
+        d[f"outi_{k}"] = ri[k]
+    for k, v in r["skip"].items():
+        d[f"skipout_{k}"] = v
+    d["fragile"] = frag
+    for k, v in noise.items():
+        d[f"noise_{k}"] = v.astype(np.float32)
+    for k, v in noisei.items():
+        d[f"noisei_{k}"] = v.astype(np.float32)
+    path = os.path.join(HERE, "init_nc6.npz")
+    np.savez_compressed(path, **d)
+    print(f"init_nc6: n={n} two-phase={np.mean(r['NPhc'] == 2):.3f} fragile={frag.sum()} "
+          f"size={os.path.getsize(path) / 1e6:.2f} MB")
+
+
 def main(only=()):
     if not O.available("reference"):
         raise SystemExit("oracle/_ref/libocpref.so missing: run `make -C oracle ref` first")
     if only:
         for name in only:
-            {"restart_nc6": restart_case, "impec_nc6": impec_case}[name]()
+            {"restart_nc6": restart_case, "impec_nc6": impec_case, "init_nc6": init_case}[name]()
         return
 
     # 1) SPE5 fluid (examples/spe5/EGOIL.in) at 160 degF, the deck's initial composition
@@ -253,6 +338,9 @@ def main(only=()):
 
     # 7) the IMPEC flash, warm-started
     impec_case()
+
+    # 8) the initialisation flashes
+    init_case()
 
 
 if __name__ == "__main__":

@@ -288,3 +288,70 @@ def test_impec_matches_reference_golden(form):
     assert set(np.unique(ref["ftype"])) == {0, 1}
     sg, sr = got["skip"], ref["skip"]
     assert np.array_equal(sg["flag"][same].astype(int), sr["flag"][same].astype(int))
+
+
+def _ni_ok(got, ref, noise, same):
+    """Ni of the cells with matching phase counts within 1e-8 relative or
+    10x the reference's own 1-ulp sensitivity."""
+    e = CMP._rel(got["Ni"], ref["Ni"]).max(axis=1)
+    allowed = np.maximum(1e-8, 10 * np.nan_to_num(noise["Ni"], nan=0.0))
+    bad = np.nonzero(same & (e > allowed))[0]
+    return bad
+
+
+@pytest.mark.parametrize("impec", [False, True], ids=["fim", "impec"])
+@pytest.mark.parametrize("form", ["plain", "batched", "mixed"])
+def test_init_flash_matches_reference_golden(form, impec):
+    """ocpf_init_flash_fim / ocpf_init_flash_impec (InitFlashFIM /
+    InitFlashIMPEC + PassFlashValue) on 512 initial states against the
+    reference: identical phase counts except knife-edge cells, the moles Ni
+    that fill the pore volume and every output within 1e-8 relative or 10x
+    the reference's own 1-ulp sensitivity, flash type 0 everywhere, and the
+    skip cache the reference leaves."""
+    from conftest import load_golden_init, run_gpu_init
+    fl, inp, ref, refi, fragile = load_golden_init()
+    r = refi if impec else ref
+    got = run_gpu_init(fl, inp, impec=impec, form=form)
+    if impec:
+        chk = CMP.check_impec(got, r, fl.nc, noise=r["noise"], fragile=fragile)
+    else:
+        chk = CMP.check(got, r, fl.nc, noise=r["noise"], fragile=fragile)
+    assert chk["ok"], f"{form}: np_mismatch={list(chk['np_mismatch'])} worst={chk['worst']}"
+    same = (got["phaseNum"] == r["phaseNum"]) & ~fragile
+    bad = _ni_ok(got, r, r["noise"], same)
+    assert len(bad) == 0, bad
+    assert np.all(got["ftype"] == 0)
+    if not impec:
+        # hydrocarbon nj: the phase fractions, as the reference's CopyPhase leaves them
+        ex = r["phaseExist"][:, :2].astype(bool) & same[:, None]
+        np.testing.assert_allclose(got["nj"][:, :2][ex], r["nj"][:, :2][ex], rtol=1e-8)
+        sg, sr = got["skip"], ref["skip"]
+        assert np.array_equal(sg["flag"][same].astype(int), sr["flag"][same].astype(int))
+
+
+def test_init_flash_then_fim_step_is_consistent():
+    """The state InitFlashFIM leaves is the one FlashFIM sees next: a
+    FlashFIM of the initialised moles at the same P and T, warm-started from
+    the initialisation's outputs, keeps every phase count and reproduces the
+    saturations and volumes to the flash's convergence tolerance (the pore
+    volume stays filled)."""
+    import torch
+    from conftest import load_golden_init
+    from opencaeporo_b200.flash import MixtureCompBatch
+    fl, inp, ref, _, fragile = load_golden_init()
+    m = MixtureCompBatch(fl)
+    n = len(inp["P"])
+    st = m.new_state(n)
+    st.load(inp["P"], inp["T"], inp["z"])
+    m.init_flash(st, inp["Vpore"], S=inp["S"], form="batched")
+    torch.cuda.synchronize()
+    a = st.to_host()
+    m.flash_fim(st, form="batched")
+    torch.cuda.synchronize()
+    b = st.to_host()
+    m.close()
+    keep = ~fragile
+    assert np.array_equal(a["phaseNum"][keep], b["phaseNum"][keep])
+    np.testing.assert_allclose(a["vf"], inp["Vpore"], rtol=1e-12)
+    np.testing.assert_allclose(b["vf"], inp["Vpore"], rtol=1e-6)
+    np.testing.assert_allclose(b["S"][keep], a["S"][keep], atol=1e-6)

@@ -183,6 +183,26 @@ def test_fast_matches_reference_goldens(case):
 
 
 @pytest.mark.gpu
+def test_fast_init_flash_matches_reference_golden():
+    """InitFlashFIM in the fast form (every initial state is a fresh cell,
+    so every one goes through the trained initialiser) against the
+    reference, with the bar of test_fast_matches_reference_goldens."""
+    from conftest import load_golden_init, run_gpu_init
+    from oracle import compare as CMP
+    fl, inp, ref, _, fragile = load_golden_init()
+    got = run_gpu_init(fl, inp, form="fast", init=_model())
+    det = np.asarray(ref["ePEC"]) <= 1e-9
+    chk = CMP.check(_sub(got, det), _sub(ref, det), fl.nc, noise=_sub(ref["noise"], det), fragile=fragile[det])
+    assert chk["ok"], CMP.check_summary(chk)
+    same = det & (got["phaseNum"] == ref["phaseNum"]) & ~fragile
+    e = CMP._rel(got["Ni"], ref["Ni"]).max(axis=1)
+    assert np.all(e[same] <= np.maximum(1e-8, 10 * ref["noise"]["Ni"][same]))
+    if (~det).any():
+        diff = (got["phaseNum"] != ref["phaseNum"]) & ~det
+        assert np.all(_clean_equilibrium(_sub(got, diff), fl.nc))
+
+
+@pytest.mark.gpu
 def test_initialiser_gain_over_mixed():
     """What the trained network buys on 65,536 held-out states of the
     workload distribution (a seed it was not trained on): the fast form ends

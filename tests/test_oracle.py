@@ -131,3 +131,25 @@ def test_reference_reproduces_impec_golden():
     assert e["same"].all()
     for k in CMP.IMPEC_FLOAT_KEYS:
         assert np.nanmax(e[k]) == 0.0, k
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SRC), reason="reference sources not present")
+@pytest.mark.parametrize("impec", [False, True], ids=["fim", "impec"])
+def test_reference_reproduces_init_golden(impec):
+    """The compiled reference's InitFlashFIM / InitFlashIMPEC, rebuilt here,
+    reproduces the initialisation fixture bit for bit (guards the fixture
+    and the harness's initialisation entry), and the initialised state
+    fills the pore volume: vf = Vpore to rounding."""
+    import subprocess
+    from conftest import load_golden_init
+    subprocess.check_call(["make", "-s", "-C", os.path.join(os.path.dirname(O.__file__)), "ref"])
+    fl, inp, ref, refi, _ = load_golden_init()
+    r = refi if impec else ref
+    got = O.init_flash(fl, inp["P"], inp["T"], inp["z"], inp["S"], inp["Vpore"], impec=impec,
+                       skip=O.new_skip(len(inp["P"]), fl.nc), nthreads=4)
+    e = CMP.impec_errors(got, r, fl.nc) if impec else CMP.per_cell_errors(got, r, fl.nc)
+    assert e["same"].all()
+    for k in (CMP.IMPEC_FLOAT_KEYS if impec else CMP.FLOAT_KEYS):
+        assert np.nanmax(e[k]) == 0.0, k
+    assert np.array_equal(got["Ni"], r["Ni"])
+    np.testing.assert_allclose(got["vf"], inp["Vpore"], rtol=1e-12)
