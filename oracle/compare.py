@@ -241,3 +241,45 @@ def check_impec(gpu: dict, ref: dict, nc: int, noise: dict = None, fragile=None,
             ok = False
     return {"ok": ok, "np_mismatch": bad_np, "np_mismatch_all": np.nonzero(~e["same"])[0], "worst": worst,
             "errors": e}
+
+
+# ------------------------------------------------- the reference's self-noise
+NOISE_TRIALS = 32
+
+
+def perturbed(P, T, X, trial, prng, eps=2.0 ** -50):
+    """Inputs of noise trial `trial`: P, T or each entry of X (Ni or z)
+    moved by a few units in the last place -- the first six trials one
+    input at a time with both signs, the rest all together with random
+    signs and sizes."""
+    P, T, X = np.array(P, dtype=np.float64), np.array(T, dtype=np.float64), np.array(X, dtype=np.float64)
+    sgn = 1 if trial % 2 == 0 else -1
+    if trial < 2:
+        P *= 1 + sgn * eps
+    elif trial < 4:
+        T = T + sgn * eps * np.maximum(np.abs(T), 1.0)
+    elif trial < 6:
+        X = X * (1 + eps * prng.choice([-1.0, 1.0], size=X.shape))
+    else:
+        P *= 1 + eps * prng.choice([-2.0, -1.0, 1.0, 2.0], size=P.shape)
+        T = T * (1 + eps * prng.choice([-1.0, 1.0], size=T.shape))
+        X = X * (1 + eps * prng.choice([-1.0, 1.0], size=X.shape))
+    return P, T, X
+
+
+def self_noise(run, P, T, X, base, nc, trials: int = NOISE_TRIALS, seed: int = 7):
+    """(noise, moved): per FIM output field and cell, the largest relative
+    change of ``run(P, T, X)`` (the reference on perturbed inputs) against
+    ``base`` over ``trials`` perturbations; and the cells whose phase count
+    moved."""
+    prng = np.random.default_rng(seed)
+    n = len(P)
+    noise = {k: np.zeros(n) for k in FLOAT_KEYS}
+    moved = np.zeros(n, bool)
+    for t in range(trials):
+        r = run(*perturbed(P, T, X, t, prng))
+        moved |= np.asarray(r["phaseNum"]) != np.asarray(base["phaseNum"])
+        e = per_cell_errors(r, base, nc)
+        for k in FLOAT_KEYS:
+            noise[k] = np.fmax(noise[k], np.nan_to_num(e[k], nan=0.0))
+    return noise, moved

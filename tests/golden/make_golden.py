@@ -122,29 +122,6 @@ def restart_case():
     run_case("restart_nc6", fl, inp, note="synthetic nc=6: bench-workload states with the most split restarts")
 
 
-NOISE_TRIALS = 32
-
-
-def perturbed(P, T, X, trial, prng, eps=2.0 ** -50):
-    """Inputs of noise trial `trial`: P, T or each entry of X (Ni or z)
-    moved by a few units in the last place -- the first six trials one
-    input at a time with both signs, the rest all together with random
-    signs and sizes."""
-    P, T, X = P.copy(), T.copy(), X.copy()
-    sgn = 1 if trial % 2 == 0 else -1
-    if trial < 2:
-        P *= 1 + sgn * eps
-    elif trial < 4:
-        T = T + sgn * eps * np.maximum(np.abs(T), 1.0)
-    elif trial < 6:
-        X = X * (1 + eps * prng.choice([-1.0, 1.0], size=X.shape))
-    else:
-        P *= 1 + eps * prng.choice([-2.0, -1.0, 1.0, 2.0], size=P.shape)
-        T = T * (1 + eps * prng.choice([-1.0, 1.0], size=T.shape))
-        X = X * (1 + eps * prng.choice([-1.0, 1.0], size=X.shape))
-    return P, T, X
-
-
 def impec_case():
     """FlashIMPEC on the 6-component fluid: a fresh step on 512 uniform states
     (the first 256) and near-envelope states (the rest), then a warm second
@@ -152,7 +129,7 @@ def impec_case():
     P and Ni perturbed (skip hits, warm two-phase starts, relaxed stability);
     the fixture holds the second step, its warm-start inputs and the
     reference's IMPEC outputs, with the fragile mask and the self-noise over
-    NOISE_TRIALS perturbations (``perturbed``)."""
+    oracle.compare.NOISE_TRIALS perturbations (``perturbed``)."""
     from oracle import compare as CMP
     fl = synthetic_fluid(6, 1234)
 
@@ -181,8 +158,8 @@ def impec_case():
     frag = np.zeros(n, bool)
     noise = {k: np.zeros(n) for k in CMP.IMPEC_FLOAT_KEYS}
     prng = np.random.default_rng(7)
-    for trial in range(NOISE_TRIALS):
-        P, T, Ni = perturbed(P2, inp["T"], N2, trial, prng)
+    for trial in range(CMP.NOISE_TRIALS):
+        P, T, Ni = CMP.perturbed(P2, inp["T"], N2, trial, prng)
         rr, _ = run(P, T, Ni)
         frag |= rr["phaseNum"] != r["phaseNum"]
         e = CMP.impec_errors(rr, r, fl.nc)
@@ -246,8 +223,8 @@ def init_case():
     noise = {k: np.zeros(n) for k in CMP.FLOAT_KEYS + ("Ni",)}
     noisei = {k: np.zeros(n) for k in CMP.IMPEC_FLOAT_KEYS + ("Ni",)}
     prng = np.random.default_rng(7)
-    for trial in range(NOISE_TRIALS):
-        Pp, Tp, zp = perturbed(P, T, z, trial, prng)
+    for trial in range(CMP.NOISE_TRIALS):
+        Pp, Tp, zp = CMP.perturbed(P, T, z, trial, prng)
         rr, rri = run(Pp, Tp, zp, False), run(Pp, Tp, zp, True)
         frag |= (rr["phaseNum"] != r["phaseNum"]) | (rri["phaseNum"] != ri["phaseNum"])
         e, ei = CMP.per_cell_errors(rr, r, fl.nc), CMP.impec_errors(rri, ri, fl.nc)
