@@ -54,9 +54,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="bench1m", choices=["bench1m", "regions4"],
+    ap.add_argument("--workload", default="bench1m", choices=["bench1m", "regions4", "entries"],
                     help="bench1m: the headline 1M-cell workload; regions4: four fluids (3, 6, 9 and 12 "
-                         "components, 524,288 states each) flashed together")
+                         "components, 524,288 states each) flashed together; entries: the initialisation "
+                         "and IMPEC entry points on the 1M-cell workload")
     ap.add_argument("--form", default="fast", choices=["plain", "batched", "mixed", "fast"])
     ap.add_argument("--ncell", type=int, default=NCELL)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -450,10 +451,128 @@ def regions_arm(args):
         "plain_fp64_per_region": {"value": total / (t_plain * 1e-3), "ms_per_step": t_plain}}), flush=True)
 
 
+def entries_arm(args):
+    """The other flash entry points on the bench workload (1,048,576 fresh
+    states of the 6-component fluid): ocpf_init_flash_fim (InitFlashFIM:
+    the initial mole fractions z = Ni / sum Ni, S_w ~ U(0.05, 0.5), pore
+    volumes ~ U(50, 5000) ft3) and ocpf_flash_impec (FlashIMPEC of fresh
+    cells), each in the chosen form and in the plain FP64 form, timed with
+    CUDA events; the reference's own calls on the first states with every
+    host thread, and the error of the chosen form against them. One JSON
+    line; not the headline metric."""
+    import torch
+    from oracle import compare as CMP
+    from oracle import oracle as O
+    from opencaeporo_b200.flash import MixtureCompBatch
+    fl = bench_fluid()
+    n = args.ncell
+    cache = args.workload_cache
+    if cache and os.path.exists(cache):
+        d = np.load(cache)
+        w = {"P": d["P"][:n], "T": d["T"][:n], "Ni": d["Ni"][:n]}
+    else:
+        w = make_workload(fl, n, SEED, 0)
+        if cache:
+            np.savez(cache, P=w["P"], T=w["T"], Ni=w["Ni"])
+    nc = fl.nc
+    z = w["Ni"] / w["Ni"][:, :nc].sum(axis=1, keepdims=True)
+    z[:, nc] = 0.0
+    rng = np.random.default_rng(SEED + 1)
+    S = np.zeros((n, 3))
+    S[:, 2] = rng.uniform(0.05, 0.5, n)
+    S[:, 0] = 1 - S[:, 2]
+    Vp = rng.uniform(50.0, 5000.0, n)
+    m = MixtureCompBatch(fl, 0)
+    if args.form == "fast":
+        from opencaeporo_b200.learn import DEFAULT_MODEL, Initializer
+        Initializer.load(DEFAULT_MODEL).attach(m)
+    st = m.new_state(n)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    Pt = torch.as_tensor(w["P"]).cuda()
+    Tt = torch.as_tensor(w["T"]).cuda()
+    Zt = torch.as_tensor(np.ascontiguousarray(z.T)).cuda()
+    Nt = torch.as_tensor(np.ascontiguousarray(w["Ni"].T)).cuda()
+    St = torch.as_tensor(np.ascontiguousarray(S.T)).cuda()
+    Vt = torch.as_tensor(Vp).cuda()
+
+    def timed(prep, call):
+        ts = []
+        for s_ in range(args.warmup + args.steps):
+            flush.zero_()
+            prep()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            call()
+            b.record(stream)
+            torch.cuda.synchronize()
+            if s_ >= args.warmup:
+                ts.append(a.elapsed_time(b))
+        return float(np.mean(ts))
+
+    def prep_init():
+        st.P.copy_(Pt)
+        st.T.copy_(Tt)
+        st.Ni.copy_(Zt)
+        st.out["S"].copy_(St)
+        st.skip["flag"].zero_()
+
+    def prep_impec():
+        st.P.copy_(Pt)
+        st.T.copy_(Tt)
+        st.Ni.copy_(Nt)
+        st.skip["flag"].zero_()
+
+    res = {}
+    for name, prep, call in (
+            ("init_flash_fim", prep_init, lambda f: m.init_flash(st, Vt, form=f)),
+            ("flash_impec", prep_impec, lambda f: m.flash_impec(st, form=f, fresh=True))):
+        t_form = timed(prep, lambda: call(args.form))
+        gpu = st.to_host()
+        if name == "init_flash_fim":
+            gpu["Ni"] = st.Ni.cpu().numpy().T.copy()
+        t_plain = timed(prep, lambda: call("plain"))
+        cores = os.cpu_count() or 1
+        ns = int(min(n, max(8192, cores * 4000)))
+        if name == "init_flash_fim":
+            ref = O.init_flash(fl, w["P"][:ns], w["T"][:ns], z[:ns], S[:ns], Vp[:ns], nthreads=cores)
+            sub = {k: v[:ns] for k, v in gpu.items() if isinstance(v, np.ndarray)}
+            e = CMP.per_cell_errors(sub, ref, nc)
+            keys = CMP.FLOAT_KEYS
+        else:
+            ref = O.flash_impec(fl, w["P"][:ns], w["T"][:ns], w["Ni"][:ns], nthreads=cores)
+            sub = {k: v[:ns] for k, v in gpu.items() if isinstance(v, np.ndarray)}
+            e = CMP.impec_errors(sub, ref, nc)
+            keys = CMP.IMPEC_FLOAT_KEYS
+        worst = np.zeros(ns)
+        for k in keys:
+            worst = np.fmax(worst, np.nan_to_num(e[k], nan=0.0))
+        det = e["same"] & ((ref["NPhc"] == 1) | (ref["ePEC"] <= 1e-9))
+        res[name] = {
+            "value": n / (t_form * 1e-3), "unit": "states/s", "ms_per_step": t_form, "form": args.form,
+            "plain_fp64_gpu": {"value": n / (t_plain * 1e-3), "ms_per_step": t_plain},
+            "reference_cpu": {"value": ns / ref["seconds"], "unit": "states/s", "cores": cores,
+                              "sample": f"first {ns} states, one call each"},
+            "parity_on_sample": {"cells": ns, "phase_count_mismatches": int(np.count_nonzero(~e["same"])),
+                                 "well_determined_cells": int(det.sum()),
+                                 "share_well_determined_le_1e-8": float(np.mean(worst[det] <= 1e-8))}}
+    m.close()
+    print(json.dumps({
+        "metric": "flash states/s of the initialisation and IMPEC entry points", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": "1,048,576 states of the bench workload; init: z = Ni / sum Ni, "
+                               "S_w ~ U(0.05, 0.5), Vpore ~ U(50, 5000) ft3; IMPEC: fresh cells",
+                   "l2": "flushed between steps (256 MiB write)"},
+        "entries": res}), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "regions4":
         regions_arm(args)
+        return
+    if args.workload == "entries":
+        entries_arm(args)
         return
     if args.impl == "reference":
         reference_arm(args)

@@ -62,7 +62,7 @@ __device__ __forceinline__ void fug_phi(const FluidConst& F, const double* sA, c
     const double L2  = fug_L2(zj, bj);
     const double ib  = 1.0 / bj;
     const double ia  = 1.0 / aj;
-    const double cf  = aj / D1MD2 * ib;
+    const double cf  = div_const(aj, D1MD2, RCPD1MD2) * ib;
     const double zm1 = zj - 1;
 #pragma unroll
     for (int i = 0; i < NC; i++) {

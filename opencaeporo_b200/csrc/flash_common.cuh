@@ -23,6 +23,30 @@ constexpr double D1PD2        = D1 + D2;
 constexpr double D1MD2        = D1 - D2;
 constexpr double D1TD2        = D1 * D2;
 
+// x / d, correctly rounded, for a constant divisor d given with its
+// correctly rounded reciprocal rd = RN(1/d): q = RN(x rd) lies within one
+// ulp of x / d, so the remainder r = x - d q is exact in one fused
+// multiply-add and RN(q + r rd) is the correctly rounded quotient
+// (Markstein's theorem: P. Markstein, "Computation of elementary functions
+// on the IBM RISC System/6000 processor", IBM J. Res. Develop. 34(1), 1990;
+// J.-M. Muller et al., Handbook of Floating-Point Arithmetic, 2nd ed., 2018,
+// ch. 4). Three dependent FP64 operations in place of a division, with the
+// same result bits. Zeros, non-finite values and magnitudes outside
+// [1e-270, 1e270] (where r or r rd could leave the normal range) take the
+// ordinary division.
+__device__ __forceinline__ double div_const(double x, double d, double rd)
+{
+    const double ax = fabs(x);
+    if (!(ax > 1e-270 && ax < 1e270)) return x / d;
+    const double q = x * rd;
+    const double r = fma(-d, q, x);
+    return fma(r, rd, q);
+}
+constexpr double RCP3     = 1.0 / 3;
+constexpr double RCP9     = 1.0 / 9;
+constexpr double RCP54    = 1.0 / 54;
+constexpr double RCPD1MD2 = 1.0 / D1MD2;
+
 // Everything a flash of one fluid reads that does not depend on the cell.
 // Passed by value as a __grid_constant__ kernel parameter, so that with a
 // compile-time component count every access is a constant-bank operand.

@@ -41,8 +41,8 @@ struct PrCubic {
         a  = (D1PD2 - 1) * bj - 1;
         b  = (aj + D1TD2 * bj * bj - D1PD2 * bj * (bj + 1));
         c  = -(aj * bj + D1TD2 * bj * bj * (bj + 1));
-        Q  = (a * a - 3 * b) / 9;
-        R  = (2 * a * a * a - 9 * a * b + 27 * c) / 54;
+        Q  = div_const(a * a - 3 * b, 9, RCP9);
+        R  = div_const(2 * a * a * a - 9 * a * b + 27 * c, 54, RCP54);
         Q3 = Q * Q * Q;
         M  = R * R - Q3;
     }
@@ -51,8 +51,8 @@ struct PrCubic {
     __device__ __forceinline__ double trig_root(int k, double theta) const
     {
         const double s2  = -2 * sqrt(Q);
-        const double a3  = a / 3;
-        const double arg = k == 1 ? (theta + 2 * PI_TRUNC) / 3 : (k == 2 ? (theta - 2 * PI_TRUNC) / 3 : theta / 3);
+        const double a3  = div_const(a, 3, RCP3);
+        const double arg = div_const(k == 1 ? theta + 2 * PI_TRUNC : (k == 2 ? theta - 2 * PI_TRUNC : theta), 3, RCP3);
         return nt_polish(s2 * cos(arg) - a3, a, b, c);
     }
     // The single real root (M > 0), polished.
@@ -63,7 +63,7 @@ struct PrCubic {
         const double t2 = R + sM;
         const double S  = signD(t1) * cbrt(fabs(t1));
         const double T  = -signD(t2) * cbrt(fabs(t2));
-        return nt_polish(S + T - a / 3, a, b, c);
+        return nt_polish(S + T - div_const(a, 3, RCP3), a, b, c);
     }
 };
 

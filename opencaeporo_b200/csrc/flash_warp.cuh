@@ -10,9 +10,12 @@
 // of one another run on different lanes and are then broadcast with
 // shuffles:
 //   * Rachford-Rice: lane i forms component i's residual term, lane 16 + i
-//     its Jacobian term (two divisions); the sums are then taken on every
-//     lane in the reference's order;
-//   * compositions, fugacity ratios and K: one component per lane;
+//     its Jacobian term (two divisions); one shuffle per component gathers
+//     both halves' terms, half 0 sums the residual and half 1 the Jacobian
+//     in the reference's order;
+//   * compositions, fugacity ratios and K: one component per lane (lanes i
+//     and 16 + i); inside SplitSSM2's loop no lane holds the full state, it
+//     is gathered once when the loop ends;
 //   * fugacities: phase 0 on lanes 0-15 and phase 1 on lanes 16-31 at once;
 //     within a half, lanes 0-2 polish the three roots of the cubic and form
 //     the three pieces of the root choice, lanes 0-3 the two logarithms and
@@ -55,34 +58,43 @@ struct WarpSplit {
         return r;
     }
 
-    // RachfordRice2, src/MixtureComp.cpp:1907-1959 (CellFlash::rachford_rice2)
-    __device__ void rachford_rice2()
+    // The Rachford-Rice bracket [1 / (1 - Kmax), 1 / (1 - Kmin)] from all K
+    // (every lane holds them): lane 0 forms the lower end, lane 16 the upper.
+    __device__ __forceinline__ void rr_bracket(const double* K, double& numin, double& numax) const
     {
-        double Kmin = f.Ks[0], Kmax = f.Ks[0];
+        double Kmin = K[0], Kmax = K[0];
 #pragma unroll
         for (int i = 1; i < NC; i++) {
-            if (f.Ks[i] < Kmin) Kmin = f.Ks[i];
-            if (f.Ks[i] > Kmax) Kmax = f.Ks[i];
+            if (K[i] < Kmin) Kmin = K[i];
+            if (K[i] > Kmax) Kmax = K[i];
         }
         const double bound = 1 / (1 - (half ? Kmin : Kmax));
-        const double numin = __shfl_sync(WARP_ALL, bound, 0);
-        const double numax = __shfl_sync(WARP_ALL, bound, 16);
-        double       v     = 0.5 * (numin + numax);
-        // loop-invariant parts of component q's terms, formed as the
-        // one-thread form forms them: z km1 / tmp and z km1 km1 / (tmp tmp)
-        const double km1 = pick(f.Ks) - 1;
-        const double zk  = pick(f.zi) * km1;
+        numin              = __shfl_sync(WARP_ALL, bound, 0);
+        numax              = __shfl_sync(WARP_ALL, bound, 16);
+    }
+
+    // RachfordRice2, src/MixtureComp.cpp:1907-1959 (CellFlash::rachford_rice2),
+    // from component q's K and z on lanes q and 16 + q and the bracket.
+    // Lane q forms component q's residual term and lane 16 + q its negated
+    // Jacobian term; one shuffle per component gathers each half's terms, so
+    // half 0 sums rj and half 1 sums J in the reference's order (x - y is
+    // x + (-y), so J equals the reference's J -= ... bit for bit).
+    __device__ void rachford_rice2(double Kq, double zq, double numin, double numax)
+    {
+        double       v   = 0.5 * (numin + numax);
+        const double km1 = Kq - 1;
+        const double zk  = zq * km1;
         const double num = half ? zk * km1 : zk;
+        const int    src = lane & 16;
         int          iter = 0;
         while (true) {
             const double tmp  = 1 + v * km1;
-            const double term = num / (half ? tmp * tmp : tmp);
-            double       rj = 0, J = 0;
+            const double term = half ? -(num / (tmp * tmp)) : num / tmp;
+            double       sum  = 0;
 #pragma unroll
-            for (int i = 0; i < NC; i++) {
-                rj += __shfl_sync(WARP_ALL, term, i);
-                J -= __shfl_sync(WARP_ALL, term, 16 + i);
-            }
+            for (int i = 0; i < NC; i++) sum += __shfl_sync(WARP_ALL, term, src + i);
+            const double rj = __shfl_sync(WARP_ALL, sum, 0);
+            const double J  = __shfl_sync(WARP_ALL, sum, 16);
             if (fabs(rj) < f.F.rr_tol || iter > f.F.rr_maxit) break;
             const double dnuj  = -rj / J;
             const double tmpnu = v + dnuj;
@@ -99,31 +111,18 @@ struct WarpSplit {
         f.nu[1] = 1 - v;
     }
 
-    // UpdateXRR (src/MixtureComp.cpp:2030-2043): lane i forms x_1i and x_0i.
-    __device__ __forceinline__ void update_x()
+    // One phase of CalFugPhi (src/MixtureComp.cpp:993-1101) on each half:
+    // half j holds phase j's composition xj; returns phi of component q of
+    // phase `half` and leaves the phase's a, b and Z on every lane of the
+    // half. Within a half, lanes 0-2 polish the cubic's roots and lanes 0-3
+    // form the two logarithms and two reciprocals.
+    __device__ __forceinline__ double fug_lane(const double* xj, double& aj, double& bj, double& zj) const
     {
-        const double tmp = 1 + f.nu[0] * (pick(f.Ks) - 1);
-        const double x1  = pick(f.zi) / tmp;
-        const double x0  = pick(f.Ks) * x1;
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            f.x[1][i] = __shfl_sync(WARP_ALL, x1, i);
-            f.x[0][i] = __shfl_sync(WARP_ALL, x0, i);
-        }
-    }
-
-    // CalFugPhiAll for NP = 2 (src/MixtureComp.cpp:1103-1145; CalFugPhi
-    // :993-1101 per phase).
-    __device__ __forceinline__ void fug_phi_all()
-    {
-        double xj[NC];
-#pragma unroll
-        for (int k = 0; k < NC; k++) xj[k] = half ? f.x[1][k] : f.x[0][k];
-        double t[NC], aj, bj;
+        double t[NC];
         mix_ab<NC>(f.F, f.sA, f.Bi, xj, t, aj, bj);
-        const double zj   = sol_eos_group(aj, bj, hmask, half << 4, q);
-        const int    base = half << 4;
-        double       piece;
+        zj              = sol_eos_group(aj, bj, hmask, half << 4, q);
+        const int base  = half << 4;
+        double    piece;
         if (q == 0)
             piece = fug_L1(zj, bj);
         else if (q == 1)
@@ -136,7 +135,7 @@ struct WarpSplit {
         const double L2  = __shfl_sync(WARP_ALL, piece, base + 1);
         const double ib  = __shfl_sync(WARP_ALL, piece, base + 2);
         const double ia  = __shfl_sync(WARP_ALL, piece, base + 3);
-        const double cf  = aj / D1MD2 * ib;
+        const double cf  = div_const(aj, D1MD2, RCPD1MD2) * ib;
         const double zm1 = zj - 1;
         double       tq = 0, bq = 0;
 #pragma unroll
@@ -146,8 +145,13 @@ struct WarpSplit {
                 bq = f.Bi[i];
             }
         }
-        double ph = 0;
-        if (q < NC) ph = phi_term(bq * ib, tq, ia, zm1, L1, cf, L2);
+        return q < NC ? phi_term(bq * ib, tq, ia, zm1, L1, cf, L2) : 0.0;
+    }
+
+    // The state of both phases on every lane from the per-lane pieces: a, b,
+    // Z from lanes 0 and 16, phi_ji from lane 16 j + i, and f = phi x P.
+    __device__ __forceinline__ void share_phases(double ph, double aj, double bj, double zj)
+    {
 #pragma unroll
         for (int j = 0; j < 2; j++) {
             f.Aj[j] = __shfl_sync(WARP_ALL, aj, 16 * j);
@@ -162,8 +166,24 @@ struct WarpSplit {
         }
     }
 
+    // CalFugPhiAll for NP = 2 (src/MixtureComp.cpp:1103-1145) from f.x.
+    __device__ __forceinline__ void fug_phi_all()
+    {
+        double xj[NC];
+#pragma unroll
+        for (int k = 0; k < NC; k++) xj[k] = half ? f.x[1][k] : f.x[0][k];
+        double aj, bj, zj;
+        const double ph = fug_lane(xj, aj, bj, zj);
+        share_phases(ph, aj, bj, zj);
+    }
+
     // SplitSSM2 with UpdateXRR, src/MixtureComp.cpp:1847-1903, 2030-2043
-    // (CellFlash::split_ssm2 with the pieces above).
+    // (CellFlash::split_ssm2 with the pieces above). Inside the loop lanes q
+    // and 16 + q keep component q's K, x and phi only: the compositions reach
+    // each half by one shuffle per component, the other phase's phi by one
+    // exchange between the halves, and the new K (lanes 16 + i) and the
+    // residual terms (lanes i) return by one gather per component. The full
+    // state is formed on every lane when the loop ends.
     __device__ void split_ssm2(bool restart)
     {
         f.ssmsp_conflag = true;
@@ -178,26 +198,60 @@ struct WarpSplit {
             Stol *= 1e-1;
             maxIt *= 2;
         }
-        int iter = 0;
+        double numin, numax;
+        rr_bracket(f.Ks, numin, numax);
+        double       Kq  = pick(f.Ks);
+        const double zq  = pick(f.zi);
+        const int    src = lane & 16;
+        double       x0q = 0, x1q = 0, ph = 0, aj = 0, bj = 0, zj = 0, v = 0;
+        int          iter = 0;
         while (Se > Stol) {
-            rachford_rice2();
-            update_x();
-            fug_phi_all();
-            // lane i: component i's squared fugacity-ratio residual; lane
-            // 16 + i: its new K
-            const double v = half ? pick(f.phi[1]) / pick(f.phi[0]) : sq(pick(f.fug[1]) / pick(f.fug[0]) - 1);
-            Se             = 0;
+            rachford_rice2(Kq, zq, numin, numax);
+            // UpdateXRR for component q
+            const double tmp = 1 + f.nu[0] * (Kq - 1);
+            x1q              = zq / tmp;
+            x0q              = Kq * x1q;
+            double xj[NC];
+#pragma unroll
+            for (int k = 0; k < NC; k++) xj[k] = __shfl_sync(WARP_ALL, half ? x1q : x0q, src + k);
+            ph               = fug_lane(xj, aj, bj, zj);
+            const double pho = __shfl_xor_sync(WARP_ALL, ph, 16);
+            // lane q: component q's squared fugacity-ratio residual; lane
+            // 16 + q: its new K
+            v = half ? ph / pho : sq(pho * x1q * f.P / (ph * x0q * f.P) - 1);
+            double Kg[NC];
+            Se = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                Se += __shfl_sync(WARP_ALL, v, i);
-                f.Ks[i] = __shfl_sync(WARP_ALL, v, 16 + i);
+                Kg[i] = __shfl_sync(WARP_ALL, v, src + i);
+                Se += Kg[i];
             }
+            Se = __shfl_sync(WARP_ALL, Se, 0);
+            Kq = __shfl_sync(WARP_ALL, v, 16 | q);
+            // the next bracket from half 1's K: lane 16 forms 1 / (1 - Kmin),
+            // lane 17 1 / (1 - Kmax)
+            double Kmin = Kg[0], Kmax = Kg[0];
+#pragma unroll
+            for (int i = 1; i < NC; i++) {
+                if (Kg[i] < Kmin) Kmin = Kg[i];
+                if (Kg[i] > Kmax) Kmax = Kg[i];
+            }
+            const double bound = 1 / (1 - ((lane & 1) ? Kmax : Kmin));
+            numax              = __shfl_sync(WARP_ALL, bound, 16);
+            numin              = __shfl_sync(WARP_ALL, bound, 17);
             iter++;
             if (iter > maxIt) {
                 f.ssmsp_conflag = false;
                 break;
             }
         }
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            f.Ks[i]   = __shfl_sync(WARP_ALL, v, 16 + i);
+            f.x[0][i] = __shfl_sync(WARP_ALL, x0q, i);
+            f.x[1][i] = __shfl_sync(WARP_ALL, x1q, i);
+        }
+        share_phases(ph, aj, bj, zj);
         f.ssmsp_realTol = sqrt(Se);
         f.it_ssmsp += iter;
     }

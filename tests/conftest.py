@@ -114,6 +114,11 @@ def load_golden_init(name="init_nc6"):
     out["noise"] = {k[6:]: d[k].astype(np.float64) for k in d.files if k.startswith("noise_")}
     outi = {k[5:]: d[k] for k in d.files if k.startswith("outi_")}
     outi["noise"] = {k[7:]: d[k].astype(np.float64) for k in d.files if k.startswith("noisei_")}
+    # the reference's next FlashFIM from the initialised state
+    nxt = {k[5:]: d[k] for k in d.files if k.startswith("out2_")}
+    nxt["noise"] = {k[7:]: d[k].astype(np.float64) for k in d.files if k.startswith("noise2_")}
+    nxt["fragile"] = d["fragile2"]
+    out["next"] = nxt
     return fl, inp, out, outi, d["fragile"]
 
 

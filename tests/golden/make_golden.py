@@ -179,6 +179,11 @@ def impec_case():
     d["fragile"] = frag
     for k, v in noise.items():
         d[f"noise_{k}"] = v.astype(np.float32)
+    for k in OUT_KEYS:
+        d[f"out2_{k}"] = s2[k]
+    for k, v in noise2.items():
+        d[f"noise2_{k}"] = v.astype(np.float32)
+    d["fragile2"] = moved2
     path = os.path.join(HERE, "impec_nc6.npz")
     np.savez_compressed(path, **d)
     print(f"impec_nc6: n={n} two-phase={np.mean(r['NPhc'] == 2):.3f} ftype={np.bincount(r['ftype'], minlength=3)} "
@@ -192,7 +197,8 @@ def init_case():
     Vpore ~ U(50, 5000) ft3. The fixture holds the inputs, the reference's
     FIM outputs (out_*) and IMPEC outputs (outi_*), each with the moles Ni
     the flash object holds afterwards, the fragile mask and the self-noise
-    of both (``perturbed``)."""
+    of both (``perturbed``); and the reference's next FlashFIM from the
+    initialised state (out2_*, noise2_*, fragile2)."""
     from oracle import compare as CMP
     fl = synthetic_fluid(6, 1234)
 
@@ -220,7 +226,7 @@ def init_case():
 
     r, ri = run(P, T, z, False), run(P, T, z, True)
     frag = np.zeros(n, bool)
-    noise = {k: np.zeros(n) for k in CMP.FLOAT_KEYS + ("Ni",)}
+    noise = {k: np.zeros(n) for k in CMP.FLOAT_KEYS + ("Ni", "nj")}
     noisei = {k: np.zeros(n) for k in CMP.IMPEC_FLOAT_KEYS + ("Ni",)}
     prng = np.random.default_rng(7)
     for trial in range(CMP.NOISE_TRIALS):
@@ -229,13 +235,26 @@ def init_case():
         frag |= (rr["phaseNum"] != r["phaseNum"]) | (rri["phaseNum"] != ri["phaseNum"])
         e, ei = CMP.per_cell_errors(rr, r, fl.nc), CMP.impec_errors(rri, ri, fl.nc)
         e["Ni"] = CMP._rel(rr["Ni"], r["Ni"]).max(axis=1)
+        e["nj"] = np.nan_to_num(CMP._rel(rr["nj"][:, :2], r["nj"][:, :2]), nan=0.0).max(axis=1)
         ei["Ni"] = CMP._rel(rri["Ni"], ri["Ni"]).max(axis=1)
         for k in noise:
             noise[k] = np.fmax(noise[k], np.nan_to_num(e[k], nan=0.0))
         for k in noisei:
             noisei[k] = np.fmax(noisei[k], np.nan_to_num(ei[k], nan=0.0))
+    # the next FlashFIM from the initialised state (IsoT_FIM's first Newton
+    # iteration at unchanged P, T): warm start from the initialisation's
+    # phase counts, saturations, compositions and skip cache
+    xij0 = np.nan_to_num(r["xij"], nan=0.0)
+    skip0 = {k: v.copy() for k, v in r["skip"].items()}
+
+    def step2(P, T, Ni):
+        return O.flash_fim("reference", fl, P, T, Ni, S=r["S"], lastNP=r["phaseNum"].astype(np.int32), xij=xij0,
+                           skip={k: v.copy() for k, v in skip0.items()}, nthreads=8)
+
+    s2 = step2(P, T, r["Ni"])
+    noise2, moved2 = CMP.self_noise(step2, P, T, r["Ni"], s2, fl.nc)
     d = fluid_arrays(fl)
-    d["note"] = np.array("InitFlashFIM / InitFlashIMPEC of initial states z, S_w, Vpore")
+    d["note"] = np.array("InitFlashFIM / InitFlashIMPEC of initial states z, S_w, Vpore; then one warm FlashFIM")
     d["in_P"], d["in_T"], d["in_z"], d["in_S"], d["in_Vpore"] = P, T, z, S, Vp
     for k in OUT_KEYS + ("Ni",):
         d[f"out_{k}"] = r[k]
@@ -247,11 +266,17 @@ def init_case():
     d["fragile"] = frag
     for k, v in noise.items():
         d[f"noise_{k}"] = v.astype(np.float32)
+    for k in OUT_KEYS:
+        d[f"out2_{k}"] = s2[k]
+    for k, v in noise2.items():
+        d[f"noise2_{k}"] = v.astype(np.float32)
+    d["fragile2"] = moved2
     for k, v in noisei.items():
         d[f"noisei_{k}"] = v.astype(np.float32)
     path = os.path.join(HERE, "init_nc6.npz")
     np.savez_compressed(path, **d)
     print(f"init_nc6: n={n} two-phase={np.mean(r['NPhc'] == 2):.3f} fragile={frag.sum()} "
+          f"step 2: phase changes={int(np.sum(s2['phaseNum'] != r['phaseNum']))} fragile={moved2.sum()} "
           f"size={os.path.getsize(path) / 1e6:.2f} MB")
 
 

@@ -324,21 +324,25 @@ def test_init_flash_matches_reference_golden(form, impec):
     if not impec:
         # hydrocarbon nj: the phase fractions, as the reference's CopyPhase leaves them
         ex = r["phaseExist"][:, :2].astype(bool) & same[:, None]
-        np.testing.assert_allclose(got["nj"][:, :2][ex], r["nj"][:, :2][ex], rtol=1e-8)
+        allowed = np.maximum(1e-8, 10 * r["noise"]["nj"])[:, None] * np.ones((1, 2))
+        e = CMP._rel(got["nj"][:, :2], r["nj"][:, :2])
+        assert np.all(e[ex] <= allowed[ex]), np.nonzero(np.any(ex & (e > allowed), axis=1))[0]
         sg, sr = got["skip"], ref["skip"]
         assert np.array_equal(sg["flag"][same].astype(int), sr["flag"][same].astype(int))
 
 
-def test_init_flash_then_fim_step_is_consistent():
-    """The state InitFlashFIM leaves is the one FlashFIM sees next: a
-    FlashFIM of the initialised moles at the same P and T, warm-started from
-    the initialisation's outputs, keeps every phase count and reproduces the
-    saturations and volumes to the flash's convergence tolerance (the pore
-    volume stays filled)."""
+def test_init_flash_then_fim_step_matches_reference():
+    """IsoT_FIM's start: InitFlashFIM, then the first FlashFIM at unchanged
+    P and T, warm-started from the initialisation's phase counts,
+    saturations, compositions and skip cache, against the reference making
+    the same two calls (the warm step changes a few phase counts in the
+    reference too: relaxed stability and skip tests replace the strict
+    test). The initialised state fills the pore volume."""
     import torch
     from conftest import load_golden_init
     from opencaeporo_b200.flash import MixtureCompBatch
     fl, inp, ref, _, fragile = load_golden_init()
+    nxt = ref["next"]
     m = MixtureCompBatch(fl)
     n = len(inp["P"])
     st = m.new_state(n)
@@ -346,12 +350,12 @@ def test_init_flash_then_fim_step_is_consistent():
     m.init_flash(st, inp["Vpore"], S=inp["S"], form="batched")
     torch.cuda.synchronize()
     a = st.to_host()
+    np.testing.assert_allclose(a["vf"], inp["Vpore"], rtol=1e-12)
     m.flash_fim(st, form="batched")
     torch.cuda.synchronize()
     b = st.to_host()
     m.close()
-    keep = ~fragile
-    assert np.array_equal(a["phaseNum"][keep], b["phaseNum"][keep])
-    np.testing.assert_allclose(a["vf"], inp["Vpore"], rtol=1e-12)
-    np.testing.assert_allclose(b["vf"], inp["Vpore"], rtol=1e-6)
-    np.testing.assert_allclose(b["S"][keep], a["S"][keep], atol=1e-6)
+    chk = CMP.check(b, nxt, fl.nc, noise=nxt["noise"], fragile=fragile | nxt["fragile"])
+    assert chk["ok"], CMP.check_summary(chk)
+    same = b["phaseNum"] == nxt["phaseNum"]
+    assert np.array_equal(b["ftype"][same], nxt["ftype"][same])

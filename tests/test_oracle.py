@@ -153,3 +153,13 @@ def test_reference_reproduces_init_golden(impec):
         assert np.nanmax(e[k]) == 0.0, k
     assert np.array_equal(got["Ni"], r["Ni"])
     np.testing.assert_allclose(got["vf"], inp["Vpore"], rtol=1e-12)
+    if not impec:
+        # the fixture's next FlashFIM from the initialised state
+        nxt = ref["next"]
+        s2 = O.flash_fim("reference", fl, inp["P"], inp["T"], got["Ni"], S=got["S"],
+                         lastNP=got["phaseNum"].astype(np.int32), xij=np.nan_to_num(got["xij"], nan=0.0),
+                         skip=got["skip"], nthreads=4)
+        e2 = CMP.per_cell_errors(s2, nxt, fl.nc)
+        assert e2["same"].all()
+        for k in CMP.FLOAT_KEYS:
+            assert np.nanmax(e2[k]) == 0.0, k
