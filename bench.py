@@ -556,6 +556,36 @@ def entries_arm(args):
             "parity_on_sample": {"cells": ns, "phase_count_mismatches": int(np.count_nonzero(~e["same"])),
                                  "well_determined_cells": int(det.sum()),
                                  "share_well_determined_le_1e-8": float(np.mean(worst[det] <= 1e-8))}}
+    # relative permeability and capillary pressure of the flash's S in place
+    # (ocpf_cal_krpc, FlowUnit_ODGW01 on two synthetic regions); HBM-bound
+    from oracle import krpc as KO
+    from opencaeporo_b200 import synth
+    from opencaeporo_b200.krpc import FlowUnitBatch
+    regions = [synth.corey_tables(501), synth.corey_tables(502, swc=0.2, sorw=0.15, nrow=9, pc_scale=(8.0, 3.0))]
+    fu = FlowUnitBatch(regions)
+    satnum = torch.as_tensor(np.random.default_rng(SEED + 2).integers(0, 2, n).astype(np.int32)).cuda()
+    kout = fu.new_outputs(n)
+    t_k = timed(lambda: None, lambda: fu.cal_krpc(st.P, st.out["S"], satnum, out=kout))
+    ns = min(n, 65536)
+    Sh = st.out["S"][:, :ns].cpu().numpy().T.copy()
+    sh = satnum[:ns].cpu().numpy()
+    want = KO.reference(regions, w["P"][:ns], Sh, sh, nthreads=os.cpu_count() or 1)
+    exact = all(np.array_equal(kout[k][:, :ns].cpu().numpy().T, want[k])
+                for k in ("kr", "Pc", "Pj", "dKr_dS", "dPcj_dS"))
+    kbytes = n * (8 + 24 + 4 + 3 * 24 + 2 * 72)
+    try:
+        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        peak = None
+    res["cal_krpc"] = {
+        "value": n / (t_k * 1e-3), "unit": "cells/s", "ms_per_step": t_k,
+        "roofline": {"bound": "hbm", "achieved": kbytes / (t_k * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": (kbytes / (t_k * 1e-3) / 1e9 / peak) if peak else None,
+                     "bytes_per_launch": kbytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+        "reference_cpu": {"value": ns / want["seconds"], "unit": "cells/s", "cores": os.cpu_count() or 1,
+                          "sample": f"first {ns} cells"},
+        "bit_identical_on_sample": bool(exact)}
+    fu.close()
     m.close()
     print(json.dumps({
         "metric": "flash states/s of the initialisation and IMPEC entry points", "n_gpus": 1,

@@ -50,6 +50,7 @@ extern "C" {
 
 /* largest batch ocpf_flash_fim_noalloc accepts */
 #define OCPF_NOALLOC_MAX_CELLS 4096
+#define OCPF_KRPC_MAX_REGIONS 64 /* saturation regions (SATNUM values) per ocpf_krpc handle */
 
 /* per-cell status bits (ocpf_fim_out.status) */
 #define OCPF_CELL_SSMSTA_CAP 0x01  /* a stability SSM trial hit maxIt */
@@ -361,6 +362,59 @@ int ocpf_set_initializer(ocpf_ctx* ctx, const float* params, const float* in_mea
  * together (per division), [2] FMA, [3] exp, [4] log, [5] acos + cos. No
  * reference counterpart (measurement utility). */
 int ocpf_measure_fp64_latency(int device, double* cycles);
+
+/* ---------------------------------------------------------------------
+ * Relative permeability and capillary pressure after the flash
+ * (IsoT_FIM::CalKrPc / IsoT_IMPEC::CalKrPc, src/OCPFluidMethod.cpp:
+ * 1189-1199 and :311-319, with the compositional model's default flow unit
+ * FlowUnit_ODGW01, src/FlowUnit.cpp:183-349, chosen by Bulk::Setup when
+ * there is no SOF3 table and no miscibility, src/Bulk.cpp:271-279).
+ * --------------------------------------------------------------------- */
+
+/* The SWOF and SGOF tables of one saturation region, in host memory, rows
+ * as the keywords list them (4 columns, row-major): Sw, krw, krow, Pcow and
+ * Sg, krg, krog, Pcgo. The first column of each must not decrease. */
+typedef struct {
+    int32_t       nrow_swof, nrow_sgof;
+    const double* swof;
+    const double* sgof;
+} ocpf_satfunc;
+
+typedef struct ocpf_krpc ocpf_krpc;
+
+/* Device inputs: P [ncell], the flash's S [3][ncell] (oil, gas, water), and
+ * the region of each cell (Bulk::SATNUM) or null for region 0. */
+typedef struct {
+    const double*  P;
+    const double*  S;
+    const int32_t* satnum;
+} ocpf_krpc_in;
+
+/* Device outputs (Bulk::kr, Pc, Pj, dKr_dS, dPcj_dS): kr, Pc, Pj
+ * [3][ncell]; dKr_dS, dPcj_dS [9][ncell] with entry 3 j + k = d/dS_k of
+ * phase j. Both derivative arrays null: the IMPEC call (no derivatives). */
+typedef struct {
+    double* kr;
+    double* Pc;
+    double* Pj;
+    double* dKr_dS;
+    double* dPcj_dS;
+} ocpf_krpc_out;
+
+/* Builds the device tables of nregion regions (FlowUnit_ODGW01's
+ * constructor, src/FlowUnit.cpp:183-203): OCPF_EINVAL for a table with
+ * fewer than 2 rows or a decreasing first column, OCPF_EUNSUPPORTED when
+ * the tables exceed 48 KB together. */
+int ocpf_krpc_create(const ocpf_satfunc* regions, int nregion, int device, ocpf_krpc** out);
+int ocpf_krpc_destroy(ocpf_krpc* k);
+
+/* For every cell: SWOF at S_w and SGOF at S_g (OCPTable::Eval_All, linear
+ * interpolation, flat outside the table), Stone II kro (negative values
+ * clipped to 0 with their derivatives), Pc = (0, Pcgo, -Pcow), Pj = P + Pc,
+ * and with derivative outputs CalKrPcDeriv's dKr_dS and dPcj_dS. A cell
+ * whose region does not exist gets NaN outputs. Results equal the
+ * reference's bit for bit. Asynchronous on `stream`. */
+int ocpf_cal_krpc(ocpf_krpc* k, int64_t ncell, const ocpf_krpc_in* in, const ocpf_krpc_out* out, void* stream);
 
 #ifdef __cplusplus
 }

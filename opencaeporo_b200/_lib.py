@@ -35,7 +35,8 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_measure_fma_peak", "ocpf_reserve", "ocpf_flash_fim_noalloc",
            "ocpf_mlp_param_count", "ocpf_mlp_forward", "ocpf_mlp_grad", "ocpf_mlp_adam",
            "ocpf_set_initializer", "ocpf_flash_fim_regions", "ocpf_measure_fp64_latency",
-           "ocpf_flash_impec", "ocpf_init_flash_fim", "ocpf_init_flash_impec")
+           "ocpf_flash_impec", "ocpf_init_flash_fim", "ocpf_init_flash_impec",
+           "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc")
 
 _vp = C.c_void_p
 
@@ -89,6 +90,19 @@ class ImpecOut(C.Structure):
 
 
 INIT_IN_FIELDS = ("P", "T", "S", "Vpore", "zi")
+KRPC_OUT_FIELDS = ("kr", "Pc", "Pj", "dKr_dS", "dPcj_dS")
+
+
+class Satfunc(C.Structure):
+    _fields_ = [("nrow_swof", C.c_int32), ("nrow_sgof", C.c_int32), ("swof", _vp), ("sgof", _vp)]
+
+
+class KrpcIn(C.Structure):
+    _fields_ = [("P", _vp), ("S", _vp), ("satnum", _vp)]
+
+
+class KrpcOut(C.Structure):
+    _fields_ = [(f, _vp) for f in KRPC_OUT_FIELDS]
 
 
 class InitIn(C.Structure):
@@ -179,6 +193,12 @@ def lib():
     L.ocpf_init_flash_impec.argtypes = [_vp, C.c_int64, C.POINTER(InitIn), C.POINTER(Skip), _vp,
                                         C.POINTER(ImpecOut), C.c_int, _vp]
     L.ocpf_init_flash_impec.restype = C.c_int
+    L.ocpf_krpc_create.argtypes = [C.POINTER(Satfunc), C.c_int, C.c_int, C.POINTER(_vp)]
+    L.ocpf_krpc_create.restype = C.c_int
+    L.ocpf_krpc_destroy.argtypes = [_vp]
+    L.ocpf_krpc_destroy.restype = C.c_int
+    L.ocpf_cal_krpc.argtypes = [_vp, C.c_int64, C.POINTER(KrpcIn), C.POINTER(KrpcOut), _vp]
+    L.ocpf_cal_krpc.restype = C.c_int
     _LIB = L
     return L
 

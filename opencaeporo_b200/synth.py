@@ -115,3 +115,24 @@ def mixed_states(fluid: Fluid, n: int, seed: int, phase_count, near_frac: float 
     base["near_mask"] = np.zeros(n, bool)
     base["near_mask"][pos] = True
     return base
+
+
+def corey_tables(seed, swc=0.15, sorw=0.2, sgc=0.05, sorg=0.1, nrow=12, pc_scale=(4.0, 1.5)):
+    """Seeded synthetic SWOF / SGOF rows (Corey-type curves with random
+    exponents and end points; capillary pressures falling with saturation),
+    the layout the keywords use: (Sw, krw, krow, Pcow), (Sg, krg, krog, Pcgo)."""
+    rng = np.random.default_rng(seed)
+    nw, now, ng, nog = rng.uniform(1.5, 4.0, 4)
+    sw = np.linspace(swc, 1.0, nrow)
+    swn = np.clip((sw - swc) / (1 - swc - sorw), 0, 1)
+    krw = rng.uniform(0.3, 1.0) * swn ** nw
+    krow = np.clip((1 - sw - sorw) / (1 - swc - sorw), 0, 1) ** now
+    pcow = pc_scale[0] * (1 - swn) ** 2
+    swof = np.stack([sw, krw, krow, pcow], axis=1)
+    sg = np.linspace(0.0, 1 - swc - sorg, nrow)
+    sgn = np.clip((sg - sgc) / (1 - swc - sgc - sorg), 0, 1)
+    krg = rng.uniform(0.5, 1.0) * sgn ** ng
+    krog = np.clip((1 - swc - sorg - sg) / (1 - swc - sorg), 0, 1) ** nog
+    pcgo = pc_scale[1] * sg / sg[-1]
+    sgof = np.stack([sg, krg, krog, pcgo], axis=1)
+    return swof, sgof

@@ -131,6 +131,36 @@ int orc_flash_impec_batch(const orc_fluid* fluid, const orc_batch* batch, double
 int orc_init_flash_batch(const orc_fluid* fluid, const orc_batch* batch, const double* Vpore, int impec,
                          double* Ni, double* vj, int nthreads, double* seconds);
 
+/* Saturation functions of one region, as the SWOF and SGOF keywords list
+ * them (row-major, 4 columns): Sw, krw, krow, Pcow and Sg, krg, krog, Pcgo. */
+typedef struct {
+    int32_t       nrow_swof, nrow_sgof;
+    const double* swof;
+    const double* sgof;
+} orc_satfunc;
+
+/* One batch of FlowUnit::CalKrPcDeriv (or CalKrPc) calls, cell-major (Bulk
+ * layout): S [n*3] in; kr, Pc, Pj = P + Pc [n*3] and, with deriv,
+ * dKr_dS, dPcj_dS [n*9] (row j: d/dS_k of phase j) out. */
+typedef struct {
+    int64_t        n;
+    int32_t        deriv;
+    const double*  P;      /* [n] */
+    const double*  S;      /* [n*3] */
+    const int32_t* satnum; /* [n] region of each cell, or null: region 0 */
+    double*        kr;
+    double*        Pc;
+    double*        Pj;
+    double*        dKr_dS;
+    double*        dPcj_dS;
+} orc_krpc_batch;
+
+/* IsoT_FIM::CalKrPc (src/OCPFluidMethod.cpp:1189-1199) with the
+ * compositional model's default flow unit, FlowUnit_ODGW01
+ * (src/FlowUnit.cpp:183-349: SWOF / SGOF interpolation, Stone II oil
+ * relative permeability). The reference oracle only. */
+int orc_krpc(int nreg, const orc_satfunc* reg, const orc_krpc_batch* batch, int nthreads, double* seconds);
+
 /* Identifies the implementation: "reference" or "port". */
 const char* orc_kind(void);
 

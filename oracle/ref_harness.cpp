@@ -5,7 +5,9 @@
  * reference sources by oracle/Makefile into oracle/_ref/libocpref.so). For each
  * cell it makes exactly the calls IsoT_FIM::CalFlash makes
  * (src/OCPFluidMethod.cpp:1108-1120): MixtureComp::FlashFIM followed by the
- * copy-out of IsoT_FIM::PassFlashValue (src/OCPFluidMethod.cpp:1122-1187).
+ * copy-out of IsoT_FIM::PassFlashValue (src/OCPFluidMethod.cpp:1122-1187);
+ * likewise FlashIMPEC, InitFlashFIM / InitFlashIMPEC and, after the flash,
+ * IsoT_FIM::CalKrPc with FlowUnit_ODGW01 (src/FlowUnit.cpp).
  * Nothing of the reference is copied here; its headers are included and its
  * objects linked. The access specifiers are opened only to read the
  * iteration counters, the flash type, the hydrocarbon phase count and the
@@ -24,6 +26,7 @@
 
 #define private public
 #define protected public
+#include "FlowUnit.hpp"
 #include "MixtureComp.hpp"
 #include "OptionalFeatures.hpp"
 #include "ParamReservoir.hpp"
@@ -337,6 +340,55 @@ extern "C" int orc_init_flash_batch(const orc_fluid* fluid, const orc_batch* bat
                        [fluid, batch, Vpore, impec, Ni, vj](int64_t lo, int64_t hi, double* s) {
                            run_chunk_init(*fluid, *batch, Vpore, impec, Ni, vj, lo, hi, s);
                        });
+}
+
+// IsoT_FIM::CalKrPc (src/OCPFluidMethod.cpp:1189-1199) or, without
+// derivatives, IsoT_IMPEC::CalKrPc, over cells [lo, hi) with one
+// FlowUnit_ODGW01 per saturation region of this thread (the tables keep a
+// search position, so threads do not share them).
+static void run_chunk_krpc(int nreg, const orc_satfunc* reg, const orc_krpc_batch* b, int64_t lo, int64_t hi,
+                           double* secs)
+{
+    ParamReservoir rs;
+    auto cols = [](const double* rows, int nrow) {
+        std::vector<std::vector<OCP_DBL>> c(4, std::vector<OCP_DBL>(nrow));
+        for (int r = 0; r < nrow; r++)
+            for (int k = 0; k < 4; k++) c[k][r] = rows[r * 4 + k];
+        return c;
+    };
+    for (int i = 0; i < nreg; i++) {
+        rs.SWOF_T.data.push_back(cols(reg[i].swof, reg[i].nrow_swof));
+        rs.SGOF_T.data.push_back(cols(reg[i].sgof, reg[i].nrow_sgof));
+    }
+    std::vector<FlowUnit_ODGW01*> fu;
+    for (int i = 0; i < nreg; i++) fu.push_back(new FlowUnit_ODGW01(rs, static_cast<USI>(i)));
+    auto t0 = std::chrono::steady_clock::now();
+    for (int64_t n = lo; n < hi; n++) {
+        const int r = b->satnum ? b->satnum[n] : 0;
+        if (b->deriv)
+            fu[r]->CalKrPcDeriv(b->S + 3 * n, b->kr + 3 * n, b->Pc + 3 * n, b->dKr_dS + 9 * n, b->dPcj_dS + 9 * n,
+                                static_cast<OCP_USI>(n));
+        else
+            fu[r]->CalKrPc(b->S + 3 * n, b->kr + 3 * n, b->Pc + 3 * n, static_cast<OCP_USI>(n));
+        for (int j = 0; j < 3; j++) b->Pj[3 * n + j] = b->P[n] + b->Pc[3 * n + j];
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    *secs   = std::chrono::duration<double>(t1 - t0).count();
+    for (auto* f : fu) delete f;
+}
+
+extern "C" int orc_krpc(int nreg, const orc_satfunc* reg, const orc_krpc_batch* b, int nthreads, double* seconds)
+{
+    if (nreg < 1 || !reg || !b || !b->P || !b->S || !b->kr || !b->Pc || !b->Pj) return 1;
+    if (b->deriv && (!b->dKr_dS || !b->dPcj_dS)) return 1;
+    for (int i = 0; i < nreg; i++)
+        if (!reg[i].swof || !reg[i].sgof || reg[i].nrow_swof < 2 || reg[i].nrow_sgof < 2) return 1;
+    if (b->satnum)
+        for (int64_t n = 0; n < b->n; n++)
+            if (b->satnum[n] < 0 || b->satnum[n] >= nreg) return 1;
+    return run_threads(b->n, nthreads, seconds, [nreg, reg, b](int64_t lo, int64_t hi, double* s) {
+        run_chunk_krpc(nreg, reg, b, lo, hi, s);
+    });
 }
 
 extern "C" const char* orc_kind(void) { return "reference"; }

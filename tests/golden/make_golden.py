@@ -11,7 +11,7 @@ edge of an iteration cap or a stability threshold; any implementation whose
 rounding differs from the reference's may legitimately land on either side.
 
     python tests/golden/make_golden.py            # writes tests/golden/*.npz
-    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6)
+    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6, krpc)
 """
 from __future__ import annotations
 
@@ -280,12 +280,53 @@ def init_case():
           f"size={os.path.getsize(path) / 1e6:.2f} MB")
 
 
+def krpc_case():
+    """IsoT_FIM::CalKrPc with FlowUnit_ODGW01 on two saturation regions of
+    synthetic tables (the second with a repeated saturation node), 4096
+    cells: random saturations, every table node exactly, values outside the
+    tables and NaN. Outputs of the compiled reference (derivatives
+    included)."""
+    from oracle import krpc as K
+    r0 = synth.corey_tables(501)
+    w1, g1 = synth.corey_tables(502, swc=0.2, sorw=0.15, nrow=9, pc_scale=(8.0, 3.0))
+    w1 = np.insert(w1, 4, w1[4], axis=0)  # a repeated node
+    regions = [r0, (w1, g1)]
+    rng = np.random.default_rng(503)
+    n = 4096
+    S = np.zeros((n, 3))
+    S[:, 2] = rng.uniform(-0.05, 1.05, n)
+    S[:, 1] = rng.uniform(-0.05, 1.0, n)
+    S[:, 0] = 1 - S[:, 1] - S[:, 2]
+    satnum = rng.integers(0, 2, n).astype(np.int32)
+    k = 0
+    for r, (w, g) in enumerate(regions):
+        for v in w[:, 0]:
+            S[k, 2], satnum[k] = v, r
+            k += 1
+        for v in g[:, 0]:
+            S[k, 1], satnum[k] = v, r
+            k += 1
+    S[k:k + 4, 1:] = [[np.nan, 0.3], [0.1, np.nan], [np.inf, -np.inf], [-np.inf, np.inf]]
+    P = rng.uniform(500.0, 6000.0, n)
+    out = K.reference(regions, P, S, satnum, deriv=True, nthreads=8)
+    d = {"note": np.array("CalKrPc, FlowUnit_ODGW01, two synthetic regions"), "in_P": P, "in_S": S,
+         "in_satnum": satnum}
+    for i, (w, g) in enumerate(regions):
+        d[f"swof{i}"], d[f"sgof{i}"] = w, g
+    for key in ("kr", "Pc", "Pj", "dKr_dS", "dPcj_dS"):
+        d[f"out_{key}"] = out[key]
+    path = os.path.join(HERE, "krpc.npz")
+    np.savez_compressed(path, **d)
+    print(f"krpc: n={n} size={os.path.getsize(path) / 1e6:.2f} MB")
+
+
 def main(only=()):
     if not O.available("reference"):
         raise SystemExit("oracle/_ref/libocpref.so missing: run `make -C oracle ref` first")
     if only:
         for name in only:
-            {"restart_nc6": restart_case, "impec_nc6": impec_case, "init_nc6": init_case}[name]()
+            {"restart_nc6": restart_case, "impec_nc6": impec_case, "init_nc6": init_case,
+             "krpc": krpc_case}[name]()
         return
 
     # 1) SPE5 fluid (examples/spe5/EGOIL.in) at 160 degF, the deck's initial composition
@@ -343,6 +384,9 @@ def main(only=()):
 
     # 8) the initialisation flashes
     init_case()
+
+    # 9) relative permeability and capillary pressure after the flash
+    krpc_case()
 
 
 if __name__ == "__main__":
