@@ -42,10 +42,17 @@ __device__ __forceinline__ double phi_term(double bi, double ti, double ia, doub
     return exp(bi * zm1 - L1 - cf * (2 * ti * ia - bi) * L2);
 }
 
-// The per-phase logarithms of CalFugPhi, ln(Z - b) and ln((Z + d1 b) /
-// (Z + d2 b)), as separate pieces (a warp forms them on different lanes).
-__device__ __forceinline__ double fug_L1(double zj, double bj) { return log(zj - bj); }
-__device__ __forceinline__ double fug_L2(double zj, double bj) { return log((zj + D1 * bj) / (zj + D2 * bj)); }
+// The per-phase pieces of CalFugPhi: q = 0: ln(Z - b), 1: ln((Z + d1 b) /
+// (Z + d2 b)), 2: 1 / b, 3: 1 / a. One division and at most one logarithm
+// with operands chosen by q, so that the lanes of a warp forming different
+// pieces run one instruction stream.
+__device__ __forceinline__ double fug_piece(int q, double zj, double aj, double bj)
+{
+    const double num = q == 0 ? zj - bj : (q == 1 ? zj + D1 * bj : 1.0);
+    const double den = q == 0 ? 1.0 : (q == 1 ? zj + D2 * bj : (q == 2 ? bj : aj));
+    const double d   = num / den;
+    return q <= 1 ? log(d) : d;
+}
 
 // CalFugPhi (src/MixtureComp.cpp:993-1101): the fugacity coefficients phi
 // and fugacities f = phi x P of composition xj (phiT may be null), with the
@@ -58,10 +65,10 @@ __device__ __forceinline__ void fug_phi(const FluidConst& F, const double* sA, c
     double t[NC];
     mix_ab<NC>(F, sA, Bi, xj, t, aj, bj);
     zj               = sol_eos(aj, bj);
-    const double L1  = fug_L1(zj, bj);
-    const double L2  = fug_L2(zj, bj);
-    const double ib  = 1.0 / bj;
-    const double ia  = 1.0 / aj;
+    const double L1  = fug_piece(0, zj, aj, bj);
+    const double L2  = fug_piece(1, zj, aj, bj);
+    const double ib  = fug_piece(2, zj, aj, bj);
+    const double ia  = fug_piece(3, zj, aj, bj);
     const double cf  = div_const(aj, D1MD2, RCPD1MD2) * ib;
     const double zm1 = zj - 1;
 #pragma unroll

@@ -71,15 +71,18 @@ struct PrCubic {
 // sign of the Gibbs-energy difference (src/MixtureComp.cpp:895-911), in
 // pieces (two logarithms and a coefficient) that a warp can form on
 // different lanes; pick_root_from combines them in one fixed expression.
-__device__ __forceinline__ double gibbs_log1(double zmin, double zmax, double bj)
+//   k = 0: ln((zmin - b) / (zmax - b)),
+//   k = 1: ln((zmin + d1 b)(zmax + d2 b) / ((zmin + d2 b)(zmax + d1 b))),
+//   k = 2: a / (b (d2 - d1)).
+// One division and at most one logarithm, with the operands chosen by k, so
+// that lanes forming different pieces run one instruction stream.
+__device__ __forceinline__ double gibbs_piece(int k, double zmin, double zmax, double aj, double bj)
 {
-    return log((zmin - bj) / (zmax - bj));
+    const double num = k == 0 ? zmin - bj : (k == 1 ? (zmin + D1 * bj) * (zmax + D2 * bj) : aj);
+    const double den = k == 0 ? zmax - bj : (k == 1 ? (zmin + D2 * bj) * (zmax + D1 * bj) : bj * (D2 - D1));
+    const double d   = num / den;
+    return k <= 1 ? log(d) : d;
 }
-__device__ __forceinline__ double gibbs_log2(double zmin, double zmax, double bj)
-{
-    return log((zmin + D1 * bj) * (zmax + D2 * bj) / ((zmin + D2 * bj) * (zmax + D1 * bj)));
-}
-__device__ __forceinline__ double gibbs_coef(double aj, double bj) { return aj / (bj * (D2 - D1)); }
 __device__ __forceinline__ double pick_root_from(double zmin, double zmax, double g1, double g2, double k)
 {
     const double dG = (zmax - zmin) + g1 - k * g2;
@@ -89,7 +92,8 @@ __device__ __forceinline__ double pick_root(double z0, double z1, double z2, dou
 {
     const double zmin = fmin(z0, fmin(z1, z2));
     const double zmax = fmax(z0, fmax(z1, z2));
-    return pick_root_from(zmin, zmax, gibbs_log1(zmin, zmax, bj), gibbs_log2(zmin, zmax, bj), gibbs_coef(aj, bj));
+    return pick_root_from(zmin, zmax, gibbs_piece(0, zmin, zmax, aj, bj), gibbs_piece(1, zmin, zmax, aj, bj),
+                          gibbs_piece(2, zmin, zmax, aj, bj));
 }
 
 // Z factor of the PR cubic for mixture parameters (aj, bj): Cardano /
@@ -126,13 +130,7 @@ __device__ __forceinline__ double sol_eos_group(double aj, double bj, unsigned m
         const double z2    = __shfl_sync(mask, zk, base + 2);
         const double zmin  = fmin(z0, fmin(z1, z2));
         const double zmax  = fmax(z0, fmax(z1, z2));
-        double       piece;
-        if (rank == 0)
-            piece = gibbs_log1(zmin, zmax, bj);
-        else if (rank == 1)
-            piece = gibbs_log2(zmin, zmax, bj);
-        else
-            piece = gibbs_coef(aj, bj);
+        const double piece = gibbs_piece(rank < 3 ? rank : 2, zmin, zmax, aj, bj);
         const double g1 = __shfl_sync(mask, piece, base);
         const double g2 = __shfl_sync(mask, piece, base + 1);
         const double k  = __shfl_sync(mask, piece, base + 2);

@@ -21,6 +21,9 @@
 //     the three pieces of the root choice, lanes 0-3 the two logarithms and
 //     two reciprocals of CalFugPhi, and lane 16j + i the exponential of
 //     phi_ij.
+// Lanes that form different pieces run the same instructions on operands
+// chosen per lane (one division, then one logarithm): different functions
+// on different lanes of a warp would run one after another.
 // Each value is formed by the same expression as in the one-thread form
 // (shared helpers), so results and iteration counts equal the one-thread
 // form's bit for bit.
@@ -89,7 +92,8 @@ struct WarpSplit {
         int          iter = 0;
         while (true) {
             const double tmp  = 1 + v * km1;
-            const double term = half ? -(num / (tmp * tmp)) : num / tmp;
+            const double quo  = num / (half ? tmp * tmp : tmp);
+            const double term = half ? -quo : quo;
             double       sum  = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) sum += __shfl_sync(WARP_ALL, term, src + i);
@@ -121,16 +125,8 @@ struct WarpSplit {
         double t[NC];
         mix_ab<NC>(f.F, f.sA, f.Bi, xj, t, aj, bj);
         zj              = sol_eos_group(aj, bj, hmask, half << 4, q);
-        const int base  = half << 4;
-        double    piece;
-        if (q == 0)
-            piece = fug_L1(zj, bj);
-        else if (q == 1)
-            piece = fug_L2(zj, bj);
-        else if (q == 2)
-            piece = 1.0 / bj;
-        else
-            piece = 1.0 / aj;
+        const int    base  = half << 4;
+        const double piece = fug_piece(q < 4 ? q : 3, zj, aj, bj);
         const double L1  = __shfl_sync(WARP_ALL, piece, base);
         const double L2  = __shfl_sync(WARP_ALL, piece, base + 1);
         const double ib  = __shfl_sync(WARP_ALL, piece, base + 2);
@@ -218,7 +214,8 @@ struct WarpSplit {
             const double pho = __shfl_xor_sync(WARP_ALL, ph, 16);
             // lane q: component q's squared fugacity-ratio residual; lane
             // 16 + q: its new K
-            v = half ? ph / pho : sq(pho * x1q * f.P / (ph * x0q * f.P) - 1);
+            const double quo = (half ? ph : pho * x1q * f.P) / (half ? pho : ph * x0q * f.P);
+            v                = half ? quo : sq(quo - 1);
             double Kg[NC];
             Se = 0;
 #pragma unroll
