@@ -237,6 +237,7 @@ def our_arm(args):
     shards.barrier()
     ms_total = t0.elapsed_time(t1)
     kern_ms = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+    per_call = m.last_launch_count()  # kernels of one flash call (the replayed sequence)
     res = st.to_host()
 
     # the plain FP64 GPU form on the same states, for the headline ratio
@@ -273,8 +274,11 @@ def our_arm(args):
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
     ach_tf = fl_launch / (kern_ms * 1e-3) / 1e12
     ach_gbs = by_launch / (kern_ms * 1e-3) / 1e9
+    # DRAM bytes of one flash call from an ncu capture (profiles/): the plain
+    # kernel, or the batched sequence of the chosen form
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "flash_plain_nc6_traffic.json")
+    tf = os.path.join(ROOT, "profiles", "flash_plain_nc6_traffic.json" if args.form == "plain"
+                      else f"flash_phased_nc6_{args.form}_traffic.json")
     if os.path.exists(tf):
         try:
             traffic = json.load(open(tf)).get("bytes_per_launch_1M")
@@ -290,7 +294,8 @@ def our_arm(args):
                                "5 % of the saturation pressure", "form": args.form, "cells_per_gpu": n,
                    "l2": "flushed between steps (256 MiB write)", "parallelism": f"independent shards x{world}",
                    "two_phase_share": float(np.mean(nphc == 2)), "near_envelope_share": 0.3},
-        "gpu_launches": args.steps,
+        "gpu_launches": args.steps * per_call if per_call > 0 else None,
+        "gpu_launches_per_step": per_call,
         "roofline": {"bound": "fp64", "achieved": ach_tf, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": ach_tf / fp64_peak, "traffic": traffic,
                      "peak_source": "FP64 FMA throughput measured in this run (ocpf_measure_fma_peak); "

@@ -310,6 +310,13 @@ int ocpf_flash_fim_host(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocp
  * CUDA events on its stream; waits for that kernel to finish. */
 int ocpf_last_kernel_ms(ocpf_ctx* ctx, float* ms);
 
+/* Number of kernels the last flash call on this context launched (1 for
+ * the plain form; for the batched forms the kernel nodes of the replayed
+ * launch sequence), or -1 when unknown (the first call of a sequence, which
+ * launches directly, or a call inside the caller's own stream capture). A
+ * measurement aid; no reference counterpart. */
+int ocpf_last_launch_count(ocpf_ctx* ctx, int* n);
+
 /* Measures the device's FMA throughput (TFLOP/s, FMA = 2 flops) in FP64
  * (bits = 64) or FP32 (bits = 32) with a short register-only kernel: the
  * compute-roofline denominator for the flash kernels. No reference

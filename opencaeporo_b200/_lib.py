@@ -36,7 +36,7 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_mlp_param_count", "ocpf_mlp_forward", "ocpf_mlp_grad", "ocpf_mlp_adam",
            "ocpf_set_initializer", "ocpf_flash_fim_regions", "ocpf_measure_fp64_latency",
            "ocpf_flash_impec", "ocpf_init_flash_fim", "ocpf_init_flash_impec",
-           "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc")
+           "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count")
 
 _vp = C.c_void_p
 
@@ -193,6 +193,8 @@ def lib():
     L.ocpf_init_flash_impec.argtypes = [_vp, C.c_int64, C.POINTER(InitIn), C.POINTER(Skip), _vp,
                                         C.POINTER(ImpecOut), C.c_int, _vp]
     L.ocpf_init_flash_impec.restype = C.c_int
+    L.ocpf_last_launch_count.argtypes = [_vp, C.POINTER(C.c_int)]
+    L.ocpf_last_launch_count.restype = C.c_int
     L.ocpf_krpc_create.argtypes = [C.POINTER(Satfunc), C.c_int, C.c_int, C.POINTER(_vp)]
     L.ocpf_krpc_create.restype = C.c_int
     L.ocpf_krpc_destroy.argtypes = [_vp]

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "flash_phased.cuh"
 
@@ -146,6 +147,8 @@ struct ocpf_ctx {
     cudaGraphExec_t gexec;
     PhasedArgs      gkey;
     bool            gvalid;
+    int32_t         gkernels;      // kernel nodes of the captured graph
+    int32_t         last_kernels;  // kernels the last call launched, -1 unknown
 };
 
 static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
@@ -194,6 +197,8 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->rs        = nullptr;
     c->evf = c->evj = nullptr;
     c->launches  = 0;
+    c->gkernels     = 0;
+    c->last_kernels = -1;
     c->gs        = nullptr;
     c->gexec     = nullptr;
     c->gvalid    = false;
@@ -334,6 +339,7 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
 {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusInvalidated;
+    c->last_kernels = -1;
     if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, st);
     if (!(c->gvalid && std::memcmp(&c->gkey, &args, sizeof(args)) == 0)) {
         c->gvalid = false;
@@ -347,6 +353,17 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
             cudaGetLastError();
             return k(c->fc, args, st);
         }
+        size_t nn = 0;
+        int    nk = 0;
+        if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+            std::vector<cudaGraphNode_t> nodes(nn);
+            if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+                for (size_t i = 0; i < nn; i++) {
+                    cudaGraphNodeType t;
+                    if (cudaGraphNodeGetType(nodes[i], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) nk++;
+                }
+        }
+        c->gkernels = nk;
         bool ok = false;
         if (c->gexec) {
             cudaGraphExecUpdateResultInfo info;
@@ -367,6 +384,7 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
         c->gkey   = args;
         c->gvalid = true;
     }
+    c->last_kernels = c->gkernels;
     return cudaGraphLaunch(c->gexec, st);
 }
 
@@ -383,7 +401,8 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         const int64_t blocks = (count + bs - 1) / bs;
         if (blocks > 0x7fffffffLL) return OCPF_EINVAL;
         if (timed) cudaEventRecord(c->ev0, st);
-        e = k(c->fc, count, stride, in, sk, out, tail, (unsigned)blocks, bs, st);
+        e               = k(c->fc, count, stride, in, sk, out, tail, (unsigned)blocks, bs, st);
+        c->last_kernels = 1;
         if (timed) cudaEventRecord(c->ev1, st);
     } else {
         int            nd = 0;
@@ -552,6 +571,13 @@ extern "C" int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int6
     }
     if (prev != dev) cudaSetDevice(prev);
     return rc;
+}
+
+extern "C" int ocpf_last_launch_count(ocpf_ctx* c, int* n)
+{
+    if (!c || !n) return OCPF_EINVAL;
+    *n = c->last_kernels;
+    return OCPF_OK;
 }
 
 extern "C" int ocpf_last_kernel_ms(ocpf_ctx* c, float* ms)

@@ -218,6 +218,12 @@ class MixtureCompBatch:
         """Pre-allocates the batched forms' device scratch for ncell cells."""
         check(lib().ocpf_reserve(self._h, int(ncell)), "ocpf_reserve")
 
+    def last_launch_count(self) -> int:
+        """Kernels the last flash call launched (-1: unknown)."""
+        k = C.c_int(0)
+        check(lib().ocpf_last_launch_count(self._h, C.byref(k)), "ocpf_last_launch_count")
+        return int(k.value)
+
     def last_kernel_ms(self) -> float:
         ms = C.c_float(0)
         check(lib().ocpf_last_kernel_ms(self._h, C.byref(ms)), "ocpf_last_kernel_ms")
