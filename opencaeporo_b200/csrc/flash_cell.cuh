@@ -45,11 +45,12 @@ __device__ __forceinline__ double phi_term(double bi, double ti, double ia, doub
 // The per-phase pieces of CalFugPhi: q = 0: ln(Z - b), 1: ln((Z + d1 b) /
 // (Z + d2 b)), 2: 1 / b, 3: 1 / a. One division and at most one logarithm
 // with operands chosen by q, so that the lanes of a warp forming different
-// pieces run one instruction stream.
+// pieces run one instruction stream; explicit fused multiply-adds keep the
+// value independent of how a kernel contracts.
 __device__ __forceinline__ double fug_piece(int q, double zj, double aj, double bj)
 {
-    const double num = q == 0 ? zj - bj : (q == 1 ? zj + D1 * bj : 1.0);
-    const double den = q == 0 ? 1.0 : (q == 1 ? zj + D2 * bj : (q == 2 ? bj : aj));
+    const double num = q == 0 ? zj - bj : (q == 1 ? fma(D1, bj, zj) : 1.0);
+    const double den = q == 0 ? 1.0 : (q == 1 ? fma(D2, bj, zj) : (q == 2 ? bj : aj));
     const double d   = num / den;
     return q <= 1 ? log(d) : d;
 }
@@ -528,7 +529,7 @@ struct CellFlash {
             Se = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                Se += sq(fug[1][i] / fug[0][i] - 1);
+                Se = __dadd_rn(Se, sq(fug[1][i] / fug[0][i] - 1));  // never fused: the warp form adds rounded squares
                 Ks[i] = phi[1][i] / phi[0][i];
             }
             iter++;

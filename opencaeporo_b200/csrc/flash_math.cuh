@@ -75,11 +75,12 @@ struct PrCubic {
 //   k = 1: ln((zmin + d1 b)(zmax + d2 b) / ((zmin + d2 b)(zmax + d1 b))),
 //   k = 2: a / (b (d2 - d1)).
 // One division and at most one logarithm, with the operands chosen by k, so
-// that lanes forming different pieces run one instruction stream.
+// that lanes forming different pieces run one instruction stream; explicit
+// fused multiply-adds keep the value independent of how a kernel contracts.
 __device__ __forceinline__ double gibbs_piece(int k, double zmin, double zmax, double aj, double bj)
 {
-    const double num = k == 0 ? zmin - bj : (k == 1 ? (zmin + D1 * bj) * (zmax + D2 * bj) : aj);
-    const double den = k == 0 ? zmax - bj : (k == 1 ? (zmin + D2 * bj) * (zmax + D1 * bj) : bj * (D2 - D1));
+    const double num = k == 0 ? zmin - bj : (k == 1 ? fma(D1, bj, zmin) * fma(D2, bj, zmax) : aj);
+    const double den = k == 0 ? zmax - bj : (k == 1 ? fma(D2, bj, zmin) * fma(D1, bj, zmax) : bj * (D2 - D1));
     const double d   = num / den;
     return k <= 1 ? log(d) : d;
 }

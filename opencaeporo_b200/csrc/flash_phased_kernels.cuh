@@ -589,7 +589,7 @@ __device__ void sp_ssm_body(const FluidConst& F, const PhasedArgs& a, int r)
             double Se = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                Se += sq(fug1[i] / fug0[i] - 1);
+                Se = __dadd_rn(Se, sq(fug1[i] / fug0[i] - 1));
                 f.Ks[i] = f.phi[1][i] / f.phi[0][i];
             }
             iter++;

@@ -221,7 +221,7 @@ struct WarpSplit {
 #pragma unroll
             for (int i = 0; i < NC; i++) {
                 Kg[i] = __shfl_sync(WARP_ALL, v, src + i);
-                Se += Kg[i];
+                Se = __dadd_rn(Se, Kg[i]);
             }
             Se = __shfl_sync(WARP_ALL, Se, 0);
             Kq = __shfl_sync(WARP_ALL, v, 16 | q);

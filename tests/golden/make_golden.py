@@ -252,7 +252,16 @@ def init_case():
                            skip={k: v.copy() for k, v in skip0.items()}, nthreads=8)
 
     s2 = step2(P, T, r["Ni"])
-    noise2, moved2 = CMP.self_noise(step2, P, T, r["Ni"], s2, fl.nc)
+
+    # the sequence's own sensitivity: perturb the initial state and rerun
+    # both calls (an ill-determined initialisation carries its noise into
+    # the warm start of the next step)
+    def both(Pp, Tp, zp):
+        r1 = run(Pp, Tp, zp, False)
+        return O.flash_fim("reference", fl, Pp, Tp, r1["Ni"], S=r1["S"], lastNP=r1["phaseNum"].astype(np.int32),
+                           xij=np.nan_to_num(r1["xij"], nan=0.0), skip=r1["skip"], nthreads=8)
+
+    noise2, moved2 = CMP.self_noise(both, P, T, z, s2, fl.nc)
     d = fluid_arrays(fl)
     d["note"] = np.array("InitFlashFIM / InitFlashIMPEC of initial states z, S_w, Vpore; then one warm FlashFIM")
     d["in_P"], d["in_T"], d["in_z"], d["in_S"], d["in_Vpore"] = P, T, z, S, Vp
