@@ -10,12 +10,9 @@
 // of one another run on different lanes and are then broadcast with
 // shuffles:
 //   * Rachford-Rice: lane i forms component i's residual term, lane 16 + i
-//     its Jacobian term (two divisions); one shuffle per component gathers
-//     both halves' terms, half 0 sums the residual and half 1 the Jacobian
-//     in the reference's order;
-//   * compositions, fugacity ratios and K: one component per lane (lanes i
-//     and 16 + i); inside SplitSSM2's loop no lane holds the full state, it
-//     is gathered once when the loop ends;
+//     its Jacobian term (two divisions); the sums are then taken on every
+//     lane in the reference's order;
+//   * compositions, fugacity ratios and K: one component per lane;
 //   * fugacities: phase 0 on lanes 0-15 and phase 1 on lanes 16-31 at once;
 //     within a half, lanes 0-2 polish the three roots of the cubic and form
 //     the three pieces of the root choice, lanes 0-3 the two logarithms and
@@ -61,44 +58,36 @@ struct WarpSplit {
         return r;
     }
 
-    // The Rachford-Rice bracket [1 / (1 - Kmax), 1 / (1 - Kmin)] from all K
-    // (every lane holds them): lane 0 forms the lower end, lane 16 the upper.
-    __device__ __forceinline__ void rr_bracket(const double* K, double& numin, double& numax) const
+    // RachfordRice2, src/MixtureComp.cpp:1907-1959 (CellFlash::rachford_rice2):
+    // lane i forms component i's residual term, lane 16 + i its Jacobian
+    // term; the sums run on every lane in the reference's order.
+    __device__ void rachford_rice2()
     {
-        double Kmin = K[0], Kmax = K[0];
+        double Kmin = f.Ks[0], Kmax = f.Ks[0];
 #pragma unroll
         for (int i = 1; i < NC; i++) {
-            if (K[i] < Kmin) Kmin = K[i];
-            if (K[i] > Kmax) Kmax = K[i];
+            if (f.Ks[i] < Kmin) Kmin = f.Ks[i];
+            if (f.Ks[i] > Kmax) Kmax = f.Ks[i];
         }
         const double bound = 1 / (1 - (half ? Kmin : Kmax));
-        numin              = __shfl_sync(WARP_ALL, bound, 0);
-        numax              = __shfl_sync(WARP_ALL, bound, 16);
-    }
-
-    // RachfordRice2, src/MixtureComp.cpp:1907-1959 (CellFlash::rachford_rice2),
-    // from component q's K and z on lanes q and 16 + q and the bracket.
-    // Lane q forms component q's residual term and lane 16 + q its negated
-    // Jacobian term; one shuffle per component gathers each half's terms, so
-    // half 0 sums rj and half 1 sums J in the reference's order (x - y is
-    // x + (-y), so J equals the reference's J -= ... bit for bit).
-    __device__ void rachford_rice2(double Kq, double zq, double numin, double numax)
-    {
-        double       v   = 0.5 * (numin + numax);
-        const double km1 = Kq - 1;
-        const double zk  = zq * km1;
+        const double numin = __shfl_sync(WARP_ALL, bound, 0);
+        const double numax = __shfl_sync(WARP_ALL, bound, 16);
+        double       v     = 0.5 * (numin + numax);
+        // loop-invariant parts of component q's terms, formed as the
+        // one-thread form forms them: z km1 / tmp and z km1 km1 / (tmp tmp)
+        const double km1 = pick(f.Ks) - 1;
+        const double zk  = pick(f.zi) * km1;
         const double num = half ? zk * km1 : zk;
-        const int    src = lane & 16;
         int          iter = 0;
         while (true) {
             const double tmp  = 1 + v * km1;
-            const double quo  = num / (half ? tmp * tmp : tmp);
-            const double term = half ? -quo : quo;
-            double       sum  = 0;
+            const double term = num / (half ? tmp * tmp : tmp);
+            double       rj = 0, J = 0;
 #pragma unroll
-            for (int i = 0; i < NC; i++) sum += __shfl_sync(WARP_ALL, term, src + i);
-            const double rj = __shfl_sync(WARP_ALL, sum, 0);
-            const double J  = __shfl_sync(WARP_ALL, sum, 16);
+            for (int i = 0; i < NC; i++) {
+                rj += __shfl_sync(WARP_ALL, term, i);
+                J -= __shfl_sync(WARP_ALL, term, 16 + i);
+            }
             if (fabs(rj) < f.F.rr_tol || iter > f.F.rr_maxit) break;
             const double dnuj  = -rj / J;
             const double tmpnu = v + dnuj;
@@ -113,6 +102,19 @@ struct WarpSplit {
         f.it_rr += iter;
         f.nu[0] = v;
         f.nu[1] = 1 - v;
+    }
+
+    // UpdateXRR (src/MixtureComp.cpp:2030-2043): lane i forms x_1i and x_0i.
+    __device__ __forceinline__ void update_x()
+    {
+        const double tmp = 1 + f.nu[0] * (pick(f.Ks) - 1);
+        const double x1  = pick(f.zi) / tmp;
+        const double x0  = pick(f.Ks) * x1;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            f.x[1][i] = __shfl_sync(WARP_ALL, x1, i);
+            f.x[0][i] = __shfl_sync(WARP_ALL, x0, i);
+        }
     }
 
     // One phase of CalFugPhi (src/MixtureComp.cpp:993-1101) on each half:
@@ -174,12 +176,7 @@ struct WarpSplit {
     }
 
     // SplitSSM2 with UpdateXRR, src/MixtureComp.cpp:1847-1903, 2030-2043
-    // (CellFlash::split_ssm2 with the pieces above). Inside the loop lanes q
-    // and 16 + q keep component q's K, x and phi only: the compositions reach
-    // each half by one shuffle per component, the other phase's phi by one
-    // exchange between the halves, and the new K (lanes 16 + i) and the
-    // residual terms (lanes i) return by one gather per component. The full
-    // state is formed on every lane when the loop ends.
+    // (CellFlash::split_ssm2 with the pieces above).
     __device__ void split_ssm2(bool restart)
     {
         f.ssmsp_conflag = true;
@@ -194,61 +191,27 @@ struct WarpSplit {
             Stol *= 1e-1;
             maxIt *= 2;
         }
-        double numin, numax;
-        rr_bracket(f.Ks, numin, numax);
-        double       Kq  = pick(f.Ks);
-        const double zq  = pick(f.zi);
-        const int    src = lane & 16;
-        double       x0q = 0, x1q = 0, ph = 0, aj = 0, bj = 0, zj = 0, v = 0;
-        int          iter = 0;
+        int iter = 0;
         while (Se > Stol) {
-            rachford_rice2(Kq, zq, numin, numax);
-            // UpdateXRR for component q
-            const double tmp = 1 + f.nu[0] * (Kq - 1);
-            x1q              = zq / tmp;
-            x0q              = Kq * x1q;
-            double xj[NC];
-#pragma unroll
-            for (int k = 0; k < NC; k++) xj[k] = __shfl_sync(WARP_ALL, half ? x1q : x0q, src + k);
-            ph               = fug_lane(xj, aj, bj, zj);
-            const double pho = __shfl_xor_sync(WARP_ALL, ph, 16);
-            // lane q: component q's squared fugacity-ratio residual; lane
-            // 16 + q: its new K
-            const double quo = (half ? ph : pho * x1q * f.P) / (half ? pho : ph * x0q * f.P);
-            v                = half ? quo : sq(quo - 1);
-            double Kg[NC];
-            Se = 0;
+            rachford_rice2();
+            update_x();
+            fug_phi_all();
+            // lane i: component i's squared fugacity-ratio residual; lane
+            // 16 + i: its new K (one division on every lane)
+            const double quo = (half ? pick(f.phi[1]) : pick(f.fug[1])) / (half ? pick(f.phi[0]) : pick(f.fug[0]));
+            const double v   = half ? quo : sq(quo - 1);
+            Se               = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                Kg[i] = __shfl_sync(WARP_ALL, v, src + i);
-                Se = __dadd_rn(Se, Kg[i]);
+                Se      = __dadd_rn(Se, __shfl_sync(WARP_ALL, v, i));
+                f.Ks[i] = __shfl_sync(WARP_ALL, v, 16 + i);
             }
-            Se = __shfl_sync(WARP_ALL, Se, 0);
-            Kq = __shfl_sync(WARP_ALL, v, 16 | q);
-            // the next bracket from half 1's K: lane 16 forms 1 / (1 - Kmin),
-            // lane 17 1 / (1 - Kmax)
-            double Kmin = Kg[0], Kmax = Kg[0];
-#pragma unroll
-            for (int i = 1; i < NC; i++) {
-                if (Kg[i] < Kmin) Kmin = Kg[i];
-                if (Kg[i] > Kmax) Kmax = Kg[i];
-            }
-            const double bound = 1 / (1 - ((lane & 1) ? Kmax : Kmin));
-            numax              = __shfl_sync(WARP_ALL, bound, 16);
-            numin              = __shfl_sync(WARP_ALL, bound, 17);
             iter++;
             if (iter > maxIt) {
                 f.ssmsp_conflag = false;
                 break;
             }
         }
-#pragma unroll
-        for (int i = 0; i < NC; i++) {
-            f.Ks[i]   = __shfl_sync(WARP_ALL, v, 16 + i);
-            f.x[0][i] = __shfl_sync(WARP_ALL, x0q, i);
-            f.x[1][i] = __shfl_sync(WARP_ALL, x1q, i);
-        }
-        share_phases(ph, aj, bj, zj);
         f.ssmsp_realTol = sqrt(Se);
         f.it_ssmsp += iter;
     }
