@@ -10,7 +10,7 @@
 //     outcome of the cells whose SplitNR the reference itself cannot settle
 //     (it stops on a small step with a residual far above its tolerance;
 //     such cells' results follow the exact arithmetic path), so it stays
-//     FP64 and bit-identical to the batched form,
+//     FP64, the batched form's code,
 //   * the end of every successive substitution: FP32 iterations stop at a
 //     residual FP32 can resolve (SSM32_TOL2 below). A stability trial's end
 //     point is then evaluated in FP64 and polished by StableNR; where that

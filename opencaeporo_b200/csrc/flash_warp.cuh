@@ -22,8 +22,9 @@
 // chosen per lane (one division, then one logarithm): different functions
 // on different lanes of a warp would run one after another.
 // Each value is formed by the same expression as in the one-thread form
-// (shared helpers), so results and iteration counts equal the one-thread
-// form's bit for bit.
+// (shared helpers); the two agree to rounding (the compiler fuses
+// multiply-adds per kernel), so an iteration count that ends on a
+// convergence threshold can differ by a step.
 #pragma once
 
 #include "flash_cell.cuh"
