@@ -266,12 +266,7 @@ def our_arm(args):
     fl_launch = roofline.flops(nc, res["iters"], nphc)
     by_launch = roofline.batch_bytes(nc, nphc, fl.controls.use_skip)
     fp64_peak = _lib.fma_peak_tflops(dev, 64)
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except OSError:
-        pass
-    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_peak, hbm_src = hbm_peak_gbs()
     ach_tf = fl_launch / (kern_ms * 1e-3) / 1e12
     ach_gbs = by_launch / (kern_ms * 1e-3) / 1e9
     # DRAM bytes of one flash call from an ncu capture (profiles/): the plain
@@ -303,7 +298,7 @@ def our_arm(args):
                      "flops_per_launch": fl_launch, "kernel_ms": kern_ms},
         "roofline_hbm": {"bound": "hbm", "achieved": ach_gbs, "peak": hbm_peak, "unit": "GB/s",
                          "frac": ach_gbs / hbm_peak, "bytes_per_launch": by_launch,
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                         "peak_source": hbm_src},
         "plain_fp64_gpu": plain,
         "initializer": init_note,
         "iters_per_cell": {k: float(v) for k, v in zip(("ssmsta", "nrsta", "ssmsp", "nrsp", "rr"),
@@ -456,6 +451,17 @@ def regions_arm(args):
         "plain_fp64_per_region": {"value": total / (t_plain * 1e-3), "ms_per_step": t_plain}}), flush=True)
 
 
+def hbm_peak_gbs():
+    """(peak HBM GB/s, its source): the measured copy bandwidth of this
+    pool's B200s from MEASURED_PEAKS.json, else the earlier pool measurement
+    of 6650 GB/s, labelled as the fallback."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), \
+            "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "6650 GB/s (of fallback: MEASURED_PEAKS.json absent)"
+
+
 def entries_arm(args):
     """The other flash entry points on the bench workload (1,048,576 fresh
     states of the 6-component fluid): ocpf_init_flash_fim (InitFlashFIM:
@@ -578,15 +584,12 @@ def entries_arm(args):
     exact = all(np.array_equal(kout[k][:, :ns].cpu().numpy().T, want[k])
                 for k in ("kr", "Pc", "Pj", "dKr_dS", "dPcj_dS"))
     kbytes = n * (8 + 24 + 4 + 3 * 24 + 2 * 72)
-    try:
-        peak = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
-    except (OSError, KeyError, ValueError):
-        peak = None
+    peak, peak_src = hbm_peak_gbs()
     res["cal_krpc"] = {
         "value": n / (t_k * 1e-3), "unit": "cells/s", "ms_per_step": t_k,
         "roofline": {"bound": "hbm", "achieved": kbytes / (t_k * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": (kbytes / (t_k * 1e-3) / 1e9 / peak) if peak else None,
-                     "bytes_per_launch": kbytes, "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"},
+                     "bytes_per_launch": kbytes, "peak_source": peak_src},
         "reference_cpu": {"value": ns / want["seconds"], "unit": "cells/s", "cores": os.cpu_count() or 1,
                           "sample": f"first {ns} cells"},
         "bit_identical_on_sample": bool(exact)}
