@@ -29,15 +29,14 @@ using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const
 
 // Batched-form launch sequences (flash_phased_ncN.cu).
 #define OCPF_DECL_PHASED(N)                                                           \
-    cudaError_t launch_phased_nc##N(const FluidConst& F, const PhasedArgs& a, cudaStream_t st, \
-                                    const PhasedAux* aux);                                        \
+    cudaError_t launch_phased_nc##N(const FluidConst& F, const PhasedArgs& a, cudaStream_t st); \
     int         phased_state_doubles_nc##N();
 OCPF_DECL_PHASED(3)
 OCPF_DECL_PHASED(6)
 OCPF_DECL_PHASED(9)
 OCPF_DECL_PHASED(12)
 
-using PhasedLauncher = cudaError_t (*)(const FluidConst&, const PhasedArgs&, cudaStream_t, const PhasedAux*);
+using PhasedLauncher = cudaError_t (*)(const FluidConst&, const PhasedArgs&, cudaStream_t);
 
 static PhasedLauncher phased_kernel(int nc, int* ndbl)
 {
@@ -149,9 +148,6 @@ struct ocpf_ctx {
     PhasedArgs      gkey;
     bool            gvalid;
     int32_t         gkernels;      // kernel nodes of the captured graph
-    // second stream and fork/join events of the batched sequence (PhasedAux)
-    cudaStream_t    as;
-    cudaEvent_t     afork, ajoin;
     int32_t         last_kernels;  // kernels the last call launched, -1 unknown
 };
 
@@ -206,19 +202,6 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->gs        = nullptr;
     c->gexec     = nullptr;
     c->gvalid    = false;
-    c->as        = nullptr;
-    c->afork = c->ajoin = nullptr;
-    // the batched sequence's second stream; without it the sequence runs on one
-    if (cudaStreamCreateWithFlags(&c->as, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->afork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&c->ajoin, cudaEventDisableTiming) != cudaSuccess) {
-        cudaGetLastError();
-        if (c->as) cudaStreamDestroy(c->as);
-        if (c->afork) cudaEventDestroy(c->afork);
-        if (c->ajoin) cudaEventDestroy(c->ajoin);
-        c->as    = nullptr;
-        c->afork = c->ajoin = nullptr;
-    }
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         cudaSetDevice(prev);
@@ -245,9 +228,6 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     if (c->gs) cudaStreamDestroy(c->gs);
     if (c->evf) cudaEventDestroy(c->evf);
     if (c->evj) cudaEventDestroy(c->evj);
-    if (c->as) cudaStreamDestroy(c->as);
-    if (c->afork) cudaEventDestroy(c->afork);
-    if (c->ajoin) cudaEventDestroy(c->ajoin);
     for (auto& s : c->hs)
         if (s) cudaStreamDestroy(s);
     cudaSetDevice(prev);
@@ -357,25 +337,21 @@ static void scratch_view(const ocpf_ctx* c, int part, int64_t cap, StateBuf& S, 
 static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs& args, cudaStream_t st,
                                  bool graph_ok)
 {
-    // the second stream only on the device-buffer path (the host path runs
-    // two parts at once on its own streams)
-    PhasedAux        ax{c->as, c->afork, c->ajoin};
-    const PhasedAux* aux = (graph_ok && c->as && c->afork && c->ajoin) ? &ax : nullptr;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusInvalidated;
     c->last_kernels = -1;
-    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, st, aux);
+    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, st);
     if (!(c->gvalid && std::memcmp(&c->gkey, &args, sizeof(args)) == 0)) {
         c->gvalid = false;
-        if (!c->gs && cudaStreamCreateWithFlags(&c->gs, cudaStreamNonBlocking) != cudaSuccess) return k(c->fc, args, st, aux);
+        if (!c->gs && cudaStreamCreateWithFlags(&c->gs, cudaStreamNonBlocking) != cudaSuccess) return k(c->fc, args, st);
         cudaGraph_t g = nullptr;
-        if (cudaStreamBeginCapture(c->gs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return k(c->fc, args, st, aux);
-        const cudaError_t le = k(c->fc, args, c->gs, aux);
+        if (cudaStreamBeginCapture(c->gs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return k(c->fc, args, st);
+        const cudaError_t le = k(c->fc, args, c->gs);
         const cudaError_t ce = cudaStreamEndCapture(c->gs, &g);
         if (le != cudaSuccess || ce != cudaSuccess || !g) {
             if (g) cudaGraphDestroy(g);
             cudaGetLastError();
-            return k(c->fc, args, st, aux);
+            return k(c->fc, args, st);
         }
         size_t nn = 0;
         int    nk = 0;
@@ -403,7 +379,7 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
         if (!ok) {
             c->gexec = nullptr;
             cudaGetLastError();
-            return k(c->fc, args, st, aux);
+            return k(c->fc, args, st);
         }
         c->gkey   = args;
         c->gvalid = true;

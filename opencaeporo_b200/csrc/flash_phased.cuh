@@ -48,10 +48,7 @@ struct SF {  // double field ids
     };
 };
 // int fields
-// IF_SLOWQ: 1 once the cell has joined the restart path's list (written by
-// the init kernel and the split's end only, so that the finalize of the
-// other cells can run beside the restart kernel).
-enum : int { IF_META = 0, IF_STATUS, IF_IT0, IF_IT1, IF_IT2, IF_IT3, IF_IT4, IF_MAXIT, IF_GUARD, IF_SLOWQ, IF_COUNT };
+enum : int { IF_META = 0, IF_STATUS, IF_IT0, IF_IT1, IF_IT2, IF_IT3, IF_IT4, IF_MAXIT, IF_GUARD, IF_COUNT };
 
 // meta bits
 constexpr uint32_t M_NP_MASK   = 0xF;     // hydrocarbon phase count
@@ -128,14 +125,6 @@ struct Lists {
 // PhasedArgs::opts bits
 constexpr uint32_t PH_MIXED = 1u;  // FP32 successive substitution (flash_mixed.cuh)
 constexpr uint32_t PH_LEARN = 2u;  // learned initialiser for fresh cells (flash_learned.cuh)
-
-// A second stream and two events: with them the launch sequence finalizes
-// the cells off the restart path on `st2` while the restart kernel runs
-// (fork after the split rounds, join before the sequence ends).
-struct PhasedAux {
-    cudaStream_t st2;
-    cudaEvent_t  fork, join;
-};
 
 struct PhasedArgs {
     int64_t      count, stride;

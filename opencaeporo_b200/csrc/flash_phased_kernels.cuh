@@ -36,7 +36,6 @@ __device__ void init_body(const FluidConst& F, const PhasedArgs& a)
             S.D(F_::Bi + i, c) = f.Bi[i];
         }
         S.I(IF_GUARD, c) = 0;
-        S.I(IF_SLOWQ, c) = 0;
         store_single_phase(f, S, c, true);  // x0 = z until a split replaces it
         if (f.ftype == 0 || f.ftype == 1) {
             f.flagSkip = true;
@@ -703,7 +702,6 @@ __device__ __forceinline__ void sp_after_nr(CellFlash<NC>& f, const PhasedArgs& 
     if (restart) {
         store_split(f, S, c);
         store_book(f, S, c, meta);
-        if (r + 1 >= SPLIT_ROUNDS) S.I(IF_SLOWQ, c) = 1;
         a.L.push(r + 1 < SPLIT_ROUNDS ? L_SP_0 + r + 1 : L_SLOW, (int32_t)c);
         return;
     }
@@ -884,13 +882,13 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
 }
 
 // --------------------------------------------------------------- finalize
-// The tail of one cell after its equilibrium (FimCell::finalize).
 template <int NC>
-__device__ void finalize_cell(const FluidConst& F, const PhasedArgs& a, int64_t c)
+__device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
 {
     using F_ = SF<NC>;
     const StateBuf& S = a.S;
-    {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
+         c += (int64_t)gridDim.x * blockDim.x) {
         FimCell<NC> f(F);
         f.load_inputs(c, a.stride, a.in, a.sk, a.tail);
         uint32_t meta;
@@ -917,24 +915,6 @@ __device__ void finalize_cell(const FluidConst& F, const PhasedArgs& a, int64_t 
             f.n[1][i] = S.D(F_::n1 + i, c);
         }
         f.finalize(c, a.stride, a.sk, a.out, a.tail);
-    }
-}
-
-// mode 0: every cell; 1: the cells off the restart path (run beside the
-// restart kernel); 2: the restart path's cells (after it).
-template <int NC>
-__device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a, int mode)
-{
-    if (mode == 2) {
-        const uint32_t n = a.L.len(L_SLOW);
-        for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-            finalize_cell<NC>(F, a, a.L.item(L_SLOW, k));
-        return;
-    }
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
-         c += (int64_t)gridDim.x * blockDim.x) {
-        if (mode == 1 && a.S.I(IF_SLOWQ, c) != 0) continue;
-        finalize_cell<NC>(F, a, c);
     }
 }
 

@@ -34,7 +34,7 @@ __global__ void __launch_bounds__(128) kp_learn_12(const __grid_constant__ Fluid
     extern __shared__ __align__(16) unsigned char smem_raw[];
     learn_body<12>(F, a, *reinterpret_cast<LearnSmem*>(smem_raw));
 }
-K128 kp_finalize_12(const __grid_constant__ FluidConst F, const PhasedArgs a, int mode) { phased_finalize_body<12>(F, a, mode); }
+K128 kp_finalize_12(const __grid_constant__ FluidConst F, const PhasedArgs a) { phased_finalize_body<12>(F, a); }
 #undef K128
 
 static int persistent_grid(const void* k, int sms)
@@ -54,7 +54,7 @@ static void split_round_12(const FluidConst& F, const PhasedArgs& a, cudaStream_
     kp_sp_nr_12<<<gnr, 128, 0, st>>>(F, a, r);
 }
 
-cudaError_t launch_phased_nc12(const FluidConst& F, const PhasedArgs& a, cudaStream_t st, const PhasedAux* aux)
+cudaError_t launch_phased_nc12(const FluidConst& F, const PhasedArgs& a, cudaStream_t st)
 {
     static int g_s01 = 0, g_sta = 0, g_sp = 0, g_sta32 = 0, g_spnr = 0, g_stnr = 0, sms = 0;
     if (!sms) {
@@ -105,20 +105,8 @@ cudaError_t launch_phased_nc12(const FluidConst& F, const PhasedArgs& a, cudaStr
     }
     for (int r = 0; r < SPLIT_ROUNDS; r++)
         split_round_12(F, a, st, r, gp, g_sp, g_spnr);
-    if (aux) {
-        // the restart kernel holds a few warps for most of the call: the other
-        // cells' tails run beside it on the second stream
-        cudaEventRecord(aux->fork, st);
-        kp_slow_12<<<gp, 128, 0, st>>>(F, a);
-        cudaStreamWaitEvent(aux->st2, aux->fork, 0);
-        kp_finalize_12<<<gcell, 128, 0, aux->st2>>>(F, a, 1);
-        cudaEventRecord(aux->join, aux->st2);
-        kp_finalize_12<<<gp, 128, 0, st>>>(F, a, 2);
-        cudaStreamWaitEvent(st, aux->join, 0);
-    } else {
-        kp_slow_12<<<gp, 128, 0, st>>>(F, a);
-        kp_finalize_12<<<gcell, 128, 0, st>>>(F, a, 0);
-    }
+    kp_slow_12<<<gp, 128, 0, st>>>(F, a);
+    kp_finalize_12<<<gcell, 128, 0, st>>>(F, a);
     return cudaGetLastError();
 }
 
