@@ -122,6 +122,11 @@ bool make_fluid_const(const ocpf_fluid& in, FluidConst& f)
 
 using namespace ocpf;
 
+// Parts of the host-buffer path in flight at once, each with its own
+// stream, staging buffers and scratch: a chunk that holds a long restart
+// chain then delays only the chunks of its own part.
+constexpr int HOST_PARTS = 4;
+
 struct ocpf_ctx {
     int         device;
     FluidConst  fc;
@@ -130,9 +135,9 @@ struct ocpf_ctx {
     // host-path staging (device) buffers, grown on demand
     int64_t     stage_cap;
     void*       stage;
-    cudaStream_t hs[2];
+    cudaStream_t hs[HOST_PARTS];
     // batched-form scratch: per-cell phase state, cell lists and list
-    // counters, in parts of part_cap cells (the host path uses two parts)
+    // counters, in parts of part_cap cells (the host path uses HOST_PARTS parts)
     int64_t     eq_cap;    // total cells the scratch holds
     void*       eq;
     // learned initialiser parameters (device, MLP_NPARAM floats) or null
@@ -190,7 +195,7 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->timed     = false;
     c->stage_cap = 0;
     c->stage     = nullptr;
-    c->hs[0] = c->hs[1] = nullptr;
+    for (auto& s : c->hs) s = nullptr;
     c->eq_cap    = 0;
     c->eq        = nullptr;
     c->mlp       = nullptr;
@@ -424,7 +429,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
             if (rc != OCPF_OK) return rc;
             scratch_view(c, 0, c->eq_cap, args.S, args.L);
         } else {
-            // host path: scratch already sized for two parts of `stride` cells
+            // host path: scratch already sized for HOST_PARTS parts of `stride` cells
             scratch_view(c, part, stride, args.S, args.L);
         }
         if (timed) cudaEventRecord(c->ev0, st);
@@ -713,7 +718,7 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
         if (c->stage) cudaFree(c->stage);
         c->stage     = nullptr;
         c->stage_cap = 0;
-        if (cudaMalloc(&c->stage, 2 * stage_stride(per, chunk)) != cudaSuccess) {
+        if (cudaMalloc(&c->stage, HOST_PARTS * stage_stride(per, chunk)) != cudaSuccess) {
             if (prev != c->device) cudaSetDevice(prev);
             return OCPF_ENOMEM;
         }
@@ -723,17 +728,17 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
         if (!s) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
     const int64_t cap = c->stage_cap;
     if (form != OCPF_FORM_PLAIN) {
-        const int r2 = ensure_scratch(c, cap, 2);
+        const int r2 = ensure_scratch(c, cap, HOST_PARTS);
         if (r2 != OCPF_OK) {
             if (prev != c->device) cudaSetDevice(prev);
             return r2;
         }
     }
-    Views         V[2];
-    for (int b = 0; b < 2; b++) V[b] = carve((char*)c->stage + b * stage_stride(per, cap), cap, L, sk, out);
+    Views V[HOST_PARTS];
+    for (int b = 0; b < HOST_PARTS; b++) V[b] = carve((char*)c->stage + b * stage_stride(per, cap), cap, L, sk, out);
     const bool use_sk = c->fc.use_skip != 0;
     int        bidx   = 0;
-    for (int64_t c0 = 0; c0 < ncell && rc == OCPF_OK; c0 += cap, bidx ^= 1) {
+    for (int64_t c0 = 0; c0 < ncell && rc == OCPF_OK; c0 += cap, bidx = (bidx + 1) % HOST_PARTS) {
         const int64_t cnt = std::min<int64_t>(cap, ncell - c0);
         cudaStream_t  st  = c->hs[bidx];
         const Views&  v   = V[bidx];
