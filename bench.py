@@ -620,6 +620,52 @@ def entries_arm(args):
         "reference_cpu": {"value": ns / want["seconds"], "unit": "cells/s", "cores": os.cpu_count() or 1,
                           "sample": f"first {ns} cells"},
         "bit_identical_on_sample": bool(exact)}
+    # the Jacobian's bulk part after a FIM flash and KrPc, on the bench grid
+    # (128 x 128 x 64 bulks, 7-point connections): upwind and assembly
+    from opencaeporo_b200.fim_jacobian import ConnGraph
+    nx, ny, nz = 128, 128, 64
+    if n == nx * ny * nz:
+        st.P.copy_(Pt)
+        st.T.copy_(Tt)
+        st.Ni.copy_(Nt)
+        st.skip["flag"].zero_()
+        m.flash_fim(st, form=args.form, fresh=True)
+        fu.cal_krpc(st.P, st.out["S"], satnum, out=kout)
+        grid = np.arange(n, dtype=np.int64).reshape(nz, ny, nx)
+        cb, ce = [], []
+        for axis in (2, 1, 0):
+            cb.append(np.take(grid, range(grid.shape[axis] - 1), axis=axis).ravel())
+            ce.append(np.take(grid, range(1, grid.shape[axis]), axis=axis).ravel())
+        cb, ce = np.concatenate(cb), np.concatenate(ce)
+        rng2 = np.random.default_rng(SEED + 3)
+        g = ConnGraph(n, cb, ce, rng2.uniform(100.0, 400.0, len(cb)))
+        bulk = {k: st.out[k] for k in ("phaseExist", "pSderExist", "pVnumCom", "S", "rho", "xi", "mu", "muP", "xiP",
+                                       "rhoP", "xij", "rhox", "xix", "mux", "dSec_dPri", "vfP", "vfi")}
+        bulk.update({"kr": kout["kr"], "Pj": kout["Pj"], "dKr_dS": kout["dKr_dS"], "dPcj_dS": kout["dPcj_dS"],
+                     "v": torch.as_tensor(rng2.uniform(5e3, 5e4, n)).cuda(),
+                     "poroP": torch.as_tensor(rng2.uniform(1e-6, 1e-5, n)).cuda(),
+                     "depth": torch.as_tensor(np.repeat(np.arange(nz) * 10.0 + 8000.0, nx * ny)).cuda()})
+        up, urho = g.upwind(bulk)
+        jout = g.jacobian(nc, 1.0, bulk, up, urho)
+        t_up = timed(lambda: None, lambda: g.upwind(bulk))
+        t_jac = timed(lambda: None, lambda: g.jacobian(nc, 1.0, bulk, up, urho, out=jout))
+        torch.cuda.synchronize()
+        finite = bool(torch.isfinite(jout["diag"]).all().item() and torch.isfinite(jout["offEB"]).all().item())
+        ncol = nc + 2
+        nconn = len(cb)
+        # algorithmic bytes: each bulk's inputs once, each connection's ends,
+        # area and upstream data, the two off-diagonal blocks and the diagonal
+        rows = st.out["bRowSizedSdP"].double().sum().item()
+        per_bulk_in = 4 * 9 + 8 * (7 * 3 + 4 * 3 * (nc + 1) + (nc + 1) + 1 + 3 * 2 + 9 * 2 + 3)
+        jbytes = n * per_bulk_in + 8 * ncol * rows + nconn * (8 * 3 + 3 * 12) + 8 * ncol * ncol * (2 * nconn + n)
+        res["fim_jacobian"] = {
+            "value": nconn / (t_jac * 1e-3), "unit": "connections/s", "ms_per_step": t_jac,
+            "connections": nconn, "bulks": n, "upwind_ms": t_up, "finite": finite,
+            "roofline": {"bound": "hbm", "achieved": jbytes / (t_jac * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": (jbytes / (t_jac * 1e-3) / 1e9 / peak) if peak else None,
+                         "bytes_per_launch": jbytes, "peak_source": peak_src},
+            "parity": "bit-identical to the restatement on the 8x8x8 test grid (tests/test_fim_jacobian.py)"}
+        g.close()
     fu.close()
     m.close()
     print(json.dumps({

@@ -423,6 +423,82 @@ int ocpf_krpc_destroy(ocpf_krpc* k);
  * reference's bit for bit. Asynchronous on `stream`. */
 int ocpf_cal_krpc(ocpf_krpc* k, int64_t ncell, const ocpf_krpc_in* in, const ocpf_krpc_out* out, void* stream);
 
+/* ---------------------------------------------------------------------
+ * The consumer of the flash's derivatives: the bulk part of the FIM
+ * Jacobian (IsoT_FIM::AssembleMatBulksNew, src/OCPFluidMethod.cpp:
+ * 1569-1840) and the upstream choice that precedes it (src/BulkConn.cpp:
+ * 170-215).
+ * --------------------------------------------------------------------- */
+
+typedef struct ocpf_conn ocpf_conn;
+
+/* The Bulk arrays the assembly reads, on the device, in the flash's
+ * layouts ([field][nbulk]): the flash outputs, CalKrPc's (kr, Pj [3];
+ * dKr_dS, dPcj_dS [9]), and the rock: bulk volume v, dporosity/dP poroP and
+ * depth [nbulk]. S and rho are read by ocpf_fim_upwind only. */
+typedef struct {
+    const uint32_t* phaseExist; /* [3] */
+    const uint32_t* pSderExist; /* [3] */
+    const uint32_t* pVnumCom;   /* [3] */
+    const double*   S;          /* [3] */
+    const double*   rho;        /* [3] */
+    const double*   xi;         /* [3] */
+    const double*   mu;         /* [3] */
+    const double*   muP;        /* [3] */
+    const double*   xiP;        /* [3] */
+    const double*   rhoP;       /* [3] */
+    const double*   xij;        /* [3*numCom] */
+    const double*   rhox;       /* [3*numCom] */
+    const double*   xix;        /* [3*numCom] */
+    const double*   mux;        /* [3*numCom] */
+    const double*   dSec_dPri;  /* [3*(numCom+1)^2], bRowSizedSdP rows used */
+    const double*   vfP;        /* [1] */
+    const double*   vfi;        /* [numCom] */
+    const double*   kr;         /* [3] */
+    const double*   Pj;         /* [3] */
+    const double*   dKr_dS;     /* [9] */
+    const double*   dPcj_dS;    /* [9] */
+    const double*   v;          /* [1] */
+    const double*   poroP;      /* [1] */
+    const double*   depth;      /* [1] */
+} ocpf_jac_bulk;
+
+/* Device outputs, blocks of (numCom+1) x (numCom+1) entries, entry
+ * r*(numCom+1)+c as the field index: diag [(numCom+1)^2][nbulk] (the
+ * accumulation block plus, in connection order, each incident connection's
+ * contribution, as the reference's AddDiag calls sum them); offEB and offBE
+ * [(numCom+1)^2][nconn]: the blocks at (row eId, column bId) and (row bId,
+ * column eId) of each connection (LinearSystem::NewOffDiag's). */
+typedef struct {
+    double* diag;
+    double* offEB;
+    double* offBE;
+} ocpf_jac_out;
+
+/* The connections of a grid (BulkConn: begin and end bulk and area of each,
+ * host arrays), copied to `device` with the per-bulk list of incident
+ * connections the diagonal blocks are gathered through. OCPF_EINVAL for a
+ * bulk index outside [0, nbulk) or a connection from a bulk to itself. */
+int ocpf_conn_create(int64_t nbulk, int64_t nconn, const int64_t* bId, const int64_t* eId, const double* area,
+                     int device, ocpf_conn** out);
+int ocpf_conn_destroy(ocpf_conn* conn);
+
+/* Upstream bulk (upblock [3][nconn]) and mean density (upblock_rho
+ * [3][nconn]) of every connection and phase from S, rho, Pj, phaseExist and
+ * depth (BulkConn's upwind choice, src/BulkConn.cpp:170-215). Results equal
+ * the reference's bit for bit. Asynchronous on `stream`. */
+int ocpf_fim_upwind(ocpf_conn* conn, const ocpf_jac_bulk* bulk, int32_t* upblock, double* upblock_rho, void* stream);
+
+/* The bulk part of the FIM Jacobian for time step dt (nc hydrocarbon
+ * components: 3, 6, 9 or 12): per connection the flux derivatives of both
+ * ends, dt (dF/dXp + dF/dXs dSec_dPri), and per bulk the accumulation plus
+ * the diagonal contributions. Each operation is rounded as written in the
+ * reference, in its order; the dense product sums in order (the reference's
+ * BLAS dgemm may round its sums differently). Connections with shapes no
+ * flash writes get NaN blocks. Asynchronous on `stream`. */
+int ocpf_fim_jacobian(ocpf_conn* conn, int nc, double dt, const ocpf_jac_bulk* bulk, const int32_t* upblock,
+                      const double* upblock_rho, ocpf_jac_out* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

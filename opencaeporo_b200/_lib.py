@@ -36,7 +36,8 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_mlp_param_count", "ocpf_mlp_forward", "ocpf_mlp_grad", "ocpf_mlp_adam",
            "ocpf_set_initializer", "ocpf_flash_fim_regions", "ocpf_measure_fp64_latency",
            "ocpf_flash_impec", "ocpf_init_flash_fim", "ocpf_init_flash_impec",
-           "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count")
+           "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count",
+           "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian")
 
 _vp = C.c_void_p
 
@@ -103,6 +104,20 @@ class KrpcIn(C.Structure):
 
 class KrpcOut(C.Structure):
     _fields_ = [(f, _vp) for f in KRPC_OUT_FIELDS]
+
+
+JAC_BULK_FIELDS = ("phaseExist", "pSderExist", "pVnumCom", "S", "rho", "xi", "mu", "muP", "xiP", "rhoP", "xij",
+                   "rhox", "xix", "mux", "dSec_dPri", "vfP", "vfi", "kr", "Pj", "dKr_dS", "dPcj_dS", "v", "poroP",
+                   "depth")
+JAC_OUT_FIELDS = ("diag", "offEB", "offBE")
+
+
+class JacBulk(C.Structure):
+    _fields_ = [(f, _vp) for f in JAC_BULK_FIELDS]
+
+
+class JacOut(C.Structure):
+    _fields_ = [(f, _vp) for f in JAC_OUT_FIELDS]
 
 
 class InitIn(C.Structure):
@@ -193,6 +208,14 @@ def lib():
     L.ocpf_init_flash_impec.argtypes = [_vp, C.c_int64, C.POINTER(InitIn), C.POINTER(Skip), _vp,
                                         C.POINTER(ImpecOut), C.c_int, _vp]
     L.ocpf_init_flash_impec.restype = C.c_int
+    L.ocpf_conn_create.argtypes = [C.c_int64, C.c_int64, _vp, _vp, _vp, C.c_int, C.POINTER(_vp)]
+    L.ocpf_conn_create.restype = C.c_int
+    L.ocpf_conn_destroy.argtypes = [_vp]
+    L.ocpf_conn_destroy.restype = C.c_int
+    L.ocpf_fim_upwind.argtypes = [_vp, C.POINTER(JacBulk), _vp, _vp, _vp]
+    L.ocpf_fim_upwind.restype = C.c_int
+    L.ocpf_fim_jacobian.argtypes = [_vp, C.c_int, C.c_double, C.POINTER(JacBulk), _vp, _vp, C.POINTER(JacOut), _vp]
+    L.ocpf_fim_jacobian.restype = C.c_int
     L.ocpf_last_launch_count.argtypes = [_vp, C.POINTER(C.c_int)]
     L.ocpf_last_launch_count.restype = C.c_int
     L.ocpf_krpc_create.argtypes = [C.POINTER(Satfunc), C.c_int, C.c_int, C.POINTER(_vp)]

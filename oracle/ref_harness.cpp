@@ -26,6 +26,7 @@
 
 #define private public
 #define protected public
+#include "DenseMat.hpp"
 #include "FlowUnit.hpp"
 #include "MixtureComp.hpp"
 #include "OptionalFeatures.hpp"
@@ -389,6 +390,13 @@ extern "C" int orc_krpc(int nreg, const orc_satfunc* reg, const orc_krpc_batch* 
     return run_threads(b->n, nthreads, seconds, [nreg, reg, b](int64_t lo, int64_t hi, double* s) {
         run_chunk_krpc(nreg, reg, b, lo, hi, s);
     });
+}
+
+// The reference's own dense product of the FIM assembly (DaABpbC,
+// src/DenseMat.cpp:75-94): C = A B + C, row-major, A m x k, B k x n.
+extern "C" void orc_daabpbc(int m, int n, int k, const double* A, const double* B, double* C)
+{
+    DaABpbC(m, n, k, 1.0, A, B, 1.0, C);
 }
 
 extern "C" const char* orc_kind(void) { return "reference"; }
