@@ -5,16 +5,18 @@
 //
 //   * k_upwind, one thread per (phase, connection): upstream bulk and mean
 //     density;
-//   * k_conn_rows, one thread per (component row, connection): row i + 1 of
-//     dF/dXp and dF/dXs of both ends in registers, then that row of
+//   * k_conn_block, a group of connections per block: thread (row,
+//     connection) builds that row of dF/dXp and dF/dXs of both ends in
+//     shared memory, then thread (column, connection) forms that column of
 //     dt (dF/dXp + dF/dXs dSec_dPri) (DaABpbC, src/DenseMat.cpp:75-94) for
-//     both ends, stored as the connection's off-diagonal blocks;
+//     both ends, so that each dSec_dPri entry is read once per connection
+//     end; stored as the connection's off-diagonal blocks;
 //   * k_diag_rows, one thread per (row, bulk): the accumulation block plus
 //     every incident connection's diagonal contribution, gathered through a
 //     per-bulk list in connection order, which is the order the reference's
 //     AddDiag calls sum them in.
 // Every operation is an explicitly rounded intrinsic in the reference's
-// left-to-right expression order; the dense product sums over k in order
+// left-to-right expression order (x / 2 as x * 0.5, the same value); the dense product sums over k in order
 // and adds the dF/dXp entry last, as dgemm with beta = 1 does.
 #include <algorithm>
 #include <cstring>
@@ -32,9 +34,6 @@ constexpr double J_CONV1 = 5.61458;      // include/OCPConst.hpp
 constexpr double J_CONV2 = 1.12712E-3;   // Darcy constant, field units
 constexpr double J_GRAV  = 0.00694444;   // GRAVITY_FACTOR
 constexpr int    J_NP    = 3;
-constexpr int    J_MAXCOM = OCPF_MAX_NC + 1;
-constexpr int    J_MAXCOL = J_MAXCOM + 1;
-constexpr int    J_MAXS   = 3 + 2 * OCPF_MAX_NC;  // dSec_dPri rows of a two-phase bulk
 
 __device__ __forceinline__ double M(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double A(double a, double b) { return __dadd_rn(a, b); }
@@ -100,162 +99,212 @@ __device__ __forceinline__ SecShape sec_shape(const ocpf_jac_bulk& B, int64_t nb
     return s;
 }
 
-// Row r = i + 1 of dt (dF/dXp + dF/dXs dSec_dPri) of one end: the sum over
-// k in order, then the dF/dXp entry (column 0 only), then the scale.
-__device__ __forceinline__ void product_row(const ocpf_jac_bulk& B, int64_t nb, int64_t n, int ncol, int nsec,
-                                            const double* srow, double prow, double dt, double* out, int64_t nout,
-                                            int64_t c, int r, bool negate)
-{
-    for (int col = 0; col < ncol; col++) {
-        double s = 0;
-        for (int k = 0; k < nsec; k++) s = A(s, M(srow[k], B.dSec_dPri[(int64_t)(k * ncol + col) * nb + n]));
-        const double v = M(A(s, col == 0 ? prow : 0.0), dt);
-        out[(int64_t)(r * ncol + col) * nout + c] = negate ? -v : v;
-    }
-}
-
+// Connections per block of k_conn_block and its shared-memory size: the
+// dF/dXs rows of both ends of every connection of the block.
 template <int NCOM>
-__global__ void __launch_bounds__(128) k_conn_rows(const ConnDev C, const ocpf_jac_bulk B, const int32_t* up,
-                                                   const double* uprho, double dt, ocpf_jac_out O)
+struct ConnBlock {
+    static constexpr int NCOL = NCOM + 1;
+    static constexpr int NSEC = 3 + 2 * (NCOM - 1);  // dSec_dPri rows of a two-phase bulk
+    static constexpr int CPB  = NCOM <= 7 ? 32 : (NCOM <= 10 ? 16 : 8);
+    static constexpr int TPC  = NCOL <= 8 ? 8 : 16;  // threads per connection (>= NCOL)
+    static constexpr int THREADS = CPB * TPC;
+    static constexpr size_t SMEM = sizeof(double) * (size_t)CPB * 2 * (NSEC * NCOM + NCOM) + sizeof(int) * CPB * 3;
+    static_assert(NCOL <= TPC, "one thread per column");
+};
+
+// Phase 1, thread (i, connection): row i + 1 of dF/dXp (column 0 only) and
+// of dF/dXs of both ends, accumulated in shared memory in the reference's
+// order. Phase 2, thread (column, connection): that column of
+// dt (dF/dXp + dF/dXs dSec_dPri) (DaABpbC + Dscalar) for both ends, the sum
+// over k in order and the dF/dXp entry last, as dgemm with beta = 1 forms
+// it; stored as (row eId, col bId) = -bmatB and (row bId, col eId) = bmatE.
+template <int NCOM>
+__global__ void __launch_bounds__(ConnBlock<NCOM>::THREADS) k_conn_block(const ConnDev C, const ocpf_jac_bulk B,
+                                                                           const int32_t* up, const double* uprho,
+                                                                           double dt, ocpf_jac_out O)
 {
-    constexpr int NCOL = NCOM + 1;
+    using CB = ConnBlock<NCOM>;
+    constexpr int NCOL = CB::NCOL, NSEC = CB::NSEC, CPB = CB::CPB;
+    extern __shared__ double sm[];
+    // rows[end][k][i][cl], prow[end][i][cl], then nsec[end][cl], ok[cl]
+    double* rows = sm;
+    double* prow = sm + (size_t)2 * NSEC * NCOM * CPB;
+    int*    meta = (int*)(prow + (size_t)2 * NCOM * CPB);
+    auto R  = [&](int end, int k, int i, int cl) -> double& { return rows[((end * NSEC + k) * NCOM + i) * CPB + cl]; };
+    auto PR = [&](int end, int i, int cl) -> double& { return prow[(end * NCOM + i) * CPB + cl]; };
     const int64_t nc = C.nconn, nb = C.nb;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < NCOM * nc;
-         t += (int64_t)gridDim.x * blockDim.x) {
-        const int     i = (int)(t / nc);
-        const int64_t c = t - i * nc;
-        const int64_t bId = C.bId[c], eId = C.eId[c];
-        const double  Akd    = M(J_CONV1 * J_CONV2, C.area[c]);
-        const double  dGamma = M(J_GRAV, S(B.depth[bId], B.depth[eId]));
-        const SecShape sB = sec_shape(B, nb, bId), sE = sec_shape(B, nb, eId);
-        bool exB[J_NP], exE[J_NP];
+    const int     lane_c = threadIdx.x % CPB, part = threadIdx.x / CPB;
+    for (int64_t g0 = (int64_t)blockIdx.x * CPB; g0 < nc; g0 += (int64_t)gridDim.x * CPB) {
+        const int64_t c     = g0 + lane_c;
+        const bool    live  = c < nc;
+        const int     i     = part;  // phase 1: row i + 1
+        __syncthreads();             // the previous group's phase 2 is done with the shared rows
+        if (i < NCOM) {
+            for (int k = 0; k < NSEC; k++) R(0, k, i, lane_c) = R(1, k, i, lane_c) = 0;
+            PR(0, i, lane_c) = PR(1, i, lane_c) = 0;
+        }
+        if (live && i < NCOM) {
+            const int64_t  bId = C.bId[c], eId = C.eId[c];
+            const double   Akd    = M(J_CONV1 * J_CONV2, C.area[c]);
+            const double   dGamma = M(J_GRAV, S(B.depth[bId], B.depth[eId]));
+            const SecShape sB = sec_shape(B, nb, bId), sE = sec_shape(B, nb, eId);
+            bool exB[J_NP], exE[J_NP];
 #pragma unroll
-        for (int j = 0; j < J_NP; j++) {
-            exB[j] = B.phaseExist[j * nb + bId] != 0;
-            exE[j] = B.phaseExist[j * nb + eId] != 0;
-        }
-        // shapes a flash writes: at most NCOM - 1 compositions per phase and
-        // 3 + 2 (NCOM - 1) dSec_dPri rows; anything else (and an upstream
-        // bulk that is neither end) gives NaN blocks instead of an access
-        // outside the arrays
-        bool ok = sB.ncol <= 3 + 2 * (NCOM - 1) && sE.ncol <= 3 + 2 * (NCOM - 1);
+            for (int j = 0; j < J_NP; j++) {
+                exB[j] = B.phaseExist[j * nb + bId] != 0;
+                exE[j] = B.phaseExist[j * nb + eId] != 0;
+            }
+            // shapes a flash writes: at most NCOM - 1 compositions per phase
+            // and NSEC dSec_dPri rows; anything else (and an upstream bulk
+            // that is neither end) gives NaN blocks instead of an access
+            // outside the arrays
+            bool ok = sB.ncol <= NSEC && sE.ncol <= NSEC;
 #pragma unroll
-        for (int j = 0; j < J_NP; j++) {
-            ok = ok && sB.vn[j] >= 0 && sB.vn[j] < NCOM && sE.vn[j] >= 0 && sE.vn[j] < NCOM;
-            const int64_t u = up[j * nc + c];
-            ok = ok && (u == bId || u == eId);
+            for (int j = 0; j < J_NP; j++) {
+                ok = ok && sB.vn[j] >= 0 && sB.vn[j] < NCOM && sE.vn[j] >= 0 && sE.vn[j] < NCOM;
+                const int64_t u = up[j * nc + c];
+                ok = ok && (u == bId || u == eId);
+            }
+            if (i == 0) {
+                meta[lane_c]           = ok ? sB.ncol : 0;
+                meta[CPB + lane_c]     = ok ? sE.ncol : 0;
+                meta[2 * CPB + lane_c] = ok ? 1 : 0;
+            }
+            if (ok) {
+                double pB = 0, pE = 0;
+                int    jxB = (sB.sd[0] ? 1 : 0) + (sB.sd[1] ? 1 : 0) + (sB.sd[2] ? 1 : 0);
+                int    jxE = (sE.sd[0] ? 1 : 0) + (sE.sd[1] ? 1 : 0) + (sE.sd[2] ? 1 : 0);
+                for (int j = 0; j < J_NP; j++) {
+                    const int64_t uId = up[j * nc + c];
+                    const bool    exU = uId == bId ? exB[j] : exE[j];
+                    if (!exU) {
+                        jxB += sB.vn[j];
+                        jxE += sE.vn[j];
+                        continue;
+                    }
+                    const int64_t uj = j * nb + uId, bj = j * nb + bId, ej = j * nb + eId;
+                    const double  dP = S(S(B.Pj[bj], B.Pj[ej]), M(uprho[j * nc + c], dGamma));
+                    const double  xi = B.xi[uj], kr = B.kr[uj], mu = B.mu[uj];
+                    const double  muP = B.muP[uj], xiP = B.xiP[uj], rhoP = B.rhoP[uj];
+                    const double  transJ  = D(M(Akd, kr), mu);
+                    const double  xij     = B.xij[(int64_t)(j * NCOM + i) * nb + uId];
+                    const double  transIJ = M(M(xij, xi), transJ);
+                    pB = A(pB, transIJ);
+                    pE = S(pE, transIJ);
+                    double tmp = M(M(M(xij, transJ), xiP), dP);
+                    tmp        = A(tmp, M(D(M(-transIJ, muP), mu), dP));
+                    if (!exE[j]) {
+                        tmp = A(tmp, M(transIJ, M(-rhoP, dGamma)));
+                        pB  = A(pB, tmp);
+                    } else if (!exB[j]) {
+                        tmp = A(tmp, M(transIJ, M(-rhoP, dGamma)));
+                        pE  = A(pE, tmp);
+                    } else {
+                        pB = A(pB, M(M(transIJ, M(-B.rhoP[bj], dGamma)), 0.5));
+                        pE = A(pE, M(M(transIJ, M(-B.rhoP[ej], dGamma)), 0.5));
+                        if (bId == uId)
+                            pB = A(pB, tmp);
+                        else
+                            pE = A(pE, tmp);
+                    }
+                    int           j1SB = 0, j1SE = 0;
+                    const double* pcJ  = B.dPcj_dS + (int64_t)(3 * j) * nb;
+                    const double* krJ  = B.dKr_dS + (int64_t)(3 * j) * nb;
+                    const double  fk   = D(M(M(Akd, xij), xi), mu);  // Akd xij xi / mu
+                    if (bId == uId) {
+                        for (int j1 = 0; j1 < J_NP; j1++) {
+                            if (sB.sd[j1]) {
+                                double& r = R(0, j1SB, i, lane_c);
+                                r         = A(r, M(transIJ, pcJ[(int64_t)j1 * nb + bId]));
+                                r         = A(r, M(M(fk, krJ[(int64_t)j1 * nb + uId]), dP));
+                                j1SB++;
+                            }
+                            if (sE.sd[j1]) {
+                                double& r = R(1, j1SE, i, lane_c);
+                                r         = S(r, M(transIJ, pcJ[(int64_t)j1 * nb + eId]));
+                                j1SE++;
+                            }
+                        }
+                        const int nv = sB.vn[j];
+                        for (int k = 0; k < nv; k++) {
+                            const int64_t ok2 = (int64_t)(j * NCOM + k) * nb;
+                            const double  rx  = exE[j] ? M(B.rhox[ok2 + bId], 0.5) : B.rhox[ok2 + uId];
+                            double        v   = M(M(-transIJ, rx), dGamma);
+                            v                 = A(v, M(M(M(xij, transJ), B.xix[ok2 + uId]), dP));
+                            v                 = A(v, M(D(M(-transIJ, B.mux[ok2 + uId]), mu), dP));
+                            double& r         = R(0, jxB + k, i, lane_c);
+                            r                 = A(r, v);
+                            if (exE[j]) {
+                                double& re = R(1, jxE + k, i, lane_c);
+                                re         = A(re, M(M(M(-transIJ, B.rhox[ok2 + eId]), 0.5), dGamma));
+                            }
+                        }
+                        if (i < nv) {
+                            double& r = R(0, jxB + i, i, lane_c);
+                            r         = A(r, M(M(xi, transJ), dP));
+                        }
+                    } else {
+                        for (int j1 = 0; j1 < J_NP; j1++) {
+                            if (sB.sd[j1]) {
+                                double& r = R(0, j1SB, i, lane_c);
+                                r         = A(r, M(transIJ, pcJ[(int64_t)j1 * nb + bId]));
+                                j1SB++;
+                            }
+                            if (sE.sd[j1]) {
+                                double& r = R(1, j1SE, i, lane_c);
+                                r         = S(r, M(transIJ, pcJ[(int64_t)j1 * nb + eId]));
+                                r         = A(r, M(M(fk, krJ[(int64_t)j1 * nb + uId]), dP));
+                                j1SE++;
+                            }
+                        }
+                        const int nv = sE.vn[j];
+                        for (int k = 0; k < nv; k++) {
+                            const int64_t ok2 = (int64_t)(j * NCOM + k) * nb;
+                            const double  rx  = exB[j] ? M(B.rhox[ok2 + eId], 0.5) : B.rhox[ok2 + uId];
+                            double        v   = M(M(-transIJ, rx), dGamma);
+                            v                 = A(v, M(M(M(xij, transJ), B.xix[ok2 + uId]), dP));
+                            v                 = A(v, M(D(M(-transIJ, B.mux[ok2 + uId]), mu), dP));
+                            double& r         = R(1, jxE + k, i, lane_c);
+                            r                 = A(r, v);
+                            if (exB[j]) {
+                                double& rb = R(0, jxB + k, i, lane_c);
+                                rb         = A(rb, M(M(M(-transIJ, B.rhox[ok2 + bId]), 0.5), dGamma));
+                            }
+                        }
+                        if (i < nv) {
+                            double& r = R(1, jxE + i, i, lane_c);
+                            r         = A(r, M(M(xi, transJ), dP));
+                        }
+                    }
+                    jxB += sB.vn[j];
+                    jxE += sE.vn[j];
+                }
+                PR(0, i, lane_c) = pB;
+                PR(1, i, lane_c) = pE;
+            }
         }
-        if (!ok) {
-            const double nan = __longlong_as_double(0x7ff8000000000000LL);
-            for (int col = 0; col < NCOL; col++) {
-                O.offEB[(int64_t)((i + 1) * NCOL + col) * nc + c] = nan;
-                O.offBE[(int64_t)((i + 1) * NCOL + col) * nc + c] = nan;
-                if (i == 0) O.offEB[(int64_t)col * nc + c] = O.offBE[(int64_t)col * nc + c] = nan;
-            }
-            continue;
-        }
-        double pB = 0, pE = 0, rB[J_MAXS], rE[J_MAXS];
-#pragma unroll
-        for (int k = 0; k < J_MAXS; k++) rB[k] = rE[k] = 0;
-        int jxB = (sB.sd[0] ? 1 : 0) + (sB.sd[1] ? 1 : 0) + (sB.sd[2] ? 1 : 0);
-        int jxE = (sE.sd[0] ? 1 : 0) + (sE.sd[1] ? 1 : 0) + (sE.sd[2] ? 1 : 0);
-        for (int j = 0; j < J_NP; j++) {
-            const int64_t uId = up[j * nc + c];
-            const bool    exU = uId == bId ? exB[j] : exE[j];
-            if (!exU) {
-                jxB += sB.vn[j];
-                jxE += sE.vn[j];
-                continue;
-            }
-            const int64_t uj = j * nb + uId, bj = j * nb + bId, ej = j * nb + eId;
-            const double  dP = S(S(B.Pj[bj], B.Pj[ej]), M(uprho[j * nc + c], dGamma));
-            const double  xi = B.xi[uj], kr = B.kr[uj], mu = B.mu[uj];
-            const double  muP = B.muP[uj], xiP = B.xiP[uj], rhoP = B.rhoP[uj];
-            const double  transJ  = D(M(Akd, kr), mu);
-            const double  xij     = B.xij[(int64_t)(j * NCOM + i) * nb + uId];
-            const double  transIJ = M(M(xij, xi), transJ);
-            pB = A(pB, transIJ);
-            pE = S(pE, transIJ);
-            double tmp = M(M(M(xij, transJ), xiP), dP);
-            tmp        = A(tmp, M(D(M(-transIJ, muP), mu), dP));
-            if (!exE[j]) {
-                tmp = A(tmp, M(transIJ, M(-rhoP, dGamma)));
-                pB  = A(pB, tmp);
-            } else if (!exB[j]) {
-                tmp = A(tmp, M(transIJ, M(-rhoP, dGamma)));
-                pE  = A(pE, tmp);
-            } else {
-                pB = A(pB, D(M(transIJ, M(-B.rhoP[bj], dGamma)), 2.0));
-                pE = A(pE, D(M(transIJ, M(-B.rhoP[ej], dGamma)), 2.0));
-                if (bId == uId)
-                    pB = A(pB, tmp);
-                else
-                    pE = A(pE, tmp);
-            }
-            int           j1SB = 0, j1SE = 0;
-            const double* pcB  = B.dPcj_dS + (int64_t)(3 * j) * nb;
-            const double* krU  = B.dKr_dS + (int64_t)(3 * j) * nb;
-            const double  fk   = D(M(M(Akd, xij), xi), mu);  // Akd xij xi / mu
-            if (bId == uId) {
-                for (int j1 = 0; j1 < J_NP; j1++) {
-                    if (sB.sd[j1]) {
-                        rB[j1SB] = A(rB[j1SB], M(transIJ, pcB[(int64_t)j1 * nb + bId]));
-                        rB[j1SB] = A(rB[j1SB], M(M(fk, krU[(int64_t)j1 * nb + uId]), dP));
-                        j1SB++;
+        __syncthreads();
+        const int col = part;  // phase 2: column col
+        if (live && col < NCOL) {
+            const int64_t bId = C.bId[c], eId = C.eId[c];
+            const bool    ok  = meta[2 * CPB + lane_c] != 0;
+            const double  nan = __longlong_as_double(0x7ff8000000000000LL);
+            for (int end = 0; end < 2; end++) {
+                const int64_t n    = end ? eId : bId;
+                const int     nsec = meta[end * CPB + lane_c];
+                double*       dst  = end ? O.offBE : O.offEB;
+                dst[(int64_t)col * nc + c] = !ok ? nan : (end ? M(0.0, dt) : -M(0.0, dt));  // row 0
+                for (int r = 1; r <= NCOM; r++) {
+                    double v = nan;
+                    if (ok) {
+                        double s2 = 0;
+                        for (int k = 0; k < nsec; k++)
+                            s2 = A(s2, M(R(end, k, r - 1, lane_c), B.dSec_dPri[(int64_t)(k * NCOL + col) * nb + n]));
+                        v = M(A(s2, col == 0 ? PR(end, r - 1, lane_c) : 0.0), dt);
+                        if (!end) v = -v;
                     }
-                    if (sE.sd[j1]) {
-                        rE[j1SE] = S(rE[j1SE], M(transIJ, pcB[(int64_t)j1 * nb + eId]));
-                        j1SE++;
-                    }
+                    dst[(int64_t)(r * NCOL + col) * nc + c] = v;
                 }
-                const int nv = sB.vn[j];
-                for (int k = 0; k < nv; k++) {
-                    const int64_t ok = (int64_t)(j * NCOM + k) * nb;
-                    const double  rx = exE[j] ? D(B.rhox[ok + bId], 2.0) : B.rhox[ok + uId];
-                    double        v  = M(M(-transIJ, rx), dGamma);
-                    v                = A(v, M(M(M(xij, transJ), B.xix[ok + uId]), dP));
-                    v                = A(v, M(D(M(-transIJ, B.mux[ok + uId]), mu), dP));
-                    rB[jxB + k]      = A(rB[jxB + k], v);
-                    if (exE[j])
-                        rE[jxE + k] = A(rE[jxE + k], M(D(M(-transIJ, B.rhox[ok + eId]), 2.0), dGamma));
-                }
-                if (i < nv) rB[jxB + i] = A(rB[jxB + i], M(M(xi, transJ), dP));
-            } else {
-                for (int j1 = 0; j1 < J_NP; j1++) {
-                    if (sB.sd[j1]) {
-                        rB[j1SB] = A(rB[j1SB], M(transIJ, pcB[(int64_t)j1 * nb + bId]));
-                        j1SB++;
-                    }
-                    if (sE.sd[j1]) {
-                        rE[j1SE] = S(rE[j1SE], M(transIJ, pcB[(int64_t)j1 * nb + eId]));
-                        rE[j1SE] = A(rE[j1SE], M(M(fk, krU[(int64_t)j1 * nb + uId]), dP));
-                        j1SE++;
-                    }
-                }
-                const int nv = sE.vn[j];
-                for (int k = 0; k < nv; k++) {
-                    const int64_t ok = (int64_t)(j * NCOM + k) * nb;
-                    const double  rx = exB[j] ? D(B.rhox[ok + eId], 2.0) : B.rhox[ok + uId];
-                    double        v  = M(M(-transIJ, rx), dGamma);
-                    v                = A(v, M(M(M(xij, transJ), B.xix[ok + uId]), dP));
-                    v                = A(v, M(D(M(-transIJ, B.mux[ok + uId]), mu), dP));
-                    rE[jxE + k]      = A(rE[jxE + k], v);
-                    if (exB[j])
-                        rB[jxB + k] = A(rB[jxB + k], M(D(M(-transIJ, B.rhox[ok + bId]), 2.0), dGamma));
-                }
-                if (i < nv) rE[jxE + i] = A(rE[jxE + i], M(M(xi, transJ), dP));
-            }
-            jxB += sB.vn[j];
-            jxE += sE.vn[j];
-        }
-        // row i + 1 of both ends; (row eId, col bId) = -bmatB, (row bId, col eId) = bmatE
-        product_row(B, nb, bId, NCOL, sB.ncol, rB, pB, dt, O.offEB, nc, c, i + 1, true);
-        product_row(B, nb, eId, NCOL, sE.ncol, rE, pE, dt, O.offBE, nc, c, i + 1, false);
-        if (i == 0) {
-            // row 0 of dF/dXp and dF/dXs is zero
-            for (int col = 0; col < NCOL; col++) {
-                O.offEB[(int64_t)col * nc + c] = -M(0.0, dt);
-                O.offBE[(int64_t)col * nc + c] = M(0.0, dt);
             }
         }
     }
@@ -295,10 +344,13 @@ template <int NCOM>
 cudaError_t launch_jac(const ConnDev& C, const ocpf_jac_bulk& B, const int32_t* up, const double* uprho, double dt,
                        const ocpf_jac_out& O, int sms, cudaStream_t st)
 {
-    const int64_t t1 = NCOM * C.nconn, t2 = (NCOM + 1) * C.nb;
-    const int     g1 = (int)std::min<int64_t>((t1 + 127) / 128, (int64_t)sms * 16);
+    using CB = ConnBlock<NCOM>;
+    // per device; cheap, so on every launch
+    cudaFuncSetAttribute(k_conn_block<NCOM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CB::SMEM);
+    const int64_t t2 = (NCOM + 1) * C.nb;
+    const int     g1 = (int)std::min<int64_t>((C.nconn + CB::CPB - 1) / CB::CPB, (int64_t)sms * 8);
     const int     g2 = (int)std::min<int64_t>((t2 + 127) / 128, (int64_t)sms * 16);
-    if (C.nconn > 0) k_conn_rows<NCOM><<<g1, 128, 0, st>>>(C, B, up, uprho, dt, O);
+    if (C.nconn > 0) k_conn_block<NCOM><<<g1, CB::THREADS, CB::SMEM, st>>>(C, B, up, uprho, dt, O);
     if (C.nb > 0) k_diag_rows<NCOM><<<g2, 128, 0, st>>>(C, B, O);
     return cudaGetLastError();
 }
