@@ -64,6 +64,24 @@ class SyntheticFIM:
         self.z_inj = np.empty(self.nc); self.z_inj[order] = zi / zi.sum()
         self.pv = poro * 1000.0                                   # ft3 of pore volume per cell
         self.noise = rng.normal(0.0, 1.0, self.shape)
+        self.lnk, self.poro, self.depth = lnk, poro, depth
+
+    def connections(self):
+        """7-point connections (begin, end, area): x, y and z neighbours,
+        area = harmonic mean permeability (mD) x 1 ft^2 face."""
+        idx = np.arange(self.n, dtype=np.int64).reshape(self.shape)
+        k = np.exp(self.lnk)
+        b, e, a = [], [], []
+        for axis in (2, 1, 0):
+            lo = [slice(None)] * 3
+            hi = [slice(None)] * 3
+            lo[axis] = slice(0, self.shape[axis] - 1)
+            hi[axis] = slice(1, self.shape[axis])
+            lo, hi = tuple(lo), tuple(hi)
+            b.append(idx[lo].ravel())
+            e.append(idx[hi].ravel())
+            a.append((2 * k[lo] * k[hi] / (k[lo] + k[hi])).ravel())
+        return np.concatenate(b), np.concatenate(e), np.concatenate(a)
 
     def _fields(self, t):
         """(P, z) at time t (fractional time steps)."""
@@ -105,14 +123,18 @@ def _gather(st, idx):
 
 
 def run(forms=("plain", "fast"), steps=20, newton=4, device=0, log=print, grid=(60, 220, 85), hook=None,
-        sample=4096, seed=5):
+        sample=4096, seed=5, chain=True):
     """Runs the loop once per form in lockstep on identical inputs; returns
     per-iteration flash times and, for every form other than the first,
     phase-count differences and output errors against the first. With
     ``hook``, for a seeded sample of ``sample`` cells every iteration calls
     hook(form, step, it, before, after): the sample's inputs and warm-start
     state before the flash and its outputs after (host arrays, cell-major),
-    e.g. to check them against an oracle."""
+    e.g. to check them against an oracle. With ``chain``, after the last
+    form's flash every iteration also runs what IsoT_FIM does next on the
+    same device arrays -- KrPc (ocpf_cal_krpc), the upstream choice and the
+    Jacobian's bulk part (ocpf_fim_upwind, ocpf_fim_jacobian) -- and their
+    times are reported."""
     torch = _torch()
     from .flash import MixtureCompBatch
     from .workload import bench_fluid
@@ -133,6 +155,24 @@ def run(forms=("plain", "fast"), steps=20, newton=4, device=0, log=print, grid=(
                               device=drv.dev)
     rec = {f: [] for f in forms}
     acc = {f: [] for f in forms[1:]}
+    chain_ms = {"krpc": [], "upwind": [], "jacobian": []}
+    if chain:
+        from . import synth
+        from .fim_jacobian import ConnGraph
+        from .krpc import FlowUnitBatch
+        cst = ctx[-1][2]
+        fu = FlowUnitBatch([synth.corey_tables(501)], device)
+        kout = fu.new_outputs(drv.n)
+        cb, ce, ca = drv.connections()
+        graph = ConnGraph(drv.n, cb, ce, ca, device)
+        bulk = {k: cst.out[k] for k in ("phaseExist", "pSderExist", "pVnumCom", "S", "rho", "xi", "mu", "muP",
+                                        "xiP", "rhoP", "xij", "rhox", "xix", "mux", "dSec_dPri", "vfP", "vfi")}
+        bulk.update({"kr": kout["kr"], "Pj": kout["Pj"], "dKr_dS": kout["dKr_dS"], "dPcj_dS": kout["dPcj_dS"],
+                     "v": torch.full((drv.n,), 1000.0, dtype=torch.float64, device=drv.dev),
+                     "poroP": torch.as_tensor(3e-6 * drv.poro.reshape(-1), device=drv.dev),
+                     "depth": torch.as_tensor(drv.depth.reshape(-1).astype(np.float64), device=drv.dev)})
+        cev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        jout = None
     for step in range(steps):
         for it in range(newton):
             P, T, N = drv.inputs(step, it, newton)
@@ -144,7 +184,18 @@ def run(forms=("plain", "fast"), steps=20, newton=4, device=0, log=print, grid=(
                 ev[k][0].record()
                 m.flash_fim(st, form=form)
                 ev[k][1].record()
+            if chain:
+                cev[0].record()
+                fu.cal_krpc(cst.P, cst.out["S"], None, out=kout)
+                cev[1].record()
+                up, urho = graph.upwind(bulk)
+                cev[2].record()
+                jout = graph.jacobian(drv.nc, 1.0, bulk, up, urho, out=jout)
+                cev[3].record()
             torch.cuda.synchronize()
+            if chain:
+                for key, a_, b_ in (("krpc", 0, 1), ("upwind", 1, 2), ("jacobian", 2, 3)):
+                    chain_ms[key].append(cev[a_].elapsed_time(cev[b_]))
             if hook is not None:
                 for form, m, st in ctx:
                     hook(form, step, it, before[form], _gather(st, idx)["out"])
@@ -172,10 +223,18 @@ def run(forms=("plain", "fast"), steps=20, newton=4, device=0, log=print, grid=(
         log(f"step {step}: " + ", ".join(f"{f} {np.mean(rec[f][-newton:]):.1f} ms" for f in forms))
     for _, m, _ in ctx:
         m.close()
+    if chain:
+        finite = bool(torch.isfinite(jout["diag"]).all().item())
+        graph.close()
+        fu.close()
     out = {"cells": drv.n, "steps": steps, "newton": newton,
            "ms_per_iteration": {f: float(np.mean(v)) for f, v in rec.items()},
            "ms_per_iteration_first": {f: float(v[0]) for f, v in rec.items()},
            "ms_per_iteration_after_first": {f: float(np.mean(v[1:])) for f, v in rec.items()}}
+    if chain:
+        out["after_flash_ms_per_iteration"] = {k: float(np.mean(v)) for k, v in chain_ms.items()}
+        out["after_flash_form"] = forms[-1]
+        out["jacobian_finite"] = finite
     for f, v in acc.items():
         out[f"{f}_vs_{forms[0]}"] = {"max_phase_mismatch": max(a["phase_mismatch"] for a in v),
                                      "max_rel_err": max(a["max_rel_err"] for a in v)}

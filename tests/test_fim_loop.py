@@ -1,7 +1,8 @@
 """The flash inside the synthetic FIM loop (warm starts across Newton
 iterations and time steps: skip cache, two-phase warm starts, relaxed
-stability), on a reduced grid: every form runs, and the faster forms agree
-with the plain FP64 form iteration by iteration."""
+stability), on a reduced grid: every form runs, the faster forms agree with
+the plain FP64 form iteration by iteration, and KrPc, the upstream choice and
+the Jacobian's bulk part run after the flash on its device arrays."""
 import pytest
 
 
@@ -15,3 +16,6 @@ def test_fim_loop_forms_agree_with_plain():
     assert b["max_rel_err"] < 1e-8, b
     m = res["mixed_vs_plain"]
     assert m["max_phase_mismatch"] <= 2, m
+    # the steps after the flash ran on its arrays every iteration
+    assert res["jacobian_finite"]
+    assert set(res["after_flash_ms_per_iteration"]) == {"krpc", "upwind", "jacobian"}
