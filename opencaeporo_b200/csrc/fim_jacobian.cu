@@ -108,7 +108,14 @@ struct ConnBlock {
     static constexpr int CPB  = NCOM <= 7 ? 32 : (NCOM <= 10 ? 16 : 8);
     static constexpr int TPC  = NCOL <= 8 ? 8 : 16;  // threads per connection (>= NCOL)
     static constexpr int THREADS = CPB * TPC;
-    static constexpr size_t SMEM = sizeof(double) * (size_t)CPB * 2 * (NSEC * NCOM + NCOM) + sizeof(int) * CPB * 3;
+    // per connection, staged once: 11 scalars of each phase's upstream
+    // (dP, xi, kr, mu, muP, xiP, rhoP of upstream, begin and end, transJ,
+    // upstream exists), the 9 saturation derivatives of each phase (dPc of
+    // both ends, dKr of upstream), and 5 composition partials of each phase
+    // and component (rhox, xix, mux of upstream, rhox of begin and end)
+    static constexpr int STG = 3 * 11 + 3 * 9 + 3 * 5 * NCOM;
+    static constexpr size_t SMEM =
+        sizeof(double) * (size_t)CPB * (2 * (NSEC * NCOM + NCOM) + STG) + sizeof(int) * CPB * 3;
     static_assert(NCOL <= TPC, "one thread per column");
 };
 
@@ -129,7 +136,13 @@ __global__ void __launch_bounds__(ConnBlock<NCOM>::THREADS) k_conn_block(const C
     // rows[end][k][i][cl], prow[end][i][cl], then nsec[end][cl], ok[cl]
     double* rows = sm;
     double* prow = sm + (size_t)2 * NSEC * NCOM * CPB;
-    int*    meta = (int*)(prow + (size_t)2 * NCOM * CPB);
+    double* stg  = prow + (size_t)2 * NCOM * CPB;
+    int*    meta = (int*)(stg + (size_t)CB::STG * CPB);
+    // staged values: scalar v of phase j, derivative q (= 3 j1 + which) of
+    // phase j, partial w of phase j and component k
+    auto SC = [&](int j, int v, int cl) -> double& { return stg[(j * 11 + v) * CPB + cl]; };
+    auto PK = [&](int j, int q, int cl) -> double& { return stg[(33 + j * 9 + q) * CPB + cl]; };
+    auto CX = [&](int j, int k, int w, int cl) -> double& { return stg[(60 + (j * NCOM + k) * 5 + w) * CPB + cl]; };
     auto R  = [&](int end, int k, int i, int cl) -> double& { return rows[((end * NSEC + k) * NCOM + i) * CPB + cl]; };
     auto PR = [&](int end, int i, int cl) -> double& { return prow[(end * NCOM + i) * CPB + cl]; };
     const int64_t nc = C.nconn, nb = C.nb;
@@ -143,6 +156,52 @@ __global__ void __launch_bounds__(ConnBlock<NCOM>::THREADS) k_conn_block(const C
             for (int k = 0; k < NSEC; k++) R(0, k, i, lane_c) = R(1, k, i, lane_c) = 0;
             PR(0, i, lane_c) = PR(1, i, lane_c) = 0;
         }
+        // phase 0: each connection's per-phase upstream data, once
+        if (live) {
+            const int64_t bId = C.bId[c], eId = C.eId[c];
+            const double  Akd    = M(J_CONV1 * J_CONV2, C.area[c]);
+            const double  dGamma = M(J_GRAV, S(B.depth[bId], B.depth[eId]));
+            for (int j = part; j < J_NP; j += CB::TPC) {
+                const int64_t u   = up[j * nc + c];
+                const bool    xb  = B.phaseExist[j * nb + bId] != 0, xe = B.phaseExist[j * nb + eId] != 0;
+                const bool    val = (u == bId || u == eId);
+                const bool    exU = val && (u == bId ? xb : xe);
+                SC(j, 10, lane_c) = exU ? 1.0 : 0.0;
+                if (exU) {
+                    const int64_t uj = j * nb + u;
+                    SC(j, 0, lane_c) = S(S(B.Pj[j * nb + bId], B.Pj[j * nb + eId]), M(uprho[j * nc + c], dGamma));
+                    SC(j, 1, lane_c) = B.xi[uj];
+                    SC(j, 2, lane_c) = B.kr[uj];
+                    SC(j, 3, lane_c) = B.mu[uj];
+                    SC(j, 4, lane_c) = B.muP[uj];
+                    SC(j, 5, lane_c) = B.xiP[uj];
+                    SC(j, 6, lane_c) = B.rhoP[uj];
+                    SC(j, 7, lane_c) = xb ? B.rhoP[j * nb + bId] : 0.0;
+                    SC(j, 8, lane_c) = xe ? B.rhoP[j * nb + eId] : 0.0;
+                    SC(j, 9, lane_c) = D(M(Akd, B.kr[uj]), B.mu[uj]);
+                }
+            }
+            for (int q = part; q < 9; q += CB::TPC) {
+                const int     j = q / 3, j1 = q % 3;
+                const int64_t u = up[j * nc + c];
+                const int64_t f = (int64_t)(3 * j + j1) * nb;
+                PK(j, 3 * j1 + 0, lane_c) = B.dPcj_dS[f + bId];
+                PK(j, 3 * j1 + 1, lane_c) = B.dPcj_dS[f + eId];
+                PK(j, 3 * j1 + 2, lane_c) = (u == bId || u == eId) ? B.dKr_dS[f + u] : 0.0;
+            }
+            for (int q = part; q < J_NP * NCOM; q += CB::TPC) {
+                const int     j = q / NCOM, k = q % NCOM;
+                const int64_t u = up[j * nc + c];
+                const int64_t f = (int64_t)(j * NCOM + k) * nb;
+                const bool    val = (u == bId || u == eId);
+                CX(j, k, 0, lane_c) = val ? B.rhox[f + u] : 0.0;
+                CX(j, k, 1, lane_c) = val ? B.xix[f + u] : 0.0;
+                CX(j, k, 2, lane_c) = val ? B.mux[f + u] : 0.0;
+                CX(j, k, 3, lane_c) = B.rhox[f + bId];
+                CX(j, k, 4, lane_c) = B.rhox[f + eId];
+            }
+        }
+        __syncthreads();
         if (live && i < NCOM) {
             const int64_t  bId = C.bId[c], eId = C.eId[c];
             const double   Akd    = M(J_CONV1 * J_CONV2, C.area[c]);
@@ -176,19 +235,17 @@ __global__ void __launch_bounds__(ConnBlock<NCOM>::THREADS) k_conn_block(const C
                 int    jxE = (sE.sd[0] ? 1 : 0) + (sE.sd[1] ? 1 : 0) + (sE.sd[2] ? 1 : 0);
                 for (int j = 0; j < J_NP; j++) {
                     const int64_t uId = up[j * nc + c];
-                    const bool    exU = uId == bId ? exB[j] : exE[j];
+                    const bool    exU = SC(j, 10, lane_c) != 0;
                     if (!exU) {
                         jxB += sB.vn[j];
                         jxE += sE.vn[j];
                         continue;
                     }
-                    const int64_t uj = j * nb + uId, bj = j * nb + bId, ej = j * nb + eId;
-                    const double  dP = S(S(B.Pj[bj], B.Pj[ej]), M(uprho[j * nc + c], dGamma));
-                    const double  xi = B.xi[uj], kr = B.kr[uj], mu = B.mu[uj];
-                    const double  muP = B.muP[uj], xiP = B.xiP[uj], rhoP = B.rhoP[uj];
-                    const double  transJ  = D(M(Akd, kr), mu);
-                    const double  xij     = B.xij[(int64_t)(j * NCOM + i) * nb + uId];
-                    const double  transIJ = M(M(xij, xi), transJ);
+                    const double dP = SC(j, 0, lane_c), xi = SC(j, 1, lane_c), mu = SC(j, 3, lane_c);
+                    const double muP = SC(j, 4, lane_c), xiP = SC(j, 5, lane_c), rhoP = SC(j, 6, lane_c);
+                    const double transJ  = SC(j, 9, lane_c);
+                    const double xij     = B.xij[(int64_t)(j * NCOM + i) * nb + uId];
+                    const double transIJ = M(M(xij, xi), transJ);
                     pB = A(pB, transIJ);
                     pE = S(pE, transIJ);
                     double tmp = M(M(M(xij, transJ), xiP), dP);
@@ -200,43 +257,43 @@ __global__ void __launch_bounds__(ConnBlock<NCOM>::THREADS) k_conn_block(const C
                         tmp = A(tmp, M(transIJ, M(-rhoP, dGamma)));
                         pE  = A(pE, tmp);
                     } else {
-                        pB = A(pB, M(M(transIJ, M(-B.rhoP[bj], dGamma)), 0.5));
-                        pE = A(pE, M(M(transIJ, M(-B.rhoP[ej], dGamma)), 0.5));
+                        pB = A(pB, M(M(transIJ, M(-SC(j, 7, lane_c), dGamma)), 0.5));
+                        pE = A(pE, M(M(transIJ, M(-SC(j, 8, lane_c), dGamma)), 0.5));
                         if (bId == uId)
                             pB = A(pB, tmp);
                         else
                             pE = A(pE, tmp);
                     }
-                    int           j1SB = 0, j1SE = 0;
-                    const double* pcJ  = B.dPcj_dS + (int64_t)(3 * j) * nb;
-                    const double* krJ  = B.dKr_dS + (int64_t)(3 * j) * nb;
-                    const double  fk   = D(M(M(Akd, xij), xi), mu);  // Akd xij xi / mu
+                    int          j1SB = 0, j1SE = 0;
+                    const double fk   = D(M(M(Akd, xij), xi), mu);  // Akd xij xi / mu
                     if (bId == uId) {
+#pragma unroll
                         for (int j1 = 0; j1 < J_NP; j1++) {
                             if (sB.sd[j1]) {
                                 double& r = R(0, j1SB, i, lane_c);
-                                r         = A(r, M(transIJ, pcJ[(int64_t)j1 * nb + bId]));
-                                r         = A(r, M(M(fk, krJ[(int64_t)j1 * nb + uId]), dP));
+                                r         = A(r, M(transIJ, PK(j, 3 * j1 + 0, lane_c)));
+                                r         = A(r, M(M(fk, PK(j, 3 * j1 + 2, lane_c)), dP));
                                 j1SB++;
                             }
                             if (sE.sd[j1]) {
                                 double& r = R(1, j1SE, i, lane_c);
-                                r         = S(r, M(transIJ, pcJ[(int64_t)j1 * nb + eId]));
+                                r         = S(r, M(transIJ, PK(j, 3 * j1 + 1, lane_c)));
                                 j1SE++;
                             }
                         }
                         const int nv = sB.vn[j];
-                        for (int k = 0; k < nv; k++) {
-                            const int64_t ok2 = (int64_t)(j * NCOM + k) * nb;
-                            const double  rx  = exE[j] ? M(B.rhox[ok2 + bId], 0.5) : B.rhox[ok2 + uId];
-                            double        v   = M(M(-transIJ, rx), dGamma);
-                            v                 = A(v, M(M(M(xij, transJ), B.xix[ok2 + uId]), dP));
-                            v                 = A(v, M(D(M(-transIJ, B.mux[ok2 + uId]), mu), dP));
-                            double& r         = R(0, jxB + k, i, lane_c);
-                            r                 = A(r, v);
+#pragma unroll
+                        for (int k = 0; k < NCOM - 1; k++) {
+                            if (k >= nv) break;
+                            const double rx = exE[j] ? M(CX(j, k, 3, lane_c), 0.5) : CX(j, k, 0, lane_c);
+                            double       v  = M(M(-transIJ, rx), dGamma);
+                            v               = A(v, M(M(M(xij, transJ), CX(j, k, 1, lane_c)), dP));
+                            v               = A(v, M(D(M(-transIJ, CX(j, k, 2, lane_c)), mu), dP));
+                            double& r       = R(0, jxB + k, i, lane_c);
+                            r               = A(r, v);
                             if (exE[j]) {
                                 double& re = R(1, jxE + k, i, lane_c);
-                                re         = A(re, M(M(M(-transIJ, B.rhox[ok2 + eId]), 0.5), dGamma));
+                                re         = A(re, M(M(M(-transIJ, CX(j, k, 4, lane_c)), 0.5), dGamma));
                             }
                         }
                         if (i < nv) {
@@ -244,31 +301,33 @@ __global__ void __launch_bounds__(ConnBlock<NCOM>::THREADS) k_conn_block(const C
                             r         = A(r, M(M(xi, transJ), dP));
                         }
                     } else {
+#pragma unroll
                         for (int j1 = 0; j1 < J_NP; j1++) {
                             if (sB.sd[j1]) {
                                 double& r = R(0, j1SB, i, lane_c);
-                                r         = A(r, M(transIJ, pcJ[(int64_t)j1 * nb + bId]));
+                                r         = A(r, M(transIJ, PK(j, 3 * j1 + 0, lane_c)));
                                 j1SB++;
                             }
                             if (sE.sd[j1]) {
                                 double& r = R(1, j1SE, i, lane_c);
-                                r         = S(r, M(transIJ, pcJ[(int64_t)j1 * nb + eId]));
-                                r         = A(r, M(M(fk, krJ[(int64_t)j1 * nb + uId]), dP));
+                                r         = S(r, M(transIJ, PK(j, 3 * j1 + 1, lane_c)));
+                                r         = A(r, M(M(fk, PK(j, 3 * j1 + 2, lane_c)), dP));
                                 j1SE++;
                             }
                         }
                         const int nv = sE.vn[j];
-                        for (int k = 0; k < nv; k++) {
-                            const int64_t ok2 = (int64_t)(j * NCOM + k) * nb;
-                            const double  rx  = exB[j] ? M(B.rhox[ok2 + eId], 0.5) : B.rhox[ok2 + uId];
-                            double        v   = M(M(-transIJ, rx), dGamma);
-                            v                 = A(v, M(M(M(xij, transJ), B.xix[ok2 + uId]), dP));
-                            v                 = A(v, M(D(M(-transIJ, B.mux[ok2 + uId]), mu), dP));
-                            double& r         = R(1, jxE + k, i, lane_c);
-                            r                 = A(r, v);
+#pragma unroll
+                        for (int k = 0; k < NCOM - 1; k++) {
+                            if (k >= nv) break;
+                            const double rx = exB[j] ? M(CX(j, k, 4, lane_c), 0.5) : CX(j, k, 0, lane_c);
+                            double       v  = M(M(-transIJ, rx), dGamma);
+                            v               = A(v, M(M(M(xij, transJ), CX(j, k, 1, lane_c)), dP));
+                            v               = A(v, M(D(M(-transIJ, CX(j, k, 2, lane_c)), mu), dP));
+                            double& r       = R(1, jxE + k, i, lane_c);
+                            r               = A(r, v);
                             if (exB[j]) {
                                 double& rb = R(0, jxB + k, i, lane_c);
-                                rb         = A(rb, M(M(M(-transIJ, B.rhox[ok2 + bId]), 0.5), dGamma));
+                                rb         = A(rb, M(M(M(-transIJ, CX(j, k, 3, lane_c)), 0.5), dGamma));
                             }
                         }
                         if (i < nv) {
@@ -294,12 +353,17 @@ __global__ void __launch_bounds__(ConnBlock<NCOM>::THREADS) k_conn_block(const C
                 const int     nsec = meta[end * CPB + lane_c];
                 double*       dst  = end ? O.offBE : O.offEB;
                 dst[(int64_t)col * nc + c] = !ok ? nan : (end ? M(0.0, dt) : -M(0.0, dt));  // row 0
+                double sec[NSEC];
+#pragma unroll
+                for (int k = 0; k < NSEC; k++) sec[k] = k < nsec ? B.dSec_dPri[(int64_t)(k * NCOL + col) * nb + n] : 0.0;
+#pragma unroll
                 for (int r = 1; r <= NCOM; r++) {
                     double v = nan;
                     if (ok) {
                         double s2 = 0;
-                        for (int k = 0; k < nsec; k++)
-                            s2 = A(s2, M(R(end, k, r - 1, lane_c), B.dSec_dPri[(int64_t)(k * NCOL + col) * nb + n]));
+#pragma unroll
+                        for (int k = 0; k < NSEC; k++)
+                            if (k < nsec) s2 = A(s2, M(R(end, k, r - 1, lane_c), sec[k]));
                         v = M(A(s2, col == 0 ? PR(end, r - 1, lane_c) : 0.0), dt);
                         if (!end) v = -v;
                     }
