@@ -105,7 +105,7 @@ template <int NCOM>
 struct ConnBlock {
     static constexpr int NCOL = NCOM + 1;
     static constexpr int NSEC = 3 + 2 * (NCOM - 1);  // dSec_dPri rows of a two-phase bulk
-    static constexpr int CPB  = NCOM <= 7 ? 32 : (NCOM <= 10 ? 16 : 8);
+    static constexpr int CPB  = NCOM <= 7 ? 16 : (NCOM <= 10 ? 8 : 4);
     static constexpr int TPC  = NCOL <= 8 ? 8 : 16;  // threads per connection (>= NCOL)
     static constexpr int THREADS = CPB * TPC;
     // per connection, staged once: 11 scalars of each phase's upstream
