@@ -487,11 +487,12 @@ def entries_arm(args):
     """The other flash entry points on the bench workload (1,048,576 fresh
     states of the 6-component fluid): ocpf_init_flash_fim (InitFlashFIM:
     the initial mole fractions z = Ni / sum Ni, S_w ~ U(0.05, 0.5), pore
-    volumes ~ U(50, 5000) ft3) and ocpf_flash_impec (FlashIMPEC of fresh
-    cells), each in the chosen form and in the plain FP64 form, timed with
-    CUDA events; the reference's own calls on the first states with every
-    host thread, and the error of the chosen form against them. One JSON
-    line; not the headline metric."""
+    volumes ~ U(50, 5000) ft3), ocpf_flash_impec (FlashIMPEC of fresh
+    cells) and ocpf_flash_fimn (FlashFIMn of fresh cells), each in the
+    chosen form and in the plain FP64 form, timed with CUDA events; the
+    reference's own calls on the first states with every host thread, and
+    the error of the chosen form against them. One JSON line; not the
+    headline metric."""
     import torch
     from oracle import compare as CMP
     from oracle import oracle as O
@@ -558,7 +559,8 @@ def entries_arm(args):
     res = {}
     for name, prep, call in (
             ("init_flash_fim", prep_init, lambda f: m.init_flash(st, Vt, form=f)),
-            ("flash_impec", prep_impec, lambda f: m.flash_impec(st, form=f, fresh=True))):
+            ("flash_impec", prep_impec, lambda f: m.flash_impec(st, form=f, fresh=True)),
+            ("flash_fimn", prep_impec, lambda f: m.flash_fimn(st, form=f, fresh=True))):
         t_form = timed(prep, lambda: call(args.form))
         gpu = st.to_host()
         if name == "init_flash_fim":
@@ -576,6 +578,11 @@ def entries_arm(args):
             sub = {k: v[ix] for k, v in gpu.items() if isinstance(v, np.ndarray)}
             e = CMP.per_cell_errors(sub, ref, nc)
             keys = CMP.FLOAT_KEYS
+        elif name == "flash_fimn":
+            ref = O.flash_fimn(fl, w["P"][ix], w["T"][ix], w["Ni"][ix], nthreads=cores)
+            sub = {k: v[ix] for k, v in gpu.items() if isinstance(v, np.ndarray)}
+            e = CMP.fimn_errors(sub, ref, nc)
+            keys = CMP.FLOAT_KEYS + ("nj",)  # res, resPc: residuals, determined only to rounding
         else:
             ref = O.flash_impec(fl, w["P"][ix], w["T"][ix], w["Ni"][ix], nthreads=cores)
             sub = {k: v[ix] for k, v in gpu.items() if isinstance(v, np.ndarray)}

@@ -284,6 +284,34 @@ int ocpf_init_flash_fim(ocpf_ctx* ctx, int64_t ncell, const ocpf_init_in* in, oc
 int ocpf_init_flash_impec(ocpf_ctx* ctx, int64_t ncell, const ocpf_init_in* in, ocpf_skip* skip, double* Ni,
                           ocpf_impec_out* out, int form, void* stream);
 
+/* Batched MixtureComp::FlashFIMn + IsoT_FIMn::PassFlashValue over ncell
+ * cells (src/MixtureComp.cpp:575-695, src/OCPFluidMethod.cpp:3152-3196),
+ * the flash of the FIM formulation whose secondary variables are the
+ * saturations and the phase moles n_ij: the same flash type and phase
+ * equilibrium as ocpf_flash_fim, then (CaldXsdXpAPI03, :4495-4631)
+ * out->dSec_dPri holds, per existing hydrocarbon phase in phase order, the
+ * rows dS_j/d(P, N), then dS_w/d(P, N), then the rows dn_ij/d(P, N)
+ * (bRowSizedSdP = NP + 1 + NP nc rows of numCom + 1 columns); xix, rhox and
+ * mux are the derivatives per n_ij (CalXiPn_partial, CalRhoPn_partial,
+ * CalMuPnLBC_partial), vfP and vfi follow CalVfiVfp_full03, and
+ * pVnumCom[w] = 0. out->nj (required here) receives the phase moles.
+ * res [3 (numCom + 1)][ncell] receives the first bRowSizedSdP entries of
+ * the solve's residual column (Bulk::res_n; zeros for a single hydrocarbon
+ * phase) and resPc [ncell] the reference's resPc (Bulk::resPc). The
+ * reference reads its njin and phaseExistin arguments only to form a phase
+ * count its branch never uses; they are not inputs here. The skip cache is
+ * read and written as by ocpf_flash_fim. Forms and asynchrony as
+ * ocpf_flash_fim. */
+int ocpf_flash_fimn(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
+                    ocpf_fim_out* out, double* res, double* resPc, int form, void* stream);
+
+/* Batched MixtureComp::InitFlashFIMn + IsoT_FIMn::PassFlashValue
+ * (src/MixtureComp.cpp:355-442, src/OCPFluidMethod.cpp:3129-3150): the
+ * initialisation of ocpf_init_flash_fim with the outputs of
+ * ocpf_flash_fimn. */
+int ocpf_init_flash_fimn(ocpf_ctx* ctx, int64_t ncell, const ocpf_init_in* in, ocpf_skip* skip, double* Ni,
+                         ocpf_fim_out* out, double* res, double* resPc, int form, void* stream);
+
 /* Several PVT regions at once -- the batched counterpart of a Bulk whose
  * cells belong to different regions (flashCal[PVTNUM[n]] in
  * src/OCPFluidMethod.cpp:1108-1120), with the cells grouped by region.

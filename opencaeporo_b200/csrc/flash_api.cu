@@ -484,10 +484,31 @@ extern "C" int ocpf_flash_impec(ocpf_ctx* c, int64_t ncell, const ocpf_impec_in*
     return rc;
 }
 
-// InitFlashFIM / InitFlashIMPEC: the initial-state inputs as the FIM input
-// record (z in place of Ni, S for the water saturation) and the launch.
+extern "C" int ocpf_flash_fimn(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* sk,
+                               ocpf_fim_out* out, double* res, double* resPc, int form, void* stream)
+{
+    if (!c || ncell < 0) return OCPF_EINVAL;
+    if (ncell == 0) return OCPF_OK;
+    if (!fim_args_ok(c, in, sk, out) || !out->nj || !res || !resPc) return OCPF_EINVAL;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    ocpf_skip s{};
+    if (sk) s = *sk;
+    const FlashTail tail{FM_FIMN, nullptr, nullptr, nullptr, res, resPc};
+    const int rc = launch_form(c, form, ncell, ncell, *in, s, *out, (cudaStream_t)stream, true, -1, tail);
+    c->timed     = (rc == OCPF_OK);
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+// InitFlashFIM / InitFlashIMPEC / InitFlashFIMn: the initial-state inputs as
+// the FIM input record (z in place of Ni, S for the water saturation) and the
+// launch; `tail` names the entry point's extra outputs (vpore and ni are
+// filled in here).
 static int launch_init(ocpf_ctx* c, int64_t ncell, const ocpf_init_in* in, ocpf_skip* sk, double* Ni,
-                       const ocpf_fim_out& fo, double* vj, int form, void* stream)
+                       const ocpf_fim_out& fo, FlashTail tail, int form, void* stream)
 {
     ocpf_fim_in fin{};
     fin.P  = in->P;
@@ -499,7 +520,9 @@ static int launch_init(ocpf_ctx* c, int64_t ncell, const ocpf_init_in* in, ocpf_
     if (prev != c->device) cudaSetDevice(c->device);
     ocpf_skip s{};
     if (sk) s = *sk;
-    const FlashTail tail{vj ? (FM_INIT | FM_IMPEC) : FM_INIT, vj, in->Vpore, Ni};
+    tail.mode |= FM_INIT;
+    tail.vpore = in->Vpore;
+    tail.ni    = Ni;
     const int rc = launch_form(c, form, ncell, ncell, fin, s, fo, (cudaStream_t)stream, true, -1, tail);
     c->timed     = (rc == OCPF_OK);
     if (prev != c->device) cudaSetDevice(prev);
@@ -518,7 +541,7 @@ extern "C" int ocpf_init_flash_fim(ocpf_ctx* c, int64_t ncell, const ocpf_init_i
     if (ncell == 0) return OCPF_OK;
     if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
     if (!init_in_ok(in) || !Ni || !fim_out_ok(out) || !skip_ok(c, sk)) return OCPF_EINVAL;
-    return launch_init(c, ncell, in, sk, Ni, *out, nullptr, form, stream);
+    return launch_init(c, ncell, in, sk, Ni, *out, FlashTail{FM_FIM, nullptr, nullptr, nullptr}, form, stream);
 }
 
 extern "C" int ocpf_init_flash_impec(ocpf_ctx* c, int64_t ncell, const ocpf_init_in* in, ocpf_skip* sk,
@@ -528,7 +551,20 @@ extern "C" int ocpf_init_flash_impec(ocpf_ctx* c, int64_t ncell, const ocpf_init
     if (ncell == 0) return OCPF_OK;
     if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
     if (!init_in_ok(in) || !Ni || !impec_out_ok(out) || !skip_ok(c, sk)) return OCPF_EINVAL;
-    return launch_init(c, ncell, in, sk, Ni, impec_as_fim(*out), out->vj, form, stream);
+    return launch_init(c, ncell, in, sk, Ni, impec_as_fim(*out), FlashTail{FM_IMPEC, out->vj, nullptr, nullptr},
+                       form, stream);
+}
+
+extern "C" int ocpf_init_flash_fimn(ocpf_ctx* c, int64_t ncell, const ocpf_init_in* in, ocpf_skip* sk, double* Ni,
+                                    ocpf_fim_out* out, double* res, double* resPc, int form, void* stream)
+{
+    if (!c || ncell < 0) return OCPF_EINVAL;
+    if (ncell == 0) return OCPF_OK;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (!init_in_ok(in) || !Ni || !fim_out_ok(out) || !out->nj || !res || !resPc || !skip_ok(c, sk))
+        return OCPF_EINVAL;
+    return launch_init(c, ncell, in, sk, Ni, *out, FlashTail{FM_FIMN, nullptr, nullptr, nullptr, res, resPc}, form,
+                       stream);
 }
 
 extern "C" int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,

@@ -8,9 +8,9 @@
 namespace ocpf {
 
 // Which of the reference's flash entry points a launch runs (bit flags):
-// FlashFIM, FlashIMPEC, InitFlashFIM (FM_INIT) or InitFlashIMPEC
-// (FM_INIT | FM_IMPEC).
-enum : int { FM_FIM = 0, FM_IMPEC = 1, FM_INIT = 2 };
+// FlashFIM, FlashIMPEC, FlashFIMn (FM_FIMN), InitFlashFIM (FM_INIT),
+// InitFlashIMPEC (FM_INIT | FM_IMPEC) or InitFlashFIMn (FM_INIT | FM_FIMN).
+enum : int { FM_FIM = 0, FM_IMPEC = 1, FM_INIT = 2, FM_FIMN = 4 };
 
 // The entry point of a launch and the arrays beyond ocpf_fim_in/out that it
 // reads or writes. With FM_INIT, ocpf_fim_in.Ni holds the mole fractions z
@@ -20,6 +20,8 @@ struct FlashTail {
     double*       vj;     // [3][n] phase volumes (FM_IMPEC), or null
     const double* vpore;  // [n] pore volumes, ft3 (FM_INIT)
     double*       ni;     // [numCom][n] moles after the flash (FM_INIT); may alias in.Ni
+    double*       res;    // [3 (numCom + 1)][n] FlashFIMn's residual terms, first rows written (FM_FIMN)
+    double*       resPc;  // [n] (FM_FIMN)
 };
 
 template <int NC>
@@ -204,13 +206,16 @@ struct FimCell : CellFlash<NC> {
     }
 
     // The whole flash of one cell on this thread (FlashFIM, FlashIMPEC,
-    // InitFlashFIM or InitFlashIMPEC by tl.mode).
+    // InitFlashFIM or InitFlashIMPEC by tl.mode; FlashFIMn or InitFlashFIMn
+    // with FIMN, which kernels of their own instantiate so that the FIMn tail
+    // adds no registers to the others).
+    template <bool FIMN = false>
     __device__ void run(int64_t n_, int64_t stride, const ocpf_fim_in& in, const ocpf_skip& sk,
                         const ocpf_fim_out& out, const FlashTail& tl)
     {
         load_inputs(n_, stride, in, sk, tl);
         this->phase_equilibrium();
-        finalize(n_, stride, sk, out, tl);
+        finalize<FIMN>(n_, stride, sk, out, tl);
     }
 
     // Everything after PhaseEquilibrium: CalFlash's property tail, the
@@ -225,6 +230,8 @@ struct FimCell : CellFlash<NC> {
     // (:276-353, :210-258): the properties are formed per mole of
     // hydrocarbon, then Nh = Vpore (1 - S_w) / vf scales the phase moles and
     // volumes, Ni = z Nh and N_w = Vpore S_w xi_w, and Ni goes to tl.ni.
+    // With FIMN, FlashFIMn's tail (finalize_fimn) after the common part.
+    template <bool FIMN = false>
     __device__ void finalize(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out,
                              const FlashTail& tl)
     {
@@ -341,6 +348,10 @@ struct FimCell : CellFlash<NC> {
             vf *= Nh;
 #pragma unroll
             for (int i = 0; i < NC; i++) Ni[i] = zi[i] * Nh;
+        }
+        if constexpr (FIMN) {
+            finalize_fimn(n_, stride, sk, out, tl, label, exist, MW, vC, xiC, rhoC, muC, muA, gT, njC, vf);
+            return;
         }
 
         // ---- CalVfiVfp_full02, src/MixtureComp.cpp:3911-3989
@@ -652,6 +663,379 @@ struct FimCell : CellFlash<NC> {
                 out.mux[at(ow)]  = 0.0;
             }
         }
+        finish_fim(n_, stride, sk, out, exist, bw, xiW, xiPW, Nw, vf, vfP, S);
+    }
+
+    // FlashFIMn's tail after CalFlash (src/MixtureComp.cpp:627-694; with
+    // FM_INIT, InitFlashFIMn's after the moles are scaled, :390-441) and
+    // IsoT_FIMn::PassFlashValue's outputs (src/OCPFluidMethod.cpp:3179-3196).
+    // The secondary variables are the saturations and the phase moles n_ij:
+    // dSec_dPri holds dS/d(P, N) and dn_ij/d(P, N) (CaldXsdXpAPI03,
+    // :4495-4631), the property partials are taken per n_ij, and the solve's
+    // residual column goes to tl.res / tl.resPc.
+    //
+    // CaldXsdXp03 (:4633-4820) solves, by LU with partial pivoting, the
+    // (3 + 2 nc)-square system of the saturation definitions, the fugacity
+    // equalities and the component balances in the unknowns (S_0, S_1, S_w,
+    // n_0, n_1). The saturation unknowns appear only in their own equations
+    // (coefficient -1), so the first three pivots are those rows, they leave
+    // the others unchanged, and the rest is the LU of the 2 nc-square
+    // phase-mole block with its rows in the order the three row swaps leave
+    // them. Here that block is solved so (one right-hand side per column: P,
+    // N_1..N_nc, the residual; N_w moves no n_ij), then the saturation rows
+    // by back substitution. (Eliminating n_1 = N - n_0 first, as FlashFIM's
+    // derivatives do, gives the nc-square system fugN_0 + fugN_1, which is
+    // far worse conditioned near the critical point.)
+    __device__ void finalize_fimn(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out,
+                                  const FlashTail& tl, const int* label, const bool* exist, const double* MW,
+                                  const double* vC, const double* xiC, const double* rhoC, const double* muC,
+                                  const double (*muA)[5], const double* gT, const double* njC, double vf)
+    {
+        const int64_t N = stride;
+        auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
+        const bool   init = (tl.mode & FM_INIT) != 0;
+        const double CgTP = GAS_CONSTANT * T / P;
+
+        // ---- CalVjpVfpVfn_partial, src/MixtureComp.cpp:2581-2626 (internal
+        // phase order; the reference files vji and vjp by phase label)
+        double vji[2][NC], vjp[2] = {0, 0}, Zn[2][NC], Zp[2] = {0, 0};
+        double vfP = 0;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            if (j < NP) {
+                const double aj = Aj[j], bj = Bj[j], zj = Zj[j];
+                double       t[NC];
+                {
+                    double w[NC];
+#pragma unroll
+                    for (int k = 0; k < NC; k++) w[k] = sA[k] * x[j][k];
+#pragma unroll
+                    for (int i = 0; i < NC; i++) {
+                        double s = 0;
+#pragma unroll
+                        for (int k = 0; k < NC; k++) s += omb(i, k) * w[k];
+                        t[i] = sA[i] * s;
+                    }
+                }
+                const DzCoef dz(aj, bj, zj);
+                const double inu = 1.0 / nu[j];
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    Zn[j][i]  = dz(2 * inu * (t[i] - aj), inu * (Bi[i] - bj));
+                    vji[j][i] = CgTP * (zj + nu[j] * Zn[j][i]) - F.Vshift[i];
+                }
+                Zp[j]  = (dz.bmz * aj + dz.num_b * bj) / P * dz.inv_den;
+                vjp[j] = CgTP * nu[j] * (Zp[j] - zj / P);
+                vfP += vjp[j];
+            }
+        }
+
+        // ---- water, src/MixtureComp.cpp:629-656 (InitFlashFIMn :392-418)
+        const double bw   = F.pvtw[1] * (1 - F.pvtw[2] * (P - F.pvtw[0]));
+        const double bwp  = -F.pvtw[2] * F.pvtw[1];
+        const double xiW  = 1 / (CONV1 * bw);
+        if (init) Ni[NC] = Vp0 * Sw0 * xiW;
+        const double Nw   = Ni[NC];
+        const double Nt   = Nh + Nw;
+        const double xiPW = -bwp / (bw * bw * CONV1);
+        const double vw   = CONV1 * Nw * bw;
+        const double vfiW = CONV1 * bw;
+        const double vwp  = CONV1 * Nw * bwp;
+        vf += vw;
+        vfP += vwp;
+
+        // CalSaturation, src/MixtureComp.cpp:1178-1186
+        double vj[NPH] = {0, 0, vw};
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+            if (j < NP) vj[label[j]] = vC[j];
+        double S[NPH];
+#pragma unroll
+        for (int j = 0; j < NPH; j++) S[j] = exist[j] ? vj[j] / vf : 0;
+#pragma unroll
+        for (int j = 0; j < NPH; j++) {
+            out.S[at(j)]          = S[j];
+            out.phaseExist[at(j)] = exist[j] ? 1u : 0u;
+        }
+        out.phaseNum[n_] = (uint32_t)(NP + 1);
+        out.Nt[n_]       = Nt;
+        out.vf[n_]       = vf;
+        if (init && tl.ni) {
+#pragma unroll
+            for (int i = 0; i < NUMCOM; i++) tl.ni[at(i)] = Ni[i];
+        }
+
+        // ---- CaldXsdXpAPI03 and CalVfiVfp_full03 (src/MixtureComp.cpp:4822-4848)
+        const double vf2  = vf * vf;
+        double*      dsd  = out.dSec_dPri;
+        auto         dput = [&](int r, int c, double v) { dsd[at(r * NCOL + c)] = v; };
+        double       vfi[NUMCOM];
+        double       resPc = 0;
+        uint32_t     rows;
+        if (NP == 1) {
+            const int    j0 = label[0];
+            const double r0 = ((vfP - vwp) * vf - vfP * vj[j0]) / vf2;
+            dput(0, 0, r0);
+            dput(1, 0, -r0);
+#pragma unroll
+            for (int m = 0; m < NC; m++) {
+                const double v = vji[0][m] * vw / vf2;
+                dput(0, 1 + m, v);
+                dput(1, 1 + m, -v);
+            }
+            const double rw = -vfiW * vj[j0] / vf2;
+            dput(0, NC + 1, rw);
+            dput(1, NC + 1, -rw);
+#pragma unroll
+            for (int i = 0; i < NC; i++)
+#pragma unroll
+                for (int c = 0; c < NCOL; c++) dput(2 + i, c, c == 1 + i ? 1.0 : 0.0);
+            rows = NC + 2;
+#pragma unroll
+            for (int r = 0; r < NC + 2; r++) tl.res[at(r)] = 0.0;
+            // CalVfiVfp_full03: vfP unchanged, vfi = vji
+#pragma unroll
+            for (int i = 0; i < NC; i++) vfi[i] = vji[0][i];
+        } else {
+            // fugN of both phases (CalFugNAll, :2168-2251) and fugP (CalFugPAll,
+            // :2519-2579, with CalVjpVfpVfn_partial's Zp)
+            double A0[NC][NC], A1[NC][NC], Zt[NC];
+            this->fugn_phase(0, A0, false, nullptr, Zt);
+            this->fugn_phase(1, A1, false, nullptr, Zt);
+            double fugP[2][NC];
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const double aj = Aj[j], bj = Bj[j], zj = Zj[j];
+                const double Bp  = bj / P;
+                const double G   = (zj + D1 * bj) / (zj + D2 * bj);
+                const double zd2 = zj + D2 * bj;
+                const double Gp  = D1MD2 / (zd2 * zd2) * (Bp * zj - Zp[j] * bj);
+                double       t[NC];
+                {
+                    double w[NC];
+#pragma unroll
+                    for (int k = 0; k < NC; k++) w[k] = sA[k] * x[j][k];
+#pragma unroll
+                    for (int i = 0; i < NC; i++) {
+                        double s = 0;
+#pragma unroll
+                        for (int k = 0; k < NC; k++) s += omb(i, k) * w[k];
+                        t[i] = sA[i] * s;
+                    }
+                }
+                const double zmb = zj - bj;
+                const double Cp  = (zmb - P * (Zp[j] - Bp)) / (zmb * zmb);
+                const double iC  = zmb / P;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    const double E  = -aj / (D1MD2 * bj) * (2 * t[i] / aj - Bi[i] / bj);
+                    const double Dp = Bi[i] / bj * Zp[j];
+                    fugP[j][i]      = Cp * iC + Dp + E / G * Gp;
+                }
+            }
+            // residual column: resF = f_0 - f_1 (fugacities), resN = N - sum x nu
+            double resN[NC];
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                double r = Ni[i];
+                r -= x[0][i] * nu[0];
+                r -= x[1][i] * nu[1];
+                resN[i] = r;
+            }
+            // the phase-mole block: the fugacity rows -dF/dn_0 = -fugN_0,
+            // -dF/dn_1 = fugN_1 and the balance rows (1 at n_0i and n_1i), in
+            // the order dgetrf leaves them after swapping the first three
+            // fugacity rows for the saturation rows: fugacity rows 3..nc-1,
+            // balance rows 0..nc-1, fugacity rows 0..2
+            constexpr int D = 2 * NC;
+            constexpr int M = NC + 2;  // P, N_1..N_nc, residual
+            static_assert(NC >= 3, "the row order below assumes at least three components");
+            double Mx[D][D], X[D][M];
+            auto   fill = [&]() {
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    const int rf = i >= 3 ? i - 3 : D - 3 + i;  // fugacity row of component i
+                    const int rn = NC - 3 + i;                  // balance row of component i
+#pragma unroll
+                    for (int k = 0; k < NC; k++) {
+                        Mx[rf][k]      = -A0[i][k];
+                        Mx[rf][NC + k] = A1[i][k];
+                        Mx[rn][k]      = k == i ? 1.0 : 0.0;
+                        Mx[rn][NC + k] = k == i ? 1.0 : 0.0;
+                    }
+                    X[rf][0] = fugP[0][i] - fugP[1][i];
+                    X[rn][0] = 0.0;
+#pragma unroll
+                    for (int m = 0; m < NC; m++) {
+                        X[rf][1 + m] = 0.0;
+                        X[rn][1 + m] = m == i ? 1.0 : 0.0;
+                    }
+                    X[rf][M - 1] = this->phi[0][i] * x[0][i] * P - this->phi[1][i] * x[1][i] * P;
+                    X[rn][M - 1] = resN[i];
+                }
+            };
+            fill();
+            if (!gauss_solve_mem<D, M>(Mx, X)) {
+                status |= ST_SINGULAR;  // dgesv leaves the right-hand sides unchanged
+                fill();
+            }
+            auto dn = [&](int j, int i, int c) -> double { return X[j * NC + i][c]; };
+            // saturation rows: dS_j = sum_mk c_jmk dn_mk - rhs_S_j
+            const double rSP[3] = {(vfP * vj[label[0]] - vjp[0] * vf) / vf2,
+                                   (vfP * vj[label[1]] - vjp[1] * vf) / vf2, (vfP * vw - vwp * vf) / vf2};
+            const double rSW[3] = {vfiW * vj[label[0]] / vf2, vfiW * vj[label[1]] / vf2, vfiW * (vw - vf) / vf2};
+            const double rSR[3] = {S[label[0]] - vj[label[0]] / vf, S[label[1]] - vj[label[1]] / vf,
+                                   S[2] - vw / vf};
+            double resv[3 + 2 * NC];
+#pragma unroll
+            for (int e = 0; e < 3; e++) {  // e: internal phase 0, 1, then water
+                const double vje = e < 2 ? vj[label[e]] : vw;
+                const int    row = e < 2 ? label[e] : 2;
+#pragma unroll
+                for (int c = 0; c < M; c++) {
+                    // back substitution, last unknown first: (rhs - sum) / -1
+                    double t = c == 0 ? rSP[e] : (c == M - 1 ? rSR[e] : 0.0);
+#pragma unroll
+                    for (int m = 1; m >= 0; m--) {
+#pragma unroll
+                        for (int k = NC - 1; k >= 0; k--) {
+                            const double cf = (e == m) ? vji[m][k] * (vf - vje) / vf2 : -vji[m][k] * vje / vf2;
+                            t -= cf * dn(m, k, c);
+                        }
+                    }
+                    const double v = -t;
+                    if (c < M - 1)
+                        dput(row, c, v);
+                    else
+                        resv[row] = v;
+                }
+                dput(row, NC + 1, -rSW[e]);
+            }
+            // phase-mole rows, filed by phase label
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const int r0 = 3 + label[j] * NC;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+#pragma unroll
+                    for (int c = 0; c < M - 1; c++) dput(r0 + i, c, dn(j, i, c));
+                    dput(r0 + i, NC + 1, 0.0);
+                    resv[r0 + i] = dn(j, i, M - 1);
+                }
+            }
+            rows = 3 + 2 * NC;
+#pragma unroll
+            for (int r = 0; r < 3 + 2 * NC; r++) tl.res[at(r)] = resv[r];
+            // resPc (:4589-4597): the reference pairs internal phase j's vji
+            // with the residual block filed at position j
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+#pragma unroll
+                for (int i = 0; i < NC; i++) resPc += vji[j][i] * resv[3 + j * NC + i];
+            // CalVfiVfp_full03: phases in label order
+#pragma unroll
+            for (int i = 0; i < NC; i++) vfi[i] = 0;
+#pragma unroll
+            for (int j1 = 0; j1 < 2; j1++) {
+                const int jj = (label[0] == j1) ? 0 : 1;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    vfP += vji[jj][i] * dn(jj, i, 0);
+#pragma unroll
+                    for (int m = 0; m < NC; m++) vfi[m] += vji[jj][i] * dn(jj, i, 1 + m);
+                }
+            }
+        }
+        vfi[NC]              = vfiW;
+        out.bRowSizedSdP[n_] = rows;
+        tl.resPc[n_]         = resPc;
+        out.vfP[n_]          = vfP;
+#pragma unroll
+        for (int i = 0; i < NUMCOM; i++) out.vfi[at(i)] = vfi[i];
+
+        // ---- CalXiPn_partial, CalRhoPn_partial, CalMuPnLBC_partial
+        // (src/MixtureComp.cpp:2628-2763): derivatives per n_ij
+        const double* L = F.L;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            if (j < NP) {
+                const int    j1  = label[j];
+                const double xi  = xiC[j];
+                const double nuj = nu[j];
+                const double tmp = -xi * xi * CgTP;
+                const double xiP = tmp * (Zp[j] - Zj[j] / P);
+                double       xT = 0, xP = 0, xV = 0;
+#pragma unroll
+                for (int i = 0; i < NC; i++) {
+                    xT += x[j][i] * F.Tc[i];
+                    xP += x[j][i] * F.Pc[i];
+                    xV += x[j][i] * F.Vcvis[i];
+                }
+                const double u    = muA[j][3];
+                const double poly = L[1] + u * (2 * L[2] + u * (3 * L[3] + u * 4 * L[4]));
+                const double m4_3 = pow(muA[j][4], 3);
+                const double m4_4 = pow(muA[j][4], 4);
+                const double muP  = (4 * 1e-4) * m4_3 * (xV * xiP * poly) / muA[j][2];
+                const double sqMW = sqrt(MW[j]);
+                const double pT16 = pow(xT, 1.0 / 6), pT56 = pow(xT, -5.0 / 6), pP23 = pow(xP, 2.0 / 3);
+                double       val2[NC];
+#pragma unroll
+                for (int i = 0; i < NC; i++) val2[i] = gT[i] / (F.muAux1I[i] / sqMW);
+
+                out.rho[at(j1)]  = rhoC[j];
+                out.xi[at(j1)]   = xi;
+                out.mu[at(j1)]   = muC[j];
+                out.xiP[at(j1)]  = xiP;
+                out.rhoP[at(j1)] = xiP * MW[j];
+                out.muP[at(j1)]  = muP;
+                out.nj[at(j1)]   = njC[j];
+#pragma unroll
+                for (int k = 0; k < NC; k++) {
+                    const int    o     = j1 * NUMCOM + k;
+                    const double xix   = tmp * Zn[j][k];
+                    const double derxT = (F.Tc[k] - xT) / nuj;
+                    const double derxP = (F.Pc[k] - xP) / nuj;
+                    const double derMW = (F.MW[k] - MW[j]) / nuj;
+                    // der1 and der2 of the reference vanish: they carry the
+                    // factor -(1 / 2), an integer division
+                    double der3 = 0, der4 = F.sqrtMW[k];
+#pragma unroll
+                    for (int i = 0; i < NC; i++) {
+                        der3 += F.sqrtMW[i] * ((dlt(i, k) - x[j][i]) * val2[i] / nuj);
+                        der4 -= x[j][i] * F.sqrtMW[i];
+                    }
+                    der4 /= nuj;
+                    const double der6 = 5.4402 *
+                                        (1.0 / 6 * pT56 * derxT - pT16 * (0.5 / MW[j] * derMW + 2.0 / 3 / xP * derxP)) /
+                                        (sqMW * pP23);
+                    const double der7 = xix * xV + (F.Vcvis[k] - xV) * xi / nuj;
+                    const double der8 = der7 * poly;
+                    const double mux  = (der3 * muA[j][1] - muA[j][0] * der4) / (muA[j][1] * muA[j][1]) +
+                                       1e-4 * (4 * m4_3 * der8 * muA[j][2] - (m4_4 - 1) * der6) /
+                                           (muA[j][2] * muA[j][2]);
+                    out.xij[at(o)]  = x[j][k];
+                    out.xix[at(o)]  = xix;
+                    out.rhox[at(o)] = xix * MW[j] + xi / nuj * (F.MW[k] - MW[j]);
+                    out.mux[at(o)]  = mux;
+                }
+                const int ow     = j1 * NUMCOM + NC;
+                out.xij[at(ow)]  = 0.0;
+                out.xix[at(ow)]  = 0.0;
+                out.rhox[at(ow)] = 0.0;
+                out.mux[at(ow)]  = 0.0;
+            }
+        }
+        finish_fim(n_, stride, sk, out, exist, bw, xiW, xiPW, Nw, vf, vfP, S);
+    }
+
+    // The last outputs of the FIM copy-out (FlashFIM and FlashFIMn): the
+    // water phase, pSderExist / pVnumCom, the skip cache and the diagnostics.
+    __device__ void finish_fim(int64_t n_, int64_t stride, const ocpf_skip& sk, const ocpf_fim_out& out,
+                               const bool* exist, double bw, double xiW, double xiPW, double Nw, double vf,
+                               double vfP, const double* S)
+    {
+        const int64_t N = stride;
+        auto at = [N, n_](int f) { return (int64_t)f * N + n_; };
         // water phase
         out.rho[at(2)]  = F.std_rho_w / bw;
         out.xi[at(2)]   = xiW;
@@ -668,7 +1052,7 @@ struct FimCell : CellFlash<NC> {
             out.rhox[at(o)] = 0.0;
             out.mux[at(o)]  = 0.0;
         }
-        // pSderExist / pVnumCom, src/MixtureComp.cpp:559-570
+        // pSderExist / pVnumCom, src/MixtureComp.cpp:559-570 (FlashFIMn :681-692)
 #pragma unroll
         for (int j = 0; j < 2; j++) {
             out.pSderExist[at(j)] = exist[j] ? 1u : 0u;

@@ -221,6 +221,58 @@ __device__ __forceinline__ bool gauss_solve(double (&A)[N][N], double (&B)[N][M]
     return ok;
 }
 
+// gauss_solve for systems too large for registers: the same elimination
+// and pivot rule with rolled loops over arrays in local memory, rows
+// swapped in place.
+template <int N, int M>
+__device__ __noinline__ bool gauss_solve_mem(double (&A)[N][N], double (&B)[N][M])
+{
+    bool ok = true;
+#pragma unroll 1
+    for (int j = 0; j < N; j++) {
+        int    p  = j;
+        double mx = fabs(A[j][j]);
+        for (int i = j + 1; i < N; i++) {
+            const double v = fabs(A[i][j]);
+            if (v > mx) {
+                mx = v;
+                p  = i;
+            }
+        }
+        if (p != j) {
+            for (int c = j; c < N; c++) {
+                const double t = A[j][c];
+                A[j][c]        = A[p][c];
+                A[p][c]        = t;
+            }
+            for (int c = 0; c < M; c++) {
+                const double t = B[j][c];
+                B[j][c]        = B[p][c];
+                B[p][c]        = t;
+            }
+        }
+        if (A[j][j] == 0.0) ok = false;
+        const double r = 1.0 / A[j][j];
+#pragma unroll 1
+        for (int i = j + 1; i < N; i++) {
+            const double l = A[i][j] * r;
+            for (int c = j + 1; c < N; c++) A[i][c] -= l * A[j][c];
+#pragma unroll
+            for (int c = 0; c < M; c++) B[i][c] -= l * B[j][c];
+        }
+    }
+#pragma unroll 1
+    for (int j = N - 1; j >= 0; j--) {
+#pragma unroll
+        for (int c = 0; c < M; c++) {
+            double s = B[j][c];
+            for (int k = j + 1; k < N; k++) s -= A[j][k] * B[k][c];
+            B[j][c] = s / A[j][j];
+        }
+    }
+    return ok;
+}
+
 // Smallest eigenvalue of a symmetric matrix given in single precision (what
 // CalEigenSY / ssyevd returns first, src/DenseMat.cpp:14-26): cyclic Jacobi in
 // FP64 on the single-precision entries, rounded to single precision.

@@ -882,7 +882,7 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
 }
 
 // --------------------------------------------------------------- finalize
-template <int NC>
+template <int NC, bool FIMN = false>
 __device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
 {
     using F_ = SF<NC>;
@@ -914,7 +914,15 @@ __device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
             f.n[0][i] = S.D(F_::n0 + i, c);
             f.n[1][i] = S.D(F_::n1 + i, c);
         }
-        f.finalize(c, a.stride, a.sk, a.out, a.tail);
+        if (FIMN && f.NP == 2) {
+            // FlashFIMn's residual reads the fugacities of the split
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                f.phi[0][i] = S.D(F_::phi0 + i, c);
+                f.phi[1][i] = S.D(F_::phi1 + i, c);
+            }
+        }
+        f.template finalize<FIMN>(c, a.stride, a.sk, a.out, a.tail);
     }
 }
 

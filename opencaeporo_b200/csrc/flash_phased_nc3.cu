@@ -35,6 +35,7 @@ __global__ void __launch_bounds__(128) kp_learn_3(const __grid_constant__ FluidC
     learn_body<3>(F, a, *reinterpret_cast<LearnSmem*>(smem_raw));
 }
 K128 kp_finalize_3(const __grid_constant__ FluidConst F, const PhasedArgs a) { phased_finalize_body<3>(F, a); }
+K128 kp_finalize_fimn_3(const __grid_constant__ FluidConst F, const PhasedArgs a) { phased_finalize_body<3, true>(F, a); }
 #undef K128
 
 static int persistent_grid(const void* k, int sms)
@@ -106,7 +107,10 @@ cudaError_t launch_phased_nc3(const FluidConst& F, const PhasedArgs& a, cudaStre
     for (int r = 0; r < SPLIT_ROUNDS; r++)
         split_round_3(F, a, st, r, gp, g_sp, g_spnr);
     kp_slow_3<<<gp, 128, 0, st>>>(F, a);
-    kp_finalize_3<<<gcell, 128, 0, st>>>(F, a);
+    if (a.tail.mode & FM_FIMN)
+        kp_finalize_fimn_3<<<gcell, 128, 0, st>>>(F, a);
+    else
+        kp_finalize_3<<<gcell, 128, 0, st>>>(F, a);
     return cudaGetLastError();
 }
 

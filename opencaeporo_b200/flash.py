@@ -177,8 +177,33 @@ class MixtureCompBatch:
                                     FORMS[form], C.c_void_p(stream.cuda_stream))
         check(rc, "ocpf_flash_impec")
 
+    def _fimn_outputs(self, st: CellState):
+        torch = _torch()
+        o, dev = st.out, st.P.device
+        if "res" not in o:
+            o["res"] = torch.zeros((NPH * (self.nc + 2), st.ncell), dtype=torch.float64, device=dev)
+            o["resPc"] = torch.zeros(st.ncell, dtype=torch.float64, device=dev)
+        return o["res"].data_ptr(), o["resPc"].data_ptr()
+
+    def flash_fimn(self, st: CellState, form: str = "plain", stream=None, diagnostics: bool = True,
+                   fresh: bool = False):
+        """Batched FlashFIMn + IsoT_FIMn::PassFlashValue (``ocpf_flash_fimn``)
+        on device state, warm-started like ``flash_fim``: ``st.out`` receives
+        the FIMn outputs (dSec_dPri with the saturation and phase-mole rows,
+        the per-n_ij partials, nj) and ``st.out['res']`` / ``st.out['resPc']``
+        the residual terms (Bulk::res_n, Bulk::resPc)."""
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        fin, sk, fo = self._structs(st, optional=diagnostics, fresh=fresh)
+        fo.nj = st.out["nj"].data_ptr()
+        res, resPc = self._fimn_outputs(st)
+        rc = lib().ocpf_flash_fimn(self._h, st.ncell, C.byref(fin), C.byref(sk), C.byref(fo), res, resPc,
+                                   FORMS[form], C.c_void_p(stream.cuda_stream))
+        check(rc, "ocpf_flash_fimn")
+
     def init_flash(self, st: CellState, Vpore, S=None, impec: bool = False, form: str = "plain", stream=None,
-                   diagnostics: bool = True):
+                   diagnostics: bool = True, fimn: bool = False):
         """IsoT_FIM::InitFlash (``ocpf_init_flash_fim``) or, with ``impec``,
         IsoT_IMPEC::InitFlash (``ocpf_init_flash_impec``) on device state.
         On entry ``st.Ni`` holds the initial mole fractions z and
@@ -186,7 +211,9 @@ class MixtureCompBatch:
         saturations, of which S_w is read; ``Vpore`` [n] are the pore volumes
         in ft3. On return ``st.Ni`` holds the moles that fill the pore
         volume and ``st.out`` the FIM (or IMPEC, with ``vj``) outputs, as the
-        reference leaves Bulk::Ni and the Bulk arrays."""
+        reference leaves Bulk::Ni and the Bulk arrays. With ``fimn``,
+        IsoT_FIMn::InitFlash (``ocpf_init_flash_fimn``) with the outputs of
+        ``flash_fimn``."""
         torch = _torch()
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
@@ -207,6 +234,13 @@ class MixtureCompBatch:
             rc = lib().ocpf_init_flash_impec(h, st.ncell, C.byref(fin), C.byref(sk), st.Ni.data_ptr(),
                                              C.byref(_lib.ImpecOut(*vals)), FORMS[form], s)
             check(rc, "ocpf_init_flash_impec")
+        elif fimn:
+            vals = [o[k].data_ptr() if (diagnostics or k not in _lib.OPTIONAL_OUT or k == "nj") else None
+                    for k in _lib.OUT_FIELDS]
+            res, resPc = self._fimn_outputs(st)
+            rc = lib().ocpf_init_flash_fimn(h, st.ncell, C.byref(fin), C.byref(sk), st.Ni.data_ptr(),
+                                            C.byref(_lib.FimOut(*vals)), res, resPc, FORMS[form], s)
+            check(rc, "ocpf_init_flash_fimn")
         else:
             vals = [o[k].data_ptr() if (diagnostics or k not in _lib.OPTIONAL_OUT) else None
                     for k in _lib.OUT_FIELDS]

@@ -105,17 +105,20 @@ def dsec_err(g, o, rows, ncol, col_floor=1e-4):
 
 
 def check(gpu: dict, ref: dict, nc: int, noise: dict = None, fragile=None, tol: float = 1e-8,
-          factor: float = 10.0) -> dict:
+          factor: float = 10.0, errors=None, keys=None) -> dict:
     """Parity verdict. Returns {'ok': bool, 'np_mismatch': indices not
     excused by ``fragile``, 'worst': {field: (ratio, cell)}} where ratio =
-    error / allowed (<= 1 passes)."""
-    e = per_cell_errors(gpu, ref, nc)
+    error / allowed (<= 1 passes). ``errors`` / ``keys``: the per-cell error
+    function and its fields (default: the FIM outputs)."""
+    errors = per_cell_errors if errors is None else errors
+    keys = FLOAT_KEYS if keys is None else keys
+    e = errors(gpu, ref, nc)
     n = len(e["same"])
     frag = np.zeros(n, bool) if fragile is None else np.asarray(fragile, bool)
     bad_np = np.nonzero(~e["same"] & ~frag)[0]
     worst = {}
     ok = len(bad_np) == 0
-    for k in FLOAT_KEYS:
+    for k in keys:
         allowed = np.full(n, tol)
         if noise is not None and k in noise:
             allowed = np.maximum(allowed, factor * np.nan_to_num(np.asarray(noise[k]), nan=0.0))
@@ -267,19 +270,55 @@ def perturbed(P, T, X, trial, prng, eps=2.0 ** -50):
     return P, T, X
 
 
-def self_noise(run, P, T, X, base, nc, trials: int = NOISE_TRIALS, seed: int = 7):
+def self_noise(run, P, T, X, base, nc, trials: int = NOISE_TRIALS, seed: int = 7, errors=None, keys=None):
     """(noise, moved): per FIM output field and cell, the largest relative
     change of ``run(P, T, X)`` (the reference on perturbed inputs) against
     ``base`` over ``trials`` perturbations; and the cells whose phase count
-    moved."""
+    moved. ``errors`` / ``keys`` as in ``check``."""
+    errors = per_cell_errors if errors is None else errors
+    keys = FLOAT_KEYS if keys is None else keys
     prng = np.random.default_rng(seed)
     n = len(P)
-    noise = {k: np.zeros(n) for k in FLOAT_KEYS}
+    noise = {k: np.zeros(n) for k in keys}
     moved = np.zeros(n, bool)
     for t in range(trials):
         r = run(*perturbed(P, T, X, t, prng))
         moved |= np.asarray(r["phaseNum"]) != np.asarray(base["phaseNum"])
-        e = per_cell_errors(r, base, nc)
-        for k in FLOAT_KEYS:
+        e = errors(r, base, nc)
+        for k in keys:
             noise[k] = np.fmax(noise[k], np.nan_to_num(e[k], nan=0.0))
     return noise, moved
+
+
+# ----------------------------------------------------------------- FIMn flash
+FIMN_KEYS = FLOAT_KEYS + ("nj", "res", "resPc")
+
+
+def fimn_errors(gpu: dict, ref: dict, nc: int, col_floor: float = 1e-4) -> dict:
+    """per_cell_errors for the outputs of IsoT_FIMn::PassFlashValue, plus the
+    phase moles nj of the existing phases, the residual terms ``res`` (the
+    first bRowSizedSdP entries; each judged against max(|entry|, col_floor x
+    the cell's largest entry), like dSec_dPri's columns: they are one
+    column of the same dense solve) and ``resPc``."""
+    e = per_cell_errors(gpu, ref, nc)
+    n = len(e["same"])
+    exist = np.asarray(ref["phaseExist"]).astype(bool)
+    r = _rel(np.asarray(gpu["nj"], dtype=np.float64).reshape(n, -1), np.asarray(ref["nj"]).reshape(n, -1))
+    r[~exist] = 0.0
+    e["nj"] = np.where(e["same"], np.nan_to_num(r, nan=0.0).max(axis=1), np.nan)
+    g = np.asarray(gpu["res"], dtype=np.float64).reshape(n, -1)
+    o = np.asarray(ref["res"], dtype=np.float64).reshape(n, -1)
+    rows = np.asarray(ref["bRowSizedSdP"]).astype(np.int64)
+    m = np.arange(o.shape[1])[None, :] < rows[:, None]
+    oa = np.where(m & np.isfinite(o), np.abs(o), 0.0)
+    den = np.maximum(np.maximum(oa, col_floor * oa.max(axis=1, keepdims=True)), 1e-300)
+    rr = np.abs(g - o) / den
+    rr[~np.isfinite(o) & ~np.isfinite(g)] = 0.0
+    rr[~m] = 0.0
+    e["res"] = np.where(e["same"], rr.max(axis=1), np.nan)
+    gp = np.asarray(gpu["resPc"], dtype=np.float64).reshape(n)
+    op = np.asarray(ref["resPc"], dtype=np.float64).reshape(n)
+    rp = np.abs(gp - op) / np.maximum(np.abs(op), 1e-300)
+    rp[(gp == op) | (~np.isfinite(op) & ~np.isfinite(gp))] = 0.0
+    e["resPc"] = np.where(e["same"], rp, np.nan)
+    return e

@@ -271,3 +271,61 @@ def flash_fim(kind: str, fluid, P, T, Ni, S=None, lastNP=None, xij=None, skip=No
     out["seconds"] = secs.value
     out["skip"] = skip
     return out
+
+
+def flash_fimn(fluid, P, T, Ni, S=None, lastNP=None, xij=None, skip=None, nthreads: int = 0):
+    """Runs one FlashFIMn per cell through the compiled reference
+    (orc_flash_fimn_batch; the restatement has no FIMn entry). Arguments as
+    flash_fim; returns its outputs (FlashFIMn's dSec_dPri rows and per-n_ij
+    partials) plus ``res`` [n, 3 (numCom + 1)] (the first bRowSizedSdP
+    entries of each cell set, NaN beyond) and ``resPc`` [n]."""
+    lib = load("reference")
+    if not fluid.controls.use_skip:
+        fluid = fluid.with_controls(use_skip=True)  # see flash_fim
+        skip = None
+    n = int(np.asarray(P).shape[0])
+    res = np.full((n, NP * (fluid.nc + 2)), np.nan)
+    resPc = np.full(n, np.nan)
+    b, f, arrays, skip, _keep = _prepare(fluid, P, T, Ni, S, lastNP, xij, skip)
+    secs = C.c_double(0.0)
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    lib.orc_flash_fimn_batch.argtypes = [C.POINTER(OrcFluid), C.POINTER(OrcBatch), _dp, _dp, C.c_int,
+                                         C.POINTER(C.c_double)]
+    lib.orc_flash_fimn_batch.restype = C.c_int
+    rc = lib.orc_flash_fimn_batch(C.byref(f), C.byref(b), res.ctypes.data_as(_dp), resPc.ctypes.data_as(_dp),
+                                  int(nthreads), C.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"orc_flash_fimn_batch failed with {rc}")
+    arrays.update(res=res, resPc=resPc, seconds=secs.value, skip=skip)
+    return arrays
+
+
+def init_flash_fimn(fluid, P, T, z, S, Vpore, skip=None, nthreads: int = 0):
+    """Runs one InitFlashFIMn per cell through the compiled reference
+    (orc_init_flash_fimn_batch): inputs as init_flash, outputs as
+    flash_fimn plus ``Ni``."""
+    lib = load("reference")
+    if not fluid.controls.use_skip:
+        fluid = fluid.with_controls(use_skip=True)  # see flash_fim
+        skip = None
+    n = int(np.asarray(P).shape[0])
+    ncom = fluid.nc + 1
+    res = np.full((n, NP * (fluid.nc + 2)), np.nan)
+    resPc = np.full(n, np.nan)
+    Niout = np.full((n, ncom), np.nan)
+    Vp = np.ascontiguousarray(Vpore, dtype=np.float64).reshape(n)
+    b, f, arrays, skip, _keep = _prepare(fluid, P, T, z, S, None, None, skip)
+    secs = C.c_double(0.0)
+    if nthreads <= 0:
+        nthreads = os.cpu_count() or 1
+    lib.orc_init_flash_fimn_batch.argtypes = [C.POINTER(OrcFluid), C.POINTER(OrcBatch), _dp, _dp, _dp, _dp,
+                                              C.c_int, C.POINTER(C.c_double)]
+    lib.orc_init_flash_fimn_batch.restype = C.c_int
+    rc = lib.orc_init_flash_fimn_batch(C.byref(f), C.byref(b), Vp.ctypes.data_as(_dp), Niout.ctypes.data_as(_dp),
+                                       res.ctypes.data_as(_dp), resPc.ctypes.data_as(_dp), int(nthreads),
+                                       C.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"orc_init_flash_fimn_batch failed with {rc}")
+    arrays.update(res=res, resPc=resPc, Ni=Niout, seconds=secs.value, skip=skip)
+    return arrays

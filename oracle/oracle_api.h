@@ -131,6 +131,19 @@ int orc_flash_impec_batch(const orc_fluid* fluid, const orc_batch* batch, double
 int orc_init_flash_batch(const orc_fluid* fluid, const orc_batch* batch, const double* Vpore, int impec,
                          double* Ni, double* vj, int nthreads, double* seconds);
 
+/* Runs FlashFIMn over the batch (src/MixtureComp.cpp:575-695) with the
+ * copy-out of IsoT_FIMn::PassFlashValue (src/OCPFluidMethod.cpp:3179-3196):
+ * the orc_flash_fim_batch outputs (with FlashFIMn's dSec_dPri rows and
+ * per-n_ij partials) plus res [n*3*(numCom+1)] (the first bRowSizedSdP
+ * entries of each cell written) and resPc [n]. The reference oracle only. */
+int orc_flash_fimn_batch(const orc_fluid* fluid, const orc_batch* batch, double* res, double* resPc,
+                         int nthreads, double* seconds);
+
+/* Runs InitFlashFIMn over the batch (src/MixtureComp.cpp:355-442), inputs as
+ * orc_init_flash_batch, outputs as orc_flash_fimn_batch. */
+int orc_init_flash_fimn_batch(const orc_fluid* fluid, const orc_batch* batch, const double* Vpore, double* Ni,
+                              double* res, double* resPc, int nthreads, double* seconds);
+
 /* Saturation functions of one region, as the SWOF and SGOF keywords list
  * them (row-major, 4 columns): Sw, krw, krow, Pcow and Sg, krg, krog, Pcgo. */
 typedef struct {

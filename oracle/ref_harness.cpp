@@ -287,6 +287,61 @@ void run_chunk_init(const orc_fluid& f, const orc_batch& b, const double* Vpore,
         });
 }
 
+// Copy-out of IsoT_FIMn::PassFlashValue (src/OCPFluidMethod.cpp:3179-3196)
+// for cell n: the FIM copy-out, then the first bRowSizedSdP entries of the
+// flash's res into res [n * 3 * (numCom + 1)] and resPc.
+void copy_fimn(const MixtureComp& mc, const orc_batch& b, double* res, double* resPc, int numCom, int64_t n)
+{
+    copy_fim(mc, b, numCom, n);
+    const int                   len = b.bRowSizedSdP[n];
+    const std::vector<OCP_DBL>& r   = mc.GetRes();
+    std::copy(r.begin(), r.begin() + len, res + n * 3 * (numCom + 1));
+    resPc[n] = mc.GetResPc();
+}
+
+// FlashFIMn over cells [lo, hi): the calls of IsoT_FIMn::CalFlash
+// (src/OCPFluidMethod.cpp:3152-3177). The flash reads its njin and
+// phaseExistin arguments only to count input phases for a branch it never
+// takes (src/MixtureComp.cpp:586-592); they are passed as zeros and the
+// saturation-based flags.
+void run_chunk_fimn(const orc_fluid& f, const orc_batch& b, double* res, double* resPc, int64_t lo, int64_t hi,
+                    double* secs)
+{
+    const int           numCom = f.nc + 1, np = 3;
+    std::vector<double> Sin(np), xin(np * numCom), Nin(numCom), njin(np, 0.0);
+    std::vector<USI>    ex(np, 0);
+    run_cells(
+        f, b, lo, hi, secs,
+        [&](MixtureComp& mc, int64_t n, OCP_USI c) {
+            std::copy(b.S_in + n * np, b.S_in + (n + 1) * np, Sin.begin());
+            std::copy(b.xij_in + n * np * numCom, b.xij_in + (n + 1) * np * numCom, xin.begin());
+            std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, Nin.begin());
+            for (int j = 0; j < np; j++) ex[j] = (j == np - 1 || Sin[j] > 0) ? 1 : 0;
+            mc.FlashFIMn(b.P[n], b.T[n], Nin.data(), Sin.data(), xin.data(), njin.data(), ex.data(),
+                         static_cast<USI>(b.lastNP[n]), c);
+        },
+        [&](const MixtureComp& mc, int64_t n) { copy_fimn(mc, b, res, resPc, numCom, n); });
+}
+
+// InitFlashFIMn over cells [lo, hi): the calls of IsoT_FIMn::InitFlash
+// (src/OCPFluidMethod.cpp:3129-3150), inputs as run_chunk_init.
+void run_chunk_init_fimn(const orc_fluid& f, const orc_batch& b, const double* Vpore, double* Niout, double* res,
+                         double* resPc, int64_t lo, int64_t hi, double* secs)
+{
+    const int           numCom = f.nc + 1, np = 3;
+    std::vector<double> Sin(np), zin(numCom);
+    run_cells(
+        f, b, lo, hi, secs,
+        [&](MixtureComp& mc, int64_t n, OCP_USI c) {
+            std::copy(b.S_in + n * np, b.S_in + (n + 1) * np, Sin.begin());
+            std::copy(b.Ni + n * numCom, b.Ni + (n + 1) * numCom, zin.begin());
+            const OCP_DBL Pbb = 0;  // unused by MixtureComp
+            mc.InitFlashFIMn(b.P[n], Pbb, b.T[n], Sin.data(), Vpore[n], zin.data(), c);
+            for (int i = 0; i < numCom; i++) Niout[n * numCom + i] = mc.GetNi(i);
+        },
+        [&](const MixtureComp& mc, int64_t n) { copy_fimn(mc, b, res, resPc, numCom, n); });
+}
+
 // Runs `chunk(lo, hi, &secs)` over nthreads host threads with the
 // reference's console output muted; *seconds: the slowest thread's loop.
 template <class Chunk>
@@ -400,3 +455,22 @@ extern "C" void orc_daabpbc(int m, int n, int k, const double* A, const double* 
 }
 
 extern "C" const char* orc_kind(void) { return "reference"; }
+
+extern "C" int orc_flash_fimn_batch(const orc_fluid* fluid, const orc_batch* batch, double* res, double* resPc,
+                                    int nthreads, double* seconds)
+{
+    if (!fluid || !batch || !res || !resPc || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
+    return run_threads(batch->n, nthreads, seconds, [fluid, batch, res, resPc](int64_t lo, int64_t hi, double* s) {
+        run_chunk_fimn(*fluid, *batch, res, resPc, lo, hi, s);
+    });
+}
+
+extern "C" int orc_init_flash_fimn_batch(const orc_fluid* fluid, const orc_batch* batch, const double* Vpore,
+                                         double* Ni, double* res, double* resPc, int nthreads, double* seconds)
+{
+    if (!fluid || !batch || !Vpore || !Ni || !res || !resPc || fluid->nc < 2 || fluid->nc > ORC_MAX_NC) return 1;
+    return run_threads(batch->n, nthreads, seconds,
+                       [fluid, batch, Vpore, Ni, res, resPc](int64_t lo, int64_t hi, double* s) {
+                           run_chunk_init_fimn(*fluid, *batch, Vpore, Ni, res, resPc, lo, hi, s);
+                       });
+}

@@ -172,3 +172,68 @@ def run_gpu(fl, inp, form="plain", init=None):
     res = st.to_host()
     m.close()
     return res
+
+
+FIMN_CALLS = ("fresh", "warm", "init")
+
+
+def load_golden_fimn(name="fimn_nc6"):
+    """(fluid, {call: (inputs, reference outputs with their self-noise under
+    ``noise``, moved mask)}) of the FlashFIMn fixture, for the calls
+    'fresh' (FlashFIMn of new bulks), 'warm' (FlashFIMn from a last step's
+    state) and 'init' (InitFlashFIMn)."""
+    d = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    fl, _, _, _ = _fluid_only(d)
+    sk_keys = ("flag", "minEig", "P", "T", "z")
+    n1 = len(d["in1_P"])
+    calls = {
+        "fresh": ({"P": d["in1_P"], "T": d["in1_T"], "Ni": d["in1_Ni"], "S": np.zeros((n1, 3)),
+                   "lastNP": np.zeros(n1, np.int32), "xij": np.zeros((n1, 3, fl.nc + 1)),
+                   "skip": {k: np.zeros_like(d[f"skipin2_{k}"][:1].repeat(n1, axis=0)) for k in sk_keys}}, "1"),
+        "warm": ({"P": d["in2_P"], "T": d["in2_T"], "Ni": d["in2_Ni"], "S": d["in2_S"],
+                  "lastNP": d["in2_lastNP"].astype(np.int32), "xij": d["in2_xij"],
+                  "skip": {k: d[f"skipin2_{k}"] for k in sk_keys}}, "2"),
+        "init": ({"P": d["ini_P"], "T": d["ini_T"], "z": d["ini_z"], "S": d["ini_S"], "Vpore": d["ini_Vpore"]}, "i"),
+    }
+    out = {}
+    for call, (inp, t) in calls.items():
+        r = {k[len(t) + 4:]: d[k] for k in d.files if k.startswith(f"out{t}_")}
+        r["skip"] = {k: d[f"skipout{t}_{k}"] for k in sk_keys}
+        r["noise"] = {k[len(t) + 6:]: d[k].astype(np.float64) for k in d.files if k.startswith(f"noise{t}_")}
+        out[call] = (inp, r, d[f"fragile{t}"])
+    return fl, out
+
+
+def run_gpu_fimn(fl, call, inp, form="plain"):
+    """One FlashFIMn ('fresh', 'warm') or InitFlashFIMn ('init') of the
+    fixture's inputs through the C ABI on cuda:0; host outputs with res,
+    resPc (and Ni for 'init')."""
+    import torch
+    from opencaeporo_b200.flash import MixtureCompBatch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    m = MixtureCompBatch(fl)
+    n = len(inp["P"])
+    st = m.new_state(n)
+    if call == "init":
+        st.load(inp["P"], inp["T"], inp["z"])
+        m.init_flash(st, inp["Vpore"], S=inp["S"], form=form, fimn=True)
+    else:
+        st.load(inp["P"], inp["T"], inp["Ni"])
+        o = st.out
+        o["S"].copy_(torch.as_tensor(np.ascontiguousarray(inp["S"].T)))
+        o["phaseNum"].copy_(torch.as_tensor(inp["lastNP"].astype(np.int32)))
+        ncom = fl.nc + 1
+        o["xij"].copy_(torch.as_tensor(np.ascontiguousarray(inp["xij"].reshape(n, 3 * ncom).T)))
+        sk = inp["skip"]
+        st.skip["flag"].copy_(torch.as_tensor(sk["flag"].astype(np.int32)))
+        for k in ("minEig", "P", "T"):
+            st.skip[k].copy_(torch.as_tensor(np.asarray(sk[k], dtype=np.float64)))
+        st.skip["z"].copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(sk["z"]).T)))
+        m.flash_fimn(st, form=form)
+    torch.cuda.synchronize()
+    res = st.to_host()
+    if call == "init":
+        res["Ni"] = st.Ni.cpu().numpy().T.copy()
+    m.close()
+    return res

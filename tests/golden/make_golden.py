@@ -11,7 +11,7 @@ edge of an iteration cap or a stability threshold; any implementation whose
 rounding differs from the reference's may legitimately land on either side.
 
     python tests/golden/make_golden.py            # writes tests/golden/*.npz
-    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6, krpc)
+    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6, krpc, fimn_nc6)
 """
 from __future__ import annotations
 
@@ -289,6 +289,74 @@ def init_case():
           f"size={os.path.getsize(path) / 1e6:.2f} MB")
 
 
+FIMN_OUT_KEYS = OUT_KEYS + ("res", "resPc")
+
+
+def fimn_case():
+    """FlashFIMn and InitFlashFIMn (the FIM formulation with the phase moles
+    as secondary variables, IsoT_FIMn) on the 6-component fluid, on inputs
+    of the FIM fixtures (FlashFIMn's phase equilibrium is FlashFIM's): a
+    fresh step on near_nc6's near-envelope states, a warm step on warm_nc6's
+    warm-start state (skip hits, warm two-phase starts, relaxed stability)
+    and InitFlashFIMn of init_nc6's initial states. (States drawn afresh near
+    the envelope can hold one on which the reference's split restarts
+    without end.) The fixture holds each call's inputs, the reference's
+    outputs (res and resPc included), the cells whose phase count moved
+    under perturbation and the self-noise over oracle.compare.NOISE_TRIALS
+    perturbations (``perturbed``)."""
+    from oracle import compare as CMP
+    fl = synthetic_fluid(6, 1234)
+    kw = dict(errors=CMP.fimn_errors, keys=CMP.FIMN_KEYS)
+    g1 = np.load(os.path.join(HERE, "near_nc6.npz"))
+    P1, T1, N1 = g1["in_P"], g1["in_T"], g1["in_Ni"]
+
+    def step1(P, T, Ni):
+        return O.flash_fimn(fl, P, T, Ni, skip=O.new_skip(len(P), fl.nc), nthreads=8)
+
+    s1 = step1(P1, T1, N1)
+    noise1, moved1 = CMP.self_noise(step1, P1, T1, N1, s1, fl.nc, **kw)
+    g2 = np.load(os.path.join(HERE, "warm_nc6.npz"))
+    P2, T2, N2 = g2["in_P"], g2["in_T"], g2["in_Ni"]
+    S2, lastNP, xij = g2["in_S"], g2["in_lastNP"].astype(np.int32), g2["in_xij"]
+    skip2 = {k: g2[f"skipin_{k}"] for k in ("flag", "minEig", "P", "T", "z")}
+
+    def step2(P, T, Ni):
+        return O.flash_fimn(fl, P, T, Ni, S=S2, lastNP=lastNP, xij=xij,
+                            skip={k: v.copy() for k, v in skip2.items()}, nthreads=8)
+
+    s2 = step2(P2, T2, N2)
+    noise2, moved2 = CMP.self_noise(step2, P2, T2, N2, s2, fl.nc, **kw)
+    gi = np.load(os.path.join(HERE, "init_nc6.npz"))
+    Pi, Ti, zi, Si, Vp = gi["in_P"], gi["in_T"], gi["in_z"], gi["in_S"], gi["in_Vpore"]
+
+    def init(P, T, z):
+        return O.init_flash_fimn(fl, P, T, z, Si, Vp, skip=O.new_skip(len(P), fl.nc), nthreads=8)
+
+    si = init(Pi, Ti, zi)
+    noisei, movedi = CMP.self_noise(init, Pi, Ti, zi, si, fl.nc, **kw)
+    d = fluid_arrays(fl)
+    d["note"] = np.array("FlashFIMn fresh (near_nc6) and warm (warm_nc6) steps; InitFlashFIMn (init_nc6)")
+    d["in1_P"], d["in1_T"], d["in1_Ni"] = P1, T1, N1
+    d["in2_P"], d["in2_T"], d["in2_Ni"], d["in2_S"], d["in2_lastNP"], d["in2_xij"] = P2, T2, N2, S2, lastNP, xij
+    for k, v in skip2.items():
+        d[f"skipin2_{k}"] = v
+    d["ini_P"], d["ini_T"], d["ini_z"], d["ini_S"], d["ini_Vpore"] = Pi, Ti, zi, Si, Vp
+    for tag, r, noise, moved in (("1", s1, noise1, moved1), ("2", s2, noise2, moved2), ("i", si, noisei, movedi)):
+        for k in FIMN_OUT_KEYS:
+            d[f"out{tag}_{k}"] = r[k]
+        for k, v in r["skip"].items():
+            d[f"skipout{tag}_{k}"] = v
+        for k, v in noise.items():
+            d[f"noise{tag}_{k}"] = v.astype(np.float32)
+        d[f"fragile{tag}"] = moved
+    d["outi_Ni"] = si["Ni"]
+    path = os.path.join(HERE, "fimn_nc6.npz")
+    np.savez_compressed(path, **d)
+    print(f"fimn_nc6: two-phase step1={np.mean(s1['NPhc'] == 2):.3f} step2 ftype="
+          f"{np.bincount(s2['ftype'], minlength=3).tolist()} init two-phase={np.mean(si['NPhc'] == 2):.3f} "
+          f"fragile={moved1.sum()}/{moved2.sum()}/{movedi.sum()} size={os.path.getsize(path) / 1e6:.2f} MB")
+
+
 def krpc_case():
     """IsoT_FIM::CalKrPc with FlowUnit_ODGW01 on two saturation regions of
     synthetic tables (the second with a repeated saturation node), 4096
@@ -335,7 +403,7 @@ def main(only=()):
     if only:
         for name in only:
             {"restart_nc6": restart_case, "impec_nc6": impec_case, "init_nc6": init_case,
-             "krpc": krpc_case}[name]()
+             "krpc": krpc_case, "fimn_nc6": fimn_case}[name]()
         return
 
     # 1) SPE5 fluid (examples/spe5/EGOIL.in) at 160 degF, the deck's initial composition
@@ -396,6 +464,9 @@ def main(only=()):
 
     # 9) relative permeability and capillary pressure after the flash
     krpc_case()
+
+    # 10) the FIMn formulation's flash and initialisation
+    fimn_case()
 
 
 if __name__ == "__main__":
