@@ -284,6 +284,22 @@ int ocpf_init_flash_fim(ocpf_ctx* ctx, int64_t ncell, const ocpf_init_in* in, oc
 int ocpf_init_flash_impec(ocpf_ctx* ctx, int64_t ncell, const ocpf_init_in* in, ocpf_skip* skip, double* Ni,
                           ocpf_impec_out* out, int form, void* stream);
 
+/* The flash of a subset of the bulks: the calls of IsoT_AIMc::CalFlashI
+ * (src/OCPFluidMethod.cpp:4293-4314, FlashFIM + PassFlashValue on the
+ * implicit bulks) and CalFlashEa / CalFlashEp (:4257-4291, FlashIMPEC on
+ * the explicit bulks). in / skip / out are the full arrays of ncell cells
+ * (the layouts of ocpf_flash_fim / ocpf_flash_impec, stride ncell); idx
+ * [nsub] (device, distinct, in [0, ncell); others are skipped) lists the
+ * cells to flash. Only the listed cells are read and written; each gets
+ * exactly what the full call gives it. The listed cells are gathered into
+ * compact copies held by the context (about 2.4 KB per cell for 6
+ * components, grown on demand; a growth synchronises the device), flashed
+ * in the chosen form and scattered back. Asynchronous on `stream`. */
+int ocpf_flash_fim_subset(ocpf_ctx* ctx, int64_t nsub, const int64_t* idx, int64_t ncell, const ocpf_fim_in* in,
+                          ocpf_skip* skip, ocpf_fim_out* out, int form, void* stream);
+int ocpf_flash_impec_subset(ocpf_ctx* ctx, int64_t nsub, const int64_t* idx, int64_t ncell,
+                            const ocpf_impec_in* in, ocpf_skip* skip, ocpf_impec_out* out, int form, void* stream);
+
 /* Batched MixtureComp::FlashFIMn + IsoT_FIMn::PassFlashValue over ncell
  * cells (src/MixtureComp.cpp:575-695, src/OCPFluidMethod.cpp:3152-3196),
  * the flash of the FIM formulation whose secondary variables are the

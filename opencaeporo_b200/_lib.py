@@ -36,7 +36,7 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_mlp_param_count", "ocpf_mlp_forward", "ocpf_mlp_grad", "ocpf_mlp_adam",
            "ocpf_set_initializer", "ocpf_flash_fim_regions", "ocpf_measure_fp64_latency",
            "ocpf_flash_impec", "ocpf_init_flash_fim", "ocpf_init_flash_impec",
-           "ocpf_flash_fimn", "ocpf_init_flash_fimn",
+           "ocpf_flash_fimn", "ocpf_init_flash_fimn", "ocpf_flash_fim_subset", "ocpf_flash_impec_subset",
            "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count",
            "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian")
 
@@ -215,6 +215,12 @@ def lib():
     L.ocpf_init_flash_fimn.argtypes = [_vp, C.c_int64, C.POINTER(InitIn), C.POINTER(Skip), _vp, C.POINTER(FimOut),
                                        _vp, _vp, C.c_int, _vp]
     L.ocpf_init_flash_fimn.restype = C.c_int
+    L.ocpf_flash_fim_subset.argtypes = [_vp, C.c_int64, _vp, C.c_int64, C.POINTER(FimIn), C.POINTER(Skip),
+                                        C.POINTER(FimOut), C.c_int, _vp]
+    L.ocpf_flash_fim_subset.restype = C.c_int
+    L.ocpf_flash_impec_subset.argtypes = [_vp, C.c_int64, _vp, C.c_int64, C.POINTER(ImpecIn), C.POINTER(Skip),
+                                          C.POINTER(ImpecOut), C.c_int, _vp]
+    L.ocpf_flash_impec_subset.restype = C.c_int
     L.ocpf_conn_create.argtypes = [C.c_int64, C.c_int64, _vp, _vp, _vp, C.c_int, C.POINTER(_vp)]
     L.ocpf_conn_create.restype = C.c_int
     L.ocpf_conn_destroy.argtypes = [_vp]

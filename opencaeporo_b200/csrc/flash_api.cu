@@ -154,6 +154,9 @@ struct ocpf_ctx {
     bool            gvalid;
     int32_t         gkernels;      // kernel nodes of the captured graph
     int32_t         last_kernels;  // kernels the last call launched, -1 unknown
+    // subset calls: compact device copies of the listed cells, grown on demand
+    int64_t sub_cap;
+    void*   sub;
 };
 
 static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
@@ -195,6 +198,8 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->timed     = false;
     c->stage_cap = 0;
     c->stage     = nullptr;
+    c->sub_cap   = 0;
+    c->sub       = nullptr;
     for (auto& s : c->hs) s = nullptr;
     c->eq_cap    = 0;
     c->eq        = nullptr;
@@ -226,6 +231,7 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
     if (c->stage) cudaFree(c->stage);
+    if (c->sub) cudaFree(c->sub);
     if (c->eq) cudaFree(c->eq);
     if (c->mlp) cudaFree(c->mlp);
     if (c->rs) cudaStreamDestroy(c->rs);
@@ -897,6 +903,223 @@ extern "C" int ocpf_set_initializer(ocpf_ctx* c, const float* params, const floa
         c->fc.learn_on   = 1;
         c->gvalid        = false;  // the constants a captured graph holds changed
     }
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+// ------------------------------------------------------------ subsets
+
+namespace {
+
+// The arrays one gather or scatter moves: `rows` fields of `esz`-byte
+// elements between a full SoA array (stride ncell) and a compact one
+// (stride nsub), for the cells idx[0..nsub).
+constexpr int SUB_MAX = 48;
+struct SubTable {
+    int            n;
+    int64_t        nsub, ncell;
+    const int64_t* idx;
+    char*          full[SUB_MAX];
+    char*          comp[SUB_MAX];
+    int            rows[SUB_MAX];
+    int            esz[SUB_MAX];
+    // cpt: carved from the context's own copies, so writable even where the
+    // view that holds it is const
+    void add(const void* f, const void* cpt, int r, int e)
+    {
+        if (!f || !cpt || n >= SUB_MAX) return;
+        full[n] = (char*)f;
+        comp[n] = (char*)cpt;
+        rows[n] = r;
+        esz[n]  = e;
+        n++;
+    }
+};
+
+template <typename T>
+__device__ __forceinline__ void sub_move(char* full, char* comp, int64_t fo, int64_t co, bool gather)
+{
+    if (gather)
+        ((T*)comp)[co] = ((const T*)full)[fo];
+    else
+        ((T*)full)[fo] = ((const T*)comp)[co];
+}
+
+// blockIdx.y: the array; x: grid-stride over its rows x nsub elements.
+// Indices outside [0, ncell) are skipped.
+__global__ void k_subset_copy(const __grid_constant__ SubTable t, bool gather)
+{
+    const int     a     = blockIdx.y;
+    const int64_t total = (int64_t)t.rows[a] * t.nsub;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = e / t.nsub, cc = e - r * t.nsub;
+        const int64_t n = t.idx[cc];
+        if (n < 0 || n >= t.ncell) continue;
+        const int64_t fo = r * t.ncell + n, co = r * t.nsub + cc;
+        switch (t.esz[a]) {
+            case 8: sub_move<uint64_t>(t.full[a], t.comp[a], fo, co, gather); break;
+            case 4: sub_move<uint32_t>(t.full[a], t.comp[a], fo, co, gather); break;
+            case 2: sub_move<uint16_t>(t.full[a], t.comp[a], fo, co, gather); break;
+            default: sub_move<uint8_t>(t.full[a], t.comp[a], fo, co, gather); break;
+        }
+    }
+}
+
+cudaError_t subset_copy(const SubTable& t, bool gather, cudaStream_t st)
+{
+    if (t.n == 0 || t.nsub == 0) return cudaSuccess;
+    dim3 grid(148 * 4, t.n);
+    k_subset_copy<<<grid, 256, 0, st>>>(t, gather);
+    return cudaGetLastError();
+}
+
+// The output arrays of a FIM record as table entries, full -> compact.
+void add_outputs(SubTable& t, const Layout& L, const ocpf_fim_out& f, const ocpf_fim_out& cpt)
+{
+    const int nph = NPH, pc = NPH * L.ncom;
+    t.add(f.phaseNum, cpt.phaseNum, 1, 4);
+    t.add(f.phaseExist, cpt.phaseExist, nph, 4);
+    t.add(f.S, cpt.S, nph, 8);
+    t.add(f.Nt, cpt.Nt, 1, 8);
+    t.add(f.vf, cpt.vf, 1, 8);
+    t.add(f.vfP, cpt.vfP, 1, 8);
+    t.add(f.vfi, cpt.vfi, L.ncom, 8);
+    t.add(f.rho, cpt.rho, nph, 8);
+    t.add(f.xi, cpt.xi, nph, 8);
+    t.add(f.mu, cpt.mu, nph, 8);
+    t.add(f.rhoP, cpt.rhoP, nph, 8);
+    t.add(f.xiP, cpt.xiP, nph, 8);
+    t.add(f.muP, cpt.muP, nph, 8);
+    t.add(f.xij, cpt.xij, pc, 8);
+    t.add(f.rhox, cpt.rhox, pc, 8);
+    t.add(f.xix, cpt.xix, pc, 8);
+    t.add(f.mux, cpt.mux, pc, 8);
+    t.add(f.dSec_dPri, cpt.dSec_dPri, NPH * L.ncol * L.ncol, 8);
+    t.add(f.bRowSizedSdP, cpt.bRowSizedSdP, 1, 4);
+    t.add(f.pSderExist, cpt.pSderExist, nph, 4);
+    t.add(f.pVnumCom, cpt.pVnumCom, nph, 4);
+    t.add(f.nj, cpt.nj, nph, 8);
+    t.add(f.ePEC, cpt.ePEC, 1, 8);
+    t.add(f.ftype, cpt.ftype, 1, 1);
+    t.add(f.iters, cpt.iters, 5, 4);
+    t.add(f.status, cpt.status, 1, 2);
+}
+
+void add_skip(SubTable& t, const Layout& L, const ocpf_skip& f, const ocpf_skip& cpt)
+{
+    t.add(f.flag, cpt.flag, 1, 4);
+    t.add(f.minEig, cpt.minEig, 1, 8);
+    t.add(f.P, cpt.P, 1, 8);
+    t.add(f.T, cpt.T, 1, 8);
+    t.add(f.z, cpt.z, L.nc, 8);
+}
+
+// A compact pointer only where the caller passed the array.
+template <typename T>
+void keep_if(T*& cpt, const void* full)
+{
+    if (!full) cpt = nullptr;
+}
+
+// The flash of the cells idx[0..nsub) of full arrays of ncell cells: the
+// listed cells' inputs, outputs and skip cache are gathered into compact
+// copies (the outputs too, so that what the flash leaves untouched -- the
+// outputs of absent phases -- goes back unchanged), the chosen form runs on
+// the copies, and the outputs and the skip cache are scattered back.
+int flash_subset(ocpf_ctx* c, int64_t nsub, const int64_t* idx, int64_t ncell, const ocpf_fim_in& in,
+                 const ocpf_skip* sk, const ocpf_fim_out& out, double* vj, FlashTail tail, int form,
+                 cudaStream_t st)
+{
+    const Layout L{c->fc.nc, c->fc.nc + 1, c->fc.nc + 2};
+    const size_t body = stage_stride(L.bytes_per_cell(), nsub);
+    const size_t need = body + stage_stride((size_t)NPH * 8, nsub);
+    if (c->sub_cap < nsub || !c->sub) {
+        if (c->sub) {
+            cudaDeviceSynchronize();  // queued work may still read the old copies
+            cudaFree(c->sub);
+        }
+        c->sub     = nullptr;
+        c->sub_cap = 0;
+        c->gvalid  = false;
+        if (cudaMalloc(&c->sub, need) != cudaSuccess) return OCPF_ENOMEM;
+        c->sub_cap = nsub;
+    }
+    Views v = carve(c->sub, nsub, L, sk, &out);
+    keep_if(v.in.S, in.S);
+    keep_if(v.in.lastNP, in.lastNP);
+    keep_if(v.in.xij, in.xij);
+    ocpf_fim_out& o = v.out;
+    keep_if(o.rhoP, out.rhoP);
+    keep_if(o.xiP, out.xiP);
+    keep_if(o.muP, out.muP);
+    keep_if(o.rhox, out.rhox);
+    keep_if(o.xix, out.xix);
+    keep_if(o.mux, out.mux);
+    keep_if(o.dSec_dPri, out.dSec_dPri);
+    keep_if(o.bRowSizedSdP, out.bRowSizedSdP);
+    keep_if(o.pSderExist, out.pSderExist);
+    keep_if(o.pVnumCom, out.pVnumCom);
+    double* vjc = vj ? (double*)((char*)c->sub + body) : nullptr;
+    SubTable gin{}, gout{};
+    gin.nsub = gout.nsub = nsub;
+    gin.ncell = gout.ncell = ncell;
+    gin.idx = gout.idx = idx;
+    gin.add(in.P, v.in.P, 1, 8);
+    gin.add(in.T, v.in.T, 1, 8);
+    gin.add(in.Ni, v.in.Ni, L.ncom, 8);
+    gin.add(in.S, v.in.S, NPH, 8);
+    gin.add(in.lastNP, v.in.lastNP, 1, 4);
+    gin.add(in.xij, v.in.xij, NPH * L.ncom, 8);
+    add_outputs(gout, L, out, o);
+    if (sk) add_skip(gout, L, *sk, v.sk);
+    gout.add(vj, vjc, NPH, 8);
+    if (subset_copy(gin, true, st) != cudaSuccess || subset_copy(gout, true, st) != cudaSuccess) return OCPF_ECUDA;
+    tail.vj  = vjc;
+    int rc   = launch_form(c, form, nsub, nsub, v.in, v.sk, o, st, true, -1, tail);
+    c->timed = (rc == OCPF_OK);
+    if (rc == OCPF_OK && subset_copy(gout, false, st) != cudaSuccess) rc = OCPF_ECUDA;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int ocpf_flash_fim_subset(ocpf_ctx* c, int64_t nsub, const int64_t* idx, int64_t ncell,
+                                     const ocpf_fim_in* in, ocpf_skip* sk, ocpf_fim_out* out, int form,
+                                     void* stream)
+{
+    if (!c || nsub < 0 || ncell < 0 || nsub > ncell) return OCPF_EINVAL;
+    if (nsub == 0) return OCPF_OK;
+    if (!idx || !fim_args_ok(c, in, sk, out)) return OCPF_EINVAL;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    const int rc = flash_subset(c, nsub, idx, ncell, *in, sk, *out, nullptr,
+                                FlashTail{FM_FIM, nullptr, nullptr, nullptr}, form, (cudaStream_t)stream);
+    if (prev != c->device) cudaSetDevice(prev);
+    return rc;
+}
+
+extern "C" int ocpf_flash_impec_subset(ocpf_ctx* c, int64_t nsub, const int64_t* idx, int64_t ncell,
+                                       const ocpf_impec_in* in, ocpf_skip* sk, ocpf_impec_out* out, int form,
+                                       void* stream)
+{
+    if (!c || nsub < 0 || ncell < 0 || nsub > ncell) return OCPF_EINVAL;
+    if (nsub == 0) return OCPF_OK;
+    if (!idx || !in || form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (!in->P || !in->T || !in->Ni || !in->lastNP || !in->xij) return OCPF_EINVAL;
+    if (!impec_out_ok(out) || !skip_ok(c, sk)) return OCPF_EINVAL;
+    ocpf_fim_in fin{};
+    fin.P      = in->P;
+    fin.T      = in->T;
+    fin.Ni     = in->Ni;
+    fin.lastNP = in->lastNP;
+    fin.xij    = in->xij;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    if (prev != c->device) cudaSetDevice(c->device);
+    const int rc = flash_subset(c, nsub, idx, ncell, fin, sk, impec_as_fim(*out), out->vj,
+                                FlashTail{FM_IMPEC, nullptr, nullptr, nullptr}, form, (cudaStream_t)stream);
     if (prev != c->device) cudaSetDevice(prev);
     return rc;
 }

@@ -177,6 +177,36 @@ class MixtureCompBatch:
                                     FORMS[form], C.c_void_p(stream.cuda_stream))
         check(rc, "ocpf_flash_impec")
 
+    def flash_subset(self, st: CellState, idx, impec: bool = False, form: str = "plain", stream=None,
+                     diagnostics: bool = True):
+        """IsoT_AIMc's flashes of a subset of the bulks
+        (``ocpf_flash_fim_subset``, or with ``impec``
+        ``ocpf_flash_impec_subset``): only the cells listed in ``idx`` (a
+        tensor of distinct cell indices) of the full state ``st`` are read
+        and written, each as the full call would, warm-started from their own
+        outputs."""
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        idx = torch.as_tensor(idx).to(device=st.P.device, dtype=torch.int64).contiguous()
+        st.__dict__["_subset_idx"] = idx  # alive until the next call on this state
+        fin, sk, fo = self._structs(st, optional=diagnostics)
+        s = C.c_void_p(stream.cuda_stream)
+        if impec:
+            o = st.out
+            if "vj" not in o:
+                o["vj"] = torch.zeros((NPH, st.ncell), dtype=torch.float64, device=st.P.device)
+            fi = _lib.ImpecIn(st.P.data_ptr(), st.T.data_ptr(), st.Ni.data_ptr(), fin.lastNP, fin.xij)
+            vals = [o[k].data_ptr() if (diagnostics or k not in _lib.OPTIONAL_OUT) else None
+                    for k in _lib.IMPEC_OUT_FIELDS]
+            rc = lib().ocpf_flash_impec_subset(self._h, int(idx.numel()), idx.data_ptr(), st.ncell, C.byref(fi),
+                                               C.byref(sk), C.byref(_lib.ImpecOut(*vals)), FORMS[form], s)
+            check(rc, "ocpf_flash_impec_subset")
+        else:
+            rc = lib().ocpf_flash_fim_subset(self._h, int(idx.numel()), idx.data_ptr(), st.ncell, C.byref(fin),
+                                             C.byref(sk), C.byref(fo), FORMS[form], s)
+            check(rc, "ocpf_flash_fim_subset")
+
     def _fimn_outputs(self, st: CellState):
         torch = _torch()
         o, dev = st.out, st.P.device

@@ -367,3 +367,91 @@ def test_init_flash_then_fim_step_matches_reference():
     assert chk["ok"], CMP.check_summary(chk)
     same = b["phaseNum"] == nxt["phaseNum"]
     assert np.array_equal(b["ftype"][same], nxt["ftype"][same])
+
+
+def _state_from(fl, inp):
+    """A device state holding a fixture's warm-start inputs and skip cache."""
+    import torch
+    from opencaeporo_b200.flash import MixtureCompBatch
+    m = MixtureCompBatch(fl)
+    n = len(inp["P"])
+    st = m.new_state(n)
+    st.load(inp["P"], inp["T"], inp["Ni"])
+    o = st.out
+    if "S" in inp:
+        o["S"].copy_(torch.as_tensor(np.ascontiguousarray(inp["S"].T)))
+    o["phaseNum"].copy_(torch.as_tensor(inp["lastNP"].astype(np.int32)))
+    ncom = fl.nc + 1
+    o["xij"].copy_(torch.as_tensor(np.ascontiguousarray(inp["xij"].reshape(n, 3 * ncom).T)))
+    sk = inp["skip"]
+    st.skip["flag"].copy_(torch.as_tensor(sk["flag"].astype(np.int32)))
+    for k in ("minEig", "P", "T"):
+        st.skip[k].copy_(torch.as_tensor(np.asarray(sk[k], dtype=np.float64)))
+    st.skip["z"].copy_(torch.as_tensor(np.ascontiguousarray(np.asarray(sk["z"]).T)))
+    return m, st
+
+
+def _host_all(st):
+    h = st.to_host()
+    sk = h.pop("skip")
+    h.update({f"skip_{k}": v for k, v in sk.items()})
+    return h
+
+
+@pytest.mark.parametrize("impec", [False, True], ids=["fim", "impec"])
+@pytest.mark.parametrize("form", ["plain", "batched"])
+def test_subset_call_equals_full_call_on_its_cells(form, impec):
+    """ocpf_flash_fim_subset / ocpf_flash_impec_subset (IsoT_AIMc's flashes
+    of the implicit or explicit bulks): on a warm-started state, the listed
+    cells (every third, in shuffled order) get exactly the full call's
+    outputs and skip cache; every other cell keeps its state bit for bit."""
+    import torch
+    from conftest import load_golden_impec
+    if impec:
+        fl, inp, _, _ = load_golden_impec()
+    else:
+        fl, inp, _, _ = load_golden("warm_nc6")
+    n = len(inp["P"])
+    idx = np.random.default_rng(5).permutation(np.arange(0, n, 3))
+    m, full = _state_from(fl, inp)
+    if impec:
+        full.out["vj"] = torch.zeros((3, n), dtype=torch.float64, device="cuda")
+    before = _host_all(full)
+    if impec:
+        m.flash_impec(full, form=form)
+    else:
+        m.flash_fim(full, form=form)
+    torch.cuda.synchronize()
+    want = _host_all(full)
+    m.close()
+    m, sub = _state_from(fl, inp)
+    if impec:
+        sub.out["vj"] = torch.zeros((3, n), dtype=torch.float64, device="cuda")
+    m.flash_subset(sub, torch.as_tensor(idx), impec=impec, form=form)
+    torch.cuda.synchronize()
+    got = _host_all(sub)
+    m.close()
+    rest = np.setdiff1d(np.arange(n), idx)
+    for k, v in got.items():
+        a, w, b = np.asarray(v), np.asarray(want[k]), np.asarray(before[k])
+        f = a.dtype.kind == "f"
+        assert np.array_equal(a[idx], w[idx], equal_nan=f), k
+        assert np.array_equal(a[rest], b[rest], equal_nan=f), k
+
+
+def test_subset_rejects_bad_arguments():
+    import ctypes as C
+    import torch
+    from opencaeporo_b200 import _lib
+    from opencaeporo_b200.flash import MixtureCompBatch
+    fl, inp, _, _ = load_golden("uniform_nc6")
+    m = MixtureCompBatch(fl)
+    st = m.new_state(16)
+    fin, sk, fo = m._structs(st)
+    idx = torch.arange(4, dtype=torch.int64, device="cuda")
+    L = _lib.lib()
+    assert L.ocpf_flash_fim_subset(m._h, 4, None, 16, C.byref(fin), C.byref(sk), C.byref(fo), 0, None) != 0
+    assert L.ocpf_flash_fim_subset(m._h, 17, idx.data_ptr(), 16, C.byref(fin), C.byref(sk), C.byref(fo), 0,
+                                   None) != 0
+    assert L.ocpf_flash_fim_subset(m._h, 0, None, 16, C.byref(fin), C.byref(sk), C.byref(fo), 0, None) == 0
+    m.close()
