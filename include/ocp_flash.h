@@ -246,6 +246,10 @@ int ocpf_reserve(ocpf_ctx* ctx, int64_t ncell);
  * OCPF_NOALLOC_MAX_CELLS.
  * The first call on a device looks up the array's device address there
  * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * That address is kept for the life of the process: after cudaDeviceReset
+ * (or anything else that destroys the device's primary context) it is
+ * stale, and the next call would write to memory that no longer belongs to
+ * the library -- do not reset a device between calls of this function.
  * Every call on a device uses the same array and leaves its contents behind;
  * the call clears what must start empty itself. Calls whose work overlaps on
  * the GPU (two streams, or two host threads) race on the array and corrupt

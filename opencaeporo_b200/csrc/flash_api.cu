@@ -946,7 +946,10 @@ __device__ __forceinline__ void sub_move(char* full, char* comp, int64_t fo, int
 }
 
 // blockIdx.y: the array; x: grid-stride over its rows x nsub elements.
-// Indices outside [0, ncell) are skipped.
+// An index outside [0, ncell) names no cell: the gather fills its compact
+// slot with zeros (a flash of zero moles ends at once with a non-finite
+// status, instead of running on whatever the slot held before) and the
+// scatter leaves the full arrays alone.
 __global__ void k_subset_copy(const __grid_constant__ SubTable t, bool gather)
 {
     const int     a     = blockIdx.y;
@@ -954,8 +957,19 @@ __global__ void k_subset_copy(const __grid_constant__ SubTable t, bool gather)
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
         const int64_t r = e / t.nsub, cc = e - r * t.nsub;
         const int64_t n = t.idx[cc];
-        if (n < 0 || n >= t.ncell) continue;
-        const int64_t fo = r * t.ncell + n, co = r * t.nsub + cc;
+        const int64_t co = r * t.nsub + cc;
+        if (n < 0 || n >= t.ncell) {
+            if (gather) {
+                switch (t.esz[a]) {
+                    case 8: ((uint64_t*)t.comp[a])[co] = 0; break;
+                    case 4: ((uint32_t*)t.comp[a])[co] = 0; break;
+                    case 2: ((uint16_t*)t.comp[a])[co] = 0; break;
+                    default: ((uint8_t*)t.comp[a])[co] = 0; break;
+                }
+            }
+            continue;
+        }
+        const int64_t fo = r * t.ncell + n;
         switch (t.esz[a]) {
             case 8: sub_move<uint64_t>(t.full[a], t.comp[a], fo, co, gather); break;
             case 4: sub_move<uint32_t>(t.full[a], t.comp[a], fo, co, gather); break;
@@ -965,10 +979,15 @@ __global__ void k_subset_copy(const __grid_constant__ SubTable t, bool gather)
     }
 }
 
-cudaError_t subset_copy(const SubTable& t, bool gather, cudaStream_t st)
+cudaError_t subset_copy(const SubTable& t, bool gather, int device, cudaStream_t st)
 {
     if (t.n == 0 || t.nsub == 0) return cudaSuccess;
-    dim3 grid(148 * 4, t.n);
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0) sms = 1;
+    int64_t rows = 0;
+    for (int a = 0; a < t.n; a++) rows = rows > t.rows[a] ? rows : t.rows[a];
+    const int64_t want = (rows * t.nsub + 255) / 256;
+    dim3 grid((unsigned)(want < (int64_t)sms * 4 ? want : (int64_t)sms * 4), t.n);
     k_subset_copy<<<grid, 256, 0, st>>>(t, gather);
     return cudaGetLastError();
 }
@@ -1073,11 +1092,12 @@ int flash_subset(ocpf_ctx* c, int64_t nsub, const int64_t* idx, int64_t ncell, c
     add_outputs(gout, L, out, o);
     if (sk) add_skip(gout, L, *sk, v.sk);
     gout.add(vj, vjc, NPH, 8);
-    if (subset_copy(gin, true, st) != cudaSuccess || subset_copy(gout, true, st) != cudaSuccess) return OCPF_ECUDA;
+    if (subset_copy(gin, true, c->device, st) != cudaSuccess || subset_copy(gout, true, c->device, st) != cudaSuccess)
+        return OCPF_ECUDA;
     tail.vj  = vjc;
     int rc   = launch_form(c, form, nsub, nsub, v.in, v.sk, o, st, true, -1, tail);
     c->timed = (rc == OCPF_OK);
-    if (rc == OCPF_OK && subset_copy(gout, false, st) != cudaSuccess) rc = OCPF_ECUDA;
+    if (rc == OCPF_OK && subset_copy(gout, false, c->device, st) != cudaSuccess) rc = OCPF_ECUDA;
     return rc;
 }
 

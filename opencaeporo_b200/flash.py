@@ -178,17 +178,30 @@ class MixtureCompBatch:
         check(rc, "ocpf_flash_impec")
 
     def flash_subset(self, st: CellState, idx, impec: bool = False, form: str = "plain", stream=None,
-                     diagnostics: bool = True):
+                     diagnostics: bool = True, check_indices: bool = False):
         """IsoT_AIMc's flashes of a subset of the bulks
         (``ocpf_flash_fim_subset``, or with ``impec``
         ``ocpf_flash_impec_subset``): only the cells listed in ``idx`` (a
         tensor of distinct cell indices) of the full state ``st`` are read
         and written, each as the full call would, warm-started from their own
-        outputs."""
+        outputs. An index outside [0, ncell) is skipped; a repeated index
+        makes two slots scatter to one cell in no fixed order.
+        ``check_indices`` raises ValueError on either before the call (one
+        device synchronisation)."""
         torch = _torch()
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
-        idx = torch.as_tensor(idx).to(device=st.P.device, dtype=torch.int64).contiguous()
+        # the index copy is ordered on the call's stream, and the allocator
+        # keeps its memory until the work queued there has read it
+        with torch.cuda.stream(stream):
+            idx = torch.as_tensor(idx).to(device=st.P.device, dtype=torch.int64).contiguous()
+        idx.record_stream(stream)
+        if check_indices and idx.numel():
+            lo, hi = int(idx.min().item()), int(idx.max().item())
+            if lo < 0 or hi >= st.ncell:
+                raise ValueError(f"flash_subset: index outside [0, {st.ncell})")
+            if int(torch.unique(idx).numel()) != int(idx.numel()):
+                raise ValueError("flash_subset: repeated index")
         st.__dict__["_subset_idx"] = idx  # alive until the next call on this state
         fin, sk, fo = self._structs(st, optional=diagnostics)
         s = C.c_void_p(stream.cuda_stream)

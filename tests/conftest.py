@@ -12,7 +12,7 @@ if ROOT not in sys.path:
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 GOLDEN_CASES = ("spe5", "uniform_nc6", "warm_nc6", "uniform_nc3", "uniform_nc9", "uniform_nc12",
-                "near_nc6", "restart_nc6")
+                "near_nc6", "restart_nc6", "config1_nc6")
 
 
 def pytest_configure(config):

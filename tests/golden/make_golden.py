@@ -11,7 +11,8 @@ edge of an iteration cap or a stability threshold; any implementation whose
 rounding differs from the reference's may legitimately land on either side.
 
     python tests/golden/make_golden.py            # writes tests/golden/*.npz
-    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6, krpc, fimn_nc6)
+    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6, krpc, fimn_nc6,
+                                                   # config1_nc6)
 """
 from __future__ import annotations
 
@@ -397,13 +398,53 @@ def krpc_case():
     print(f"krpc: n={n} size={os.path.getsize(path) / 1e6:.2f} MB")
 
 
+def config1_case():
+    """The CPU-runnable configuration in full: the 6-component fluid and 4096
+    independent fresh states, P ~ U(5, 40) MPa, T ~ U(340, 400) K,
+    z ~ Dirichlet(1), N_tot ~ U(1e3, 1e4) (synth.uniform_states, seed 1234;
+    uniform_nc6 keeps 512 of the same states). Fragile mask and self-noise
+    over oracle.compare.NOISE_TRIALS perturbations (``perturbed``)."""
+    from oracle import compare as CMP
+    fl = synthetic_fluid(6, 1234)
+    inp = synth.uniform_states(fl, 4096, 1234)
+    n = len(inp["P"])
+    skip_in = O.new_skip(n, fl.nc)
+    skip_run = {k: v.copy() for k, v in skip_in.items()}
+    r = O.flash_fim("reference", fl, inp["P"], inp["T"], inp["Ni"], skip=skip_run, nthreads=8)
+
+    def run(P, T, Ni):
+        return O.flash_fim("reference", fl, P, T, Ni, nthreads=8)
+
+    noise, moved = CMP.self_noise(run, inp["P"], inp["T"], inp["Ni"], r, fl.nc)
+    d = fluid_arrays(fl)
+    d["note"] = np.array("config 1: synthetic nc=6 seed 1234, 4096 uniform_states seed 1234, fresh cells")
+    d["index"] = np.arange(n)
+    d["in_P"], d["in_T"], d["in_Ni"] = inp["P"], inp["T"], inp["Ni"]
+    d["in_S"] = np.zeros((n, 3))
+    d["in_lastNP"] = np.zeros(n, np.int32)
+    d["in_xij"] = np.zeros((n, 3, fl.nc + 1))
+    for k, v in skip_in.items():
+        d[f"skipin_{k}"] = v
+    for k, v in skip_run.items():
+        d[f"skipout_{k}"] = v
+    for k in OUT_KEYS:
+        d[f"out_{k}"] = r[k]
+    d["fragile"] = moved
+    for k, v in noise.items():
+        d[f"noise_{k}"] = v.astype(np.float32)
+    path = os.path.join(HERE, "config1_nc6.npz")
+    np.savez_compressed(path, **d)
+    print(f"config1_nc6: n={n} two-phase={np.mean(r['NPhc'] == 2):.3f} fragile={moved.sum()} "
+          f"size={os.path.getsize(path) / 1e6:.2f} MB")
+
+
 def main(only=()):
     if not O.available("reference"):
         raise SystemExit("oracle/_ref/libocpref.so missing: run `make -C oracle ref` first")
     if only:
         for name in only:
             {"restart_nc6": restart_case, "impec_nc6": impec_case, "init_nc6": init_case,
-             "krpc": krpc_case, "fimn_nc6": fimn_case}[name]()
+             "krpc": krpc_case, "fimn_nc6": fimn_case, "config1_nc6": config1_case}[name]()
         return
 
     # 1) SPE5 fluid (examples/spe5/EGOIL.in) at 160 degF, the deck's initial composition
@@ -467,6 +508,9 @@ def main(only=()):
 
     # 10) the FIMn formulation's flash and initialisation
     fimn_case()
+
+    # 11) the CPU-runnable configuration in full (4096 fresh states)
+    config1_case()
 
 
 if __name__ == "__main__":

@@ -455,3 +455,36 @@ def test_subset_rejects_bad_arguments():
                                    None) != 0
     assert L.ocpf_flash_fim_subset(m._h, 0, None, 16, C.byref(fin), C.byref(sk), C.byref(fo), 0, None) == 0
     m.close()
+
+
+def test_subset_skips_indices_outside_the_arrays():
+    """An index outside [0, ncell) in a subset call names no cell: the other
+    listed cells get the full call's outputs, no cell outside the list
+    changes, and the Python mirror's optional check rejects such a list (and
+    a repeated index) before calling."""
+    import torch
+    fl, inp, _, _ = load_golden("warm_nc6")
+    n = len(inp["P"])
+    good = np.arange(1, n, 5)
+    m, full = _state_from(fl, inp)
+    before = _host_all(full)
+    m.flash_fim(full, form="batched")
+    torch.cuda.synchronize()
+    want = _host_all(full)
+    m.close()
+    m, sub = _state_from(fl, inp)
+    idx = np.concatenate([good[:7], [-3, n, n + 100], good[7:]])
+    m.flash_subset(sub, torch.as_tensor(idx), form="batched")
+    torch.cuda.synchronize()
+    got = _host_all(sub)
+    with pytest.raises(ValueError):
+        m.flash_subset(sub, torch.as_tensor(idx), form="batched", check_indices=True)
+    with pytest.raises(ValueError):
+        m.flash_subset(sub, torch.as_tensor(np.array([0, 2, 2])), form="batched", check_indices=True)
+    m.close()
+    rest = np.setdiff1d(np.arange(n), good)
+    for k, v in got.items():
+        a, w, b = np.asarray(v), np.asarray(want[k]), np.asarray(before[k])
+        f = a.dtype.kind == "f"
+        assert np.array_equal(a[good], w[good], equal_nan=f), k
+        assert np.array_equal(a[rest], b[rest], equal_nan=f), k

@@ -8,11 +8,12 @@ import os
 import numpy as np
 import pytest
 
+from oracle import REF_ROOT
 from oracle import krpc as K
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 GOLDEN = os.path.join(HERE, "golden", "krpc.npz")
-REF_SRC = "/root/reference/src/FlowUnit.cpp"
+REF_SRC = os.path.join(REF_ROOT, "src", "FlowUnit.cpp")
 KEYS = ("kr", "Pc", "Pj", "dKr_dS", "dPcj_dS")
 
 

@@ -153,7 +153,7 @@ def _clean_equilibrium(res, nc):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["uniform_nc6", "near_nc6", "warm_nc6", "restart_nc6"])
+@pytest.mark.parametrize("case", ["uniform_nc6", "near_nc6", "warm_nc6", "restart_nc6", "config1_nc6"])
 def test_fast_matches_reference_goldens(case):
     """Fast form (mixed + trained initialiser) against the reference. Where
     the reference converged (ePEC <= 1e-9: its answer is an equilibrium),
@@ -255,3 +255,19 @@ def test_initialiser_gain_over_mixed():
     assert it_f[0] < 0.95 * it_m[0], (it_m, it_f)
     assert it_f[1] < it_m[1], (it_m, it_f)
     assert work_f < 0.98 * work_m, (work_m, work_f)
+
+
+@pytest.mark.gpu
+def test_fast_form_config1_at_the_plain_bar():
+    """The CPU-runnable configuration in full (4096 fresh states) in the fast
+    form, held to the bar of the FP64 forms on every cell: identical phase
+    counts except where the reference itself flips under 1-ulp input
+    perturbations, every output within 1e-8 relative or 10x the reference's
+    own 1-ulp sensitivity -- no exception for cells whose reference split
+    did not converge."""
+    from conftest import load_golden, run_gpu
+    from oracle import compare as CMP
+    fl, inp, ref, fragile = load_golden("config1_nc6")
+    got = run_gpu(fl, inp, form="fast", init=_model())
+    chk = CMP.check(got, ref, fl.nc, noise=ref["noise"], fragile=fragile)
+    assert chk["ok"], CMP.check_summary(chk)

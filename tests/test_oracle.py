@@ -8,9 +8,10 @@ import pytest
 
 from conftest import GOLDEN_CASES, load_golden
 from oracle import compare as CMP
+from oracle import REF_ROOT
 from oracle import oracle as O
 
-REF_SRC = "/root/reference/src/MixtureComp.cpp"
+REF_SRC = os.path.join(REF_ROOT, "src", "MixtureComp.cpp")
 
 
 def _run(kind, fl, inp):
