@@ -396,10 +396,11 @@ def cpu_baseline(fl, w, forms):
         errs[name] = (e, worst)
     conv = (r["NPhc"] == 1) | (r["ePEC"] <= 1e-9)
     # cells that need the reference's own sensitivity: every phase-count
-    # mismatch and every converged cell above 1e-8, in any form
-    need = np.zeros(ns, bool)
+    # mismatch, every cell whose split did not converge and every converged
+    # cell above 1e-8, in any form
+    need = ~conv
     for e, worst in errs.values():
-        need |= ~e["same"] | (e["same"] & conv & (worst > 1e-8))
+        need = need | ~e["same"] | (e["same"] & conv & (worst > 1e-8))
     cand = np.nonzero(need)[0]
     noise = {k: np.zeros(ns) for k in CMP.FLOAT_KEYS}
     moved = np.zeros(ns, bool)
