@@ -54,15 +54,18 @@ __device__ __forceinline__ double div_const(double x, double d, double rd)
 // Scientific Computing on Itanium-based Systems, Intel Press 2002, ch. 8).
 // Operands whose magnitudes lie outside [2^-500, 2^501) -- zeros,
 // non-finite values and extremes where the estimate, the quotient or the
-// remainder could leave the normal range -- take the ordinary division.
+// remainder could leave the normal range -- take the ordinary division, in
+// one out-of-line copy (ddiv_wide) so that each use adds only the short
+// sequence to the kernel's code.
 // Bit-identical to a / b: checked on the device against '/' over 10^9
 // operand pairs per run (ocpf_selfcheck_division), including divisors and
 // dividends next to powers of two and quotients next to one.
+static __device__ __noinline__ double ddiv_wide(double a, double b) { return a / b; }
 __device__ __forceinline__ double ddiv(double a, double b)
 {
     const unsigned ea = ((unsigned)__double2hiint(a) >> 20) & 0x7ffu;
     const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
-    if (ea - 523u > 1000u || eb - 523u > 1000u) return a / b;
+    if (ea - 523u > 1000u || eb - 523u > 1000u) return ddiv_wide(a, b);
     double y;
     asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
     const double e  = fma(-b, y, 1.0);

@@ -75,10 +75,17 @@ def saturation_pressure(phase_count, T, Ni, p_lo_mpa=0.5, p_hi_mpa=80.0, steps=4
 
 
 def near_envelope_states(fluid: Fluid, n: int, seed: int, phase_count, t_k=(340.0, 400.0),
-                         alpha: float = 1.0, band=(0.95, 1.05), max_rounds: int = 20, steps: int = 40):
+                         alpha: float = 1.0, band=(0.95, 1.05), max_rounds: int = 20, steps: int = 40,
+                         record=None, replay=None):
     """n states with P within ``band`` of the seeded state's saturation
     pressure. Candidates that have no upper saturation pressure in range are
-    redrawn (deterministically, from the same generator stream)."""
+    redrawn (deterministically, from the same generator stream).
+
+    ``record``: a list that receives, per round, the accepted candidates'
+    indices and saturation pressures; ``replay``: such a list, used instead
+    of ``phase_count`` to rebuild the same states bit for bit without a
+    flash (the bisection's outcome is the only part of a state that depends
+    on a flash; everything else comes from the seeded generators)."""
     rng = np.random.default_rng(seed)
     nc = fluid.nc
     outT, outNi, outP = [], [], []
@@ -87,11 +94,19 @@ def near_envelope_states(fluid: Fluid, n: int, seed: int, phase_count, t_k=(340.
     while have < n and rounds < max_rounds:
         m = max(2 * (n - have), 64)
         cand = uniform_states(fluid, m, int(rng.integers(1 << 62)), t_k=t_k, alpha=alpha)
-        psat, ok = saturation_pressure(phase_count, cand["T"], cand["Ni"], steps=steps)
-        idx = np.nonzero(ok)[0][: n - have]
+        if replay is not None:
+            idx, psat = replay[rounds]
+            idx = np.asarray(idx, np.int64)
+            psat = np.asarray(psat, np.float64)
+        else:
+            psat, ok = saturation_pressure(phase_count, cand["T"], cand["Ni"], steps=steps)
+            idx = np.nonzero(ok)[0][: n - have]
+            psat = psat[idx]
+            if record is not None:
+                record.append((idx.astype(np.uint32), psat))
         outT.append(cand["T"][idx])
         outNi.append(cand["Ni"][idx])
-        outP.append(psat[idx] * rng.uniform(band[0], band[1], size=len(idx)))
+        outP.append(psat * rng.uniform(band[0], band[1], size=len(idx)))
         have += len(idx)
         rounds += 1
     if have < n:
@@ -100,16 +115,18 @@ def near_envelope_states(fluid: Fluid, n: int, seed: int, phase_count, t_k=(340.
             "Ni": np.concatenate(outNi)[:n].reshape(n, nc + 1)}
 
 
-def mixed_states(fluid: Fluid, n: int, seed: int, phase_count, near_frac: float = 0.3, steps: int = 40):
+def mixed_states(fluid: Fluid, n: int, seed: int, phase_count, near_frac: float = 0.3, steps: int = 40,
+                 record=None, replay=None):
     """Uniform states with ``near_frac`` of them replaced by near-envelope
-    states at seeded positions."""
+    states at seeded positions (``record`` / ``replay``: see
+    ``near_envelope_states``)."""
     base = uniform_states(fluid, n, seed)
     m = int(round(near_frac * n))
     if m == 0:
         return base
     rng = np.random.default_rng(seed + 1)
     pos = np.sort(rng.choice(n, size=m, replace=False))
-    near = near_envelope_states(fluid, m, seed + 2, phase_count, steps=steps)
+    near = near_envelope_states(fluid, m, seed + 2, phase_count, steps=steps, record=record, replay=replay)
     for k in ("P", "T", "Ni"):
         base[k][pos] = near[k]
     base["near_mask"] = np.zeros(n, bool)

@@ -183,12 +183,24 @@ def test_batched_equals_plain(case):
     ends on a convergence threshold may move by a few steps (the total
     modelled work stays within 1 %), outputs agree to 1e-9 or 10x the
     reference's own 1-ulp sensitivity."""
-    from opencaeporo_b200 import roofline
+    from opencaeporo_b200 import _lib, roofline
     fl, inp, ref, _ = load_golden(case)
     a = _run_gpu(fl, inp, form="plain")
     b = _run_gpu(fl, inp, form="batched")
-    for k in ("phaseNum", "status", "ftype"):
+    for k in ("phaseNum", "ftype"):
         np.testing.assert_array_equal(a[k], b[k], err_msg=k)
+    # status: the outcome bits agree everywhere; the bits that record an
+    # intermediate event (an iteration that hit its cap or stopped short of
+    # its tolerance, a singular dense solve on the way) agree wherever the
+    # iteration counts do -- rounding moves such an event only together with
+    # the counts of the iteration it ends
+    event = (_lib.CELL_SSMSTA_CAP | _lib.CELL_NRSTA_FAIL | _lib.CELL_SSMSP_FAIL | _lib.CELL_NRSP_FAIL |
+             _lib.CELL_SINGULAR)
+    np.testing.assert_array_equal(a["status"] & ~event, b["status"] & ~event, err_msg="status")
+    same_it = np.all(a["iters"] == b["iters"], axis=1)
+    diff = np.nonzero(same_it & (a["status"] != b["status"]))[0]
+    assert len(diff) == 0, [(int(c), int(a["status"][c]), int(b["status"][c]), a["iters"][c].tolist())
+                            for c in diff[:8]]
     wa = roofline.flops(fl.nc, a["iters"], a["phaseNum"] - 1)
     wb = roofline.flops(fl.nc, b["iters"], b["phaseNum"] - 1)
     assert abs(wb / wa - 1) < 0.01, (wa, wb)
