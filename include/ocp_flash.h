@@ -418,17 +418,6 @@ int ocpf_set_initializer(ocpf_ctx* ctx, const float* params, const float* in_mea
  * reference counterpart (measurement utility). */
 int ocpf_measure_fp64_latency(int device, double* cycles);
 
-/* Checks the library's FP64 division (the correctly rounded rcp.approx +
- * Newton-Raphson + remainder-correction sequence the flash kernels use in
- * place of the division routine) against the device's '/' on about `pairs`
- * seeded random operand pairs: exponents in [-20, 20] and [-500, 500],
- * divisors and dividends next to powers of two, quotients next to one, and
- * operands outside the sequence's range (zeros, extremes, infinities).
- * *mismatches = pairs whose results differ in any bit (NaN against NaN
- * excepted); *cycles (may be null) = its dependent-chain latency on one
- * thread. No reference counterpart (self-check utility). */
-int ocpf_selfcheck_division(int device, int64_t pairs, uint64_t seed, int64_t* mismatches, double* cycles);
-
 /* ---------------------------------------------------------------------
  * Relative permeability and capillary pressure after the flash
  * (IsoT_FIM::CalKrPc / IsoT_IMPEC::CalKrPc, src/OCPFluidMethod.cpp:

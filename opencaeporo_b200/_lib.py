@@ -38,8 +38,7 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_flash_impec", "ocpf_init_flash_fim", "ocpf_init_flash_impec",
            "ocpf_flash_fimn", "ocpf_init_flash_fimn", "ocpf_flash_fim_subset", "ocpf_flash_impec_subset",
            "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count",
-           "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian",
-           "ocpf_selfcheck_division")
+           "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian")
 
 _vp = C.c_void_p
 
@@ -201,9 +200,6 @@ def lib():
     L.ocpf_flash_fim_regions.restype = C.c_int
     L.ocpf_measure_fp64_latency.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.ocpf_measure_fp64_latency.restype = C.c_int
-    L.ocpf_selfcheck_division.argtypes = [C.c_int, C.c_int64, C.c_uint64, C.POINTER(C.c_int64),
-                                          C.POINTER(C.c_double)]
-    L.ocpf_selfcheck_division.restype = C.c_int
     L.ocpf_flash_impec.argtypes = [_vp, C.c_int64, C.POINTER(ImpecIn), C.POINTER(Skip), C.POINTER(ImpecOut),
                                    C.c_int, _vp]
     L.ocpf_flash_impec.restype = C.c_int
@@ -283,17 +279,6 @@ def fp64_latency_cycles(device: int = 0) -> dict:
     v = (C.c_double * 6)()
     check(lib().ocpf_measure_fp64_latency(int(device), v), "ocpf_measure_fp64_latency")
     return dict(zip(("div", "div_x12_each", "fma", "exp", "log", "acos_cos"), list(v)))
-
-
-def selfcheck_division(pairs: int, seed: int = 1, device: int = 0) -> tuple:
-    """(mismatches, cycles): the library's FP64 division against the
-    device's '/' on about ``pairs`` seeded operand pairs, and its
-    dependent-chain latency on one thread."""
-    n = C.c_int64(-1)
-    cyc = C.c_double(0)
-    check(lib().ocpf_selfcheck_division(int(device), int(pairs), int(seed), C.byref(n), C.byref(cyc)),
-          "ocpf_selfcheck_division")
-    return int(n.value), float(cyc.value)
 
 
 def fma_peak_tflops(device: int = 0, bits: int = 64) -> float:

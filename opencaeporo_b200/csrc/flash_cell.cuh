@@ -51,7 +51,7 @@ __device__ __forceinline__ double fug_piece(int q, double zj, double aj, double 
 {
     const double num = q == 0 ? zj - bj : (q == 1 ? fma(D1, bj, zj) : 1.0);
     const double den = q == 0 ? 1.0 : (q == 1 ? fma(D2, bj, zj) : (q == 2 ? bj : aj));
-    const double d   = ddiv(num, den);
+    const double d   = num / den;
     return q <= 1 ? log(d) : d;
 }
 
@@ -160,9 +160,9 @@ struct CellFlash {
     {
         const double k0 = Kw0[i];
         if (k == 0) return k0;
-        if (k == 1) return drcp(k0);
+        if (k == 1) return 1 / k0;
         if (k == 2) return pow(k0, 1.0 / 3);
-        return pow(drcp(k0), 1.0 / 3);
+        return pow(1 / k0, 1.0 / 3);
     }
 
     // ---------------- stability ------------------------------------------
@@ -201,32 +201,32 @@ struct CellFlash {
                 Zx[i] = dz(Ax[i], Bi[i]);
             }
             const double zmb  = zj - bj;
-            const double G    = ddiv(zj + D1 * bj, zj + D2 * bj);
+            const double G    = (zj + D1 * bj) / (zj + D2 * bj);
             const double lnG  = log(G);
-            const double ib   = drcp(bj);
+            const double ib   = 1.0 / bj;
             const double zd2  = zj + D2 * bj;
-            const double gfac = ddiv(ddiv(D1MD2, zd2), zd2);
+            const double gfac = D1MD2 / zd2 / zd2;
             double       fx[NC][NC];
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                const double E = ddiv(-aj, D1MD2 * bj) * (ddiv(Ax[i], aj) - Bi[i] * ib);
+                const double E = -aj / (D1MD2 * bj) * (Ax[i] / aj - Bi[i] * ib);
 #pragma unroll
                 for (int k = 0; k < NC; k++) {
                     const double a_ik = omb(i, k) * sA[i] * sA[k];
                     // 1/C * Cxk with C = Y_i P / (z - b)
-                    const double cterm = ddiv(zmb * dlt(i, k) - Y[i] * (Zx[k] - Bi[k]), Y[i] * zmb);
+                    const double cterm = (zmb * dlt(i, k) - Y[i] * (Zx[k] - Bi[k])) / (Y[i] * zmb);
                     const double Dxk   = Bi[i] * ib * (Zx[k] - Bi[k] * (zj - 1) * ib);
                     double       Exk   = (2 * (aj * ib * Bi[k] * Bi[i] + bj * a_ik) - Ax[i] * Bi[k] -
                                   Ax[k] * Bi[i]) *
                                  (ib * ib);
                     Exk /= -D1MD2;
                     const double Gxk = gfac * (zj * Bi[k] - Zx[k] * bj);
-                    fx[i][k]         = cterm + Dxk + Exk * lnG + ddiv(E, G) * Gxk;
+                    fx[i][k]         = cterm + Dxk + Exk * lnG + E / G * Gxk;
                 }
             }
             // AssembleJmatSTA: J[i][j] = (fx[i][j] - sum_k Y_k fx[i][k] + 1) / Yt;
             // symmetric matrix from J's lower triangle.
-            const double iYt = drcp(Yt_);
+            const double iYt = 1.0 / Yt_;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
                 double s = 0;
@@ -255,7 +255,7 @@ struct CellFlash {
             ys += Y[i];
         }
         Yt_            = ys;
-        const double r = drcp(Yt_);
+        const double r = 1 / Yt_;
 #pragma unroll
         for (int i = 0; i < NC; i++) Y[i] *= r;
     }
@@ -266,7 +266,7 @@ struct CellFlash {
     {
         double res[NC];
 #pragma unroll
-        for (int i = 0; i < NC; i++) res[i] = log(ddiv(fugId[i], fugSta[i] * Yt));
+        for (int i = 0; i < NC; i++) res[i] = log(fugId[i] / (fugSta[i] * Yt));
         double Se = 0;
 #pragma unroll
         for (int i = 0; i < NC; i++) Se += res[i] * res[i];
@@ -278,7 +278,7 @@ struct CellFlash {
             Se = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                res[i] = log(ddiv(fugId[i], fugSta[i] * Yt));
+                res[i] = log(fugId[i] / (fugSta[i] * Yt));
                 Se += res[i] * res[i];
             }
             Se = sqrt(Se);
@@ -316,31 +316,31 @@ struct CellFlash {
             Yt = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                Y[i] = ddiv(x[0][i], kw(k, i));
+                Y[i] = x[0][i] / kw(k, i);
                 Yt += Y[i];
             }
-            double r = drcp(Yt);
+            double r = 1 / Yt;
 #pragma unroll
             for (int i = 0; i < NC; i++) Y[i] *= r;
             fug_phi(Y, phiSta, fugSta, Asta, Bsta, Zsta);
             Se = 0;
 #pragma unroll
-            for (int i = 0; i < NC; i++) Se += sq(log(ddiv(fugSta[i], fugId[i]) * Yt));
+            for (int i = 0; i < NC; i++) Se += sq(log(fugSta[i] / fugId[i] * Yt));
             int iter = 0;
             while (Se > F.ssmsta_tol2) {
                 Yt = 0;
 #pragma unroll
                 for (int i = 0; i < NC; i++) {
-                    Y[i] = ddiv(di[i], phiSta[i]);
+                    Y[i] = di[i] / phiSta[i];
                     Yt += Y[i];
                 }
-                r = drcp(Yt);
+                r = 1 / Yt;
 #pragma unroll
                 for (int i = 0; i < NC; i++) Y[i] *= r;
                 fug_phi(Y, phiSta, fugSta, Asta, Bsta, Zsta);
                 Se = 0;
 #pragma unroll
-                for (int i = 0; i < NC; i++) Se += sq(log(ddiv(fugSta[i], fugId[i]) * Yt));
+                for (int i = 0; i < NC; i++) Se += sq(log(fugSta[i] / fugId[i] * Yt));
                 iter++;
                 if (iter > F.ssmsta_maxit) {
                     status |= ST_SSMSTA_CAP;
@@ -387,7 +387,7 @@ struct CellFlash {
                     Y[i] = x[0][i] * ks[i];
                     Yt += Y[i];
                 }
-                const double r = drcp(Yt);
+                const double r = 1 / Yt;
 #pragma unroll
                 for (int i = 0; i < NC; i++) Y[i] *= r;
                 if (iter > 0) {
@@ -405,7 +405,7 @@ struct CellFlash {
                 Sk = 0;
 #pragma unroll
                 for (int i = 0; i < NC; i++) {
-                    di[i] = ddiv(fugId[i], fugSta[i] * Yt);
+                    di[i] = fugId[i] / (fugSta[i] * Yt);
                     ks[i] *= di[i];
                     Se += sq(di[i] - 1);
                     Sk += sq(log(ks[i]));
@@ -469,8 +469,8 @@ struct CellFlash {
             if (Ks[i] < Kmin) Kmin = Ks[i];
             if (Ks[i] > Kmax) Kmax = Ks[i];
         }
-        const double numin = drcp(1 - Kmax);
-        const double numax = drcp(1 - Kmin);
+        const double numin = 1 / (1 - Kmax);
+        const double numax = 1 / (1 - Kmin);
         double       v     = 0.5 * (numin + numax);
         int          iter  = 0;
         while (true) {
@@ -479,11 +479,11 @@ struct CellFlash {
             for (int i = 0; i < NC; i++) {
                 const double km1 = Ks[i] - 1;
                 const double tmp = 1 + v * km1;
-                rj += ddiv(zi[i] * km1, tmp);
-                J -= ddiv(zi[i] * km1 * km1, tmp * tmp);
+                rj += zi[i] * km1 / tmp;
+                J -= zi[i] * km1 * km1 / (tmp * tmp);
             }
             if (fabs(rj) < F.rr_tol || iter > F.rr_maxit) break;
-            const double dnuj  = ddiv(-rj, J);
+            const double dnuj  = -rj / J;
             const double tmpnu = v + dnuj;
             if (tmpnu < numax && tmpnu > numin)
                 v = tmpnu;
@@ -522,15 +522,15 @@ struct CellFlash {
 #pragma unroll
             for (int i = 0; i < NC; i++) {
                 const double tmp = 1 + nu[0] * (Ks[i] - 1);
-                x[1][i]          = ddiv(zi[i], tmp);
+                x[1][i]          = zi[i] / tmp;
                 x[0][i]          = Ks[i] * x[1][i];
             }
             fug_phi_all();
             Se = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                Se = __dadd_rn(Se, sq(ddiv(fug[1][i], fug[0][i]) - 1));  // never fused: the warp form adds rounded squares
-                Ks[i] = ddiv(phi[1][i], phi[0][i]);
+                Se = __dadd_rn(Se, sq(fug[1][i] / fug[0][i] - 1));  // never fused: the warp form adds rounded squares
+                Ks[i] = phi[1][i] / phi[0][i];
             }
             iter++;
             if (iter > maxIt) {
@@ -564,7 +564,7 @@ struct CellFlash {
             }
         }
         const DzCoef dz(aj, bj, zj);
-        const double inu = drcp(nuj);
+        const double inu = 1.0 / nuj;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             An[i]  = 2 * inu * (t[i] - aj);
@@ -572,26 +572,26 @@ struct CellFlash {
             Znj[i] = dz(An[i], Bn[i]);
         }
         const double zmb  = zj - bj;
-        const double G    = ddiv(zj + D1 * bj, zj + D2 * bj);
+        const double G    = (zj + D1 * bj) / (zj + D2 * bj);
         const double lnG  = log(G);
-        const double ib   = drcp(bj);
+        const double ib   = 1.0 / bj;
         const double zd2  = zj + D2 * bj;
-        const double gfac = ddiv(D1MD2, zd2 * zd2);
+        const double gfac = D1MD2 / (zd2 * zd2);
         const double efac = -1 / D1MD2 * (ib * ib);
 #pragma unroll
         for (int i = 0; i < NC; i++) {
-            const double E   = ddiv(-aj, D1MD2 * bj) * (ddiv(2 * t[i], aj) - Bi[i] * ib);
-            const double iC  = ddiv(zmb, xj[i] * P);
+            const double E   = -aj / (D1MD2 * bj) * (2 * t[i] / aj - Bi[i] * ib);
+            const double iC  = zmb / (xj[i] * P);
 #pragma unroll
             for (int k = 0; k <= i; k++) {
                 const double a_ik = omb(i, k) * sA[i] * sA[k];
-                const double Cnk  = ddiv(ddiv(P, zmb), zmb) * (zmb * inu * (dlt(i, k) - xj[i]) - xj[i] * (Znj[k] - Bn[k]));
+                const double Cnk  = P / zmb / zmb * (zmb * inu * (dlt(i, k) - xj[i]) - xj[i] * (Znj[k] - Bn[k]));
                 const double Dnk  = Bi[i] * ib * (Znj[k] - (Bi[k] - bj) * (zj - 1) * inu * ib);
                 const double Gnk  = gfac * (Bn[k] * zj - Znj[k] * bj);
                 double       Enk  = efac * (2 * (bj * a_ik * inu + Bn[k] * (Bi[i] * aj * ib - t[i])) -
                                    An[k] * Bi[i] - aj * Bi[i] * inu);
                 Enk -= E * inu;
-                const double v = iC * Cnk + Dnk + Enk * lnG + ddiv(E, G) * Gnk;
+                const double v = iC * Cnk + Dnk + Enk * lnG + E / G * Gnk;
                 if (accumulate) {
                     S[i][k] += v;
                     if (k != i) S[k][i] += v;
@@ -638,7 +638,7 @@ struct CellFlash {
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             const double tmp = n[0][i] + alpha * res[i];
-            if (tmp < 0) alpha *= 0.9 * fabs(ddiv(n[0][i], res[i]));
+            if (tmp < 0) alpha *= 0.9 * fabs(n[0][i] / res[i]);
         }
         double s0 = 0, s1 = 0;
 #pragma unroll
@@ -652,8 +652,8 @@ struct CellFlash {
         nu[1] = s1;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
-            x[0][i] = fabs(ddiv(n[0][i], nu[0]));
-            x[1][i] = fabs(ddiv(n[1][i], nu[1]));
+            x[0][i] = fabs(n[0][i] / nu[0]);
+            x[1][i] = fabs(n[1][i] / nu[1]);
         }
         double e0 = 0, e1 = 0;
 #pragma unroll
@@ -676,7 +676,7 @@ struct CellFlash {
         double eNR = 0;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
-            res[i] = log(ddiv(fug[1][i], fug[0][i]));
+            res[i] = log(fug[1][i] / fug[0][i]);
             eNR += res[i] * res[i];
         }
         eNR               = sqrt(eNR);
@@ -688,7 +688,7 @@ struct CellFlash {
             eNR = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                res[i] = log(ddiv(fug[1][i], fug[0][i]));
+                res[i] = log(fug[1][i] / fug[0][i]);
                 eNR += res[i] * res[i];
             }
             eNR = sqrt(eNR);

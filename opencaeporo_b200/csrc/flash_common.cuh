@@ -42,45 +42,6 @@ __device__ __forceinline__ double div_const(double x, double d, double rd)
     const double r = fma(-d, q, x);
     return fma(r, rd, q);
 }
-// a / b, correctly rounded, as a short branch-free sequence in place of the
-// division routine (which costs ~114 cycles of latency on the B200, against
-// ~60 here): a reciprocal estimate y0 = rcp.approx.ftz.f64(b) (relative
-// error below 2^-19), e = 1 - b y0 exact in one fused multiply-add, the
-// reciprocal and the quotient q0 = a y0 each refined by the factors (1 + e)
-// and (1 + e^2) (Newton-Raphson on 1/b, carried on both together: relative
-// error ~e^4 ~ 2^-76 plus a few roundings), and a final remainder
-// correction RN(q + (a - b q) y) (Markstein's theorem: P. Markstein, IBM J.
-// Res. Develop. 34(1), 1990; M. Cornea, J. Harrison, P. T. P. Tang,
-// Scientific Computing on Itanium-based Systems, Intel Press 2002, ch. 8).
-// Operands whose magnitudes lie outside [2^-500, 2^501) -- zeros,
-// non-finite values and extremes where the estimate, the quotient or the
-// remainder could leave the normal range -- take the ordinary division, in
-// one out-of-line copy (ddiv_wide) so that each use adds only the short
-// sequence to the kernel's code.
-// Bit-identical to a / b: checked on the device against '/' over 10^9
-// operand pairs per run (ocpf_selfcheck_division), including divisors and
-// dividends next to powers of two and quotients next to one.
-static __device__ __noinline__ double ddiv_wide(double a, double b) { return a / b; }
-__device__ __forceinline__ double ddiv(double a, double b)
-{
-    const unsigned ea = ((unsigned)__double2hiint(a) >> 20) & 0x7ffu;
-    const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
-    if (ea - 523u > 1000u || eb - 523u > 1000u) return ddiv_wide(a, b);
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
-    const double e  = fma(-b, y, 1.0);
-    const double q  = a * y;
-    const double e2 = e * e;
-    const double y1 = fma(y, e, y);
-    const double q1 = fma(q, e, q);
-    const double y2 = fma(y1, e2, y1);
-    const double q2 = fma(q1, e2, q1);
-    const double r  = fma(-b, q2, a);
-    return fma(r, y2, q2);
-}
-// 1 / b, correctly rounded (ddiv with a = 1)
-__device__ __forceinline__ double drcp(double b) { return ddiv(1.0, b); }
-
 constexpr double RCP3     = 1.0 / 3;
 constexpr double RCP9     = 1.0 / 9;
 constexpr double RCP54    = 1.0 / 54;

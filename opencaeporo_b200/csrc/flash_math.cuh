@@ -17,7 +17,7 @@ __device__ __forceinline__ double nt_polish(double root, double a, double b, dou
     int    iter    = 0;
     while (fabs(e) > 1e-8) {
         const double df = root * (3 * root + 2 * a) + b;
-        root            = root - ddiv(e, df);
+        root            = root - e / df;
         iter++;
         if (iter > 10) break;
         e = root * (root * (root + a) + b) + c;
@@ -81,7 +81,7 @@ __device__ __forceinline__ double gibbs_piece(int k, double zmin, double zmax, d
 {
     const double num = k == 0 ? zmin - bj : (k == 1 ? fma(D1, bj, zmin) * fma(D2, bj, zmax) : aj);
     const double den = k == 0 ? zmax - bj : (k == 1 ? fma(D2, bj, zmin) * fma(D1, bj, zmax) : bj * (D2 - D1));
-    const double d   = ddiv(num, den);
+    const double d   = num / den;
     return k <= 1 ? log(d) : d;
 }
 __device__ __forceinline__ double pick_root_from(double zmin, double zmax, double g1, double g2, double k)
@@ -105,7 +105,7 @@ __device__ __forceinline__ double sol_eos(double aj, double bj)
 {
     const PrCubic cu(aj, bj);
     if (cu.M <= 0) {
-        const double theta = acos(ddiv(cu.R, sqrt(cu.Q3)));
+        const double theta = acos(cu.R / sqrt(cu.Q3));
         const double z0    = cu.trig_root(0, theta);
         const double z1    = cu.trig_root(1, theta);
         const double z2    = cu.trig_root(2, theta);
@@ -124,7 +124,7 @@ __device__ __forceinline__ double sol_eos_group(double aj, double bj, unsigned m
 {
     const PrCubic cu(aj, bj);
     if (cu.M <= 0) {
-        const double theta = acos(ddiv(cu.R, sqrt(cu.Q3)));
+        const double theta = acos(cu.R / sqrt(cu.Q3));
         const double zk    = cu.trig_root(rank < 3 ? rank : 0, theta);
         const double z0    = __shfl_sync(mask, zk, base);
         const double z1    = __shfl_sync(mask, zk, base + 1);
@@ -151,8 +151,8 @@ struct DzCoef {
         bmz   = bj - zj;
         num_b = (aj + D1TD2 * (3 * bj * bj + 2 * bj)) +
                 (D1PD2 * (2 * bj + 1) - 2 * D1TD2 * bj) * zj - (D1PD2 - 1) * zj * zj;
-        inv_den = drcp(3 * zj * zj + 2 * ((D1PD2 - 1) * bj - 1) * zj +
-                       (aj + D1TD2 * bj * bj - D1PD2 * bj * (bj + 1)));
+        inv_den = 1.0 / (3 * zj * zj + 2 * ((D1PD2 - 1) * bj - 1) * zj +
+                         (aj + D1TD2 * bj * bj - D1PD2 * bj * (bj + 1)));
     }
     __device__ __forceinline__ double operator()(double dA, double dB) const
     {
@@ -198,7 +198,7 @@ __device__ __forceinline__ bool gauss_solve(double (&A)[N][N], double (&B)[N][M]
             }
         }
         if (A[j][j] == 0.0) ok = false;
-        const double r = drcp(A[j][j]);
+        const double r = 1.0 / A[j][j];
 #pragma unroll
         for (int i = j + 1; i < N; i++) {
             const double l = A[i][j] * r;
@@ -215,7 +215,7 @@ __device__ __forceinline__ bool gauss_solve(double (&A)[N][N], double (&B)[N][M]
             double s = B[j][c];
 #pragma unroll
             for (int k = j + 1; k < N; k++) s -= A[j][k] * B[k][c];
-            B[j][c] = ddiv(s, A[j][j]);
+            B[j][c] = s / A[j][j];
         }
     }
     return ok;
@@ -252,7 +252,7 @@ __device__ __noinline__ bool gauss_solve_mem(double (&A)[N][N], double (&B)[N][M
             }
         }
         if (A[j][j] == 0.0) ok = false;
-        const double r = drcp(A[j][j]);
+        const double r = 1.0 / A[j][j];
 #pragma unroll 1
         for (int i = j + 1; i < N; i++) {
             const double l = A[i][j] * r;
@@ -267,7 +267,7 @@ __device__ __noinline__ bool gauss_solve_mem(double (&A)[N][N], double (&B)[N][M
         for (int c = 0; c < M; c++) {
             double s = B[j][c];
             for (int k = j + 1; k < N; k++) s -= A[j][k] * B[k][c];
-            B[j][c] = ddiv(s, A[j][j]);
+            B[j][c] = s / A[j][j];
         }
     }
     return ok;

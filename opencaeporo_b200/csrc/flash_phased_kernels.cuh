@@ -80,10 +80,10 @@ __device__ void sta_prep_body(const FluidConst& F, const PhasedArgs& a, int k)
         double Yt = 0, Y[NC];
 #pragma unroll
         for (int i = 0; i < NC; i++) {
-            Y[i] = ddiv(f.zi[i], f.kw(k, i));
+            Y[i] = f.zi[i] / f.kw(k, i);
             Yt += Y[i];
         }
-        const double r = drcp(Yt);
+        const double r = 1 / Yt;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             S.D(F_::Y + i, c)  = Y[i] * r;
@@ -137,7 +137,7 @@ __device__ void sta_ssm_body(const FluidConst& F, const PhasedArgs& a, int list)
             fug_phi<NC>(F, sA, Bi, P, Y, phi, nullptr, aj, bj, zj);
             double Se = 0;
 #pragma unroll
-            for (int i = 0; i < NC; i++) Se += sq(log(ddiv(phi[i] * Y[i] * P, di[i] * P) * Yt));
+            for (int i = 0; i < NC; i++) Se += sq(log((phi[i] * Y[i] * P) / (di[i] * P) * Yt));
             bool done;
             if (first) {
                 first = false;
@@ -165,10 +165,10 @@ __device__ void sta_ssm_body(const FluidConst& F, const PhasedArgs& a, int list)
                 Yt = 0;
 #pragma unroll
                 for (int i = 0; i < NC; i++) {
-                    Y[i] = ddiv(di[i], phi[i]);
+                    Y[i] = di[i] / phi[i];
                     Yt += Y[i];
                 }
-                const double r = drcp(Yt);
+                const double r = 1 / Yt;
 #pragma unroll
                 for (int i = 0; i < NC; i++) Y[i] *= r;
             }
@@ -247,7 +247,7 @@ __device__ void sta_verdict_body(const FluidConst& F, const PhasedArgs& a, int k
         for (int i = 0; i < NC; i++) {
             const double fz = S.D(F_::di + i, c) * P;
             const double fs = S.D(F_::phiS + i, c) * S.D(F_::Y + i, c) * P;
-            Se += sq(log(ddiv(fz, fs * f.Yt)));
+            Se += sq(log(fz / (fs * f.Yt)));
         }
         if (from32) S.D(F_::SeSSM, c) = Se;
         Se = sqrt(Se);
@@ -284,7 +284,7 @@ __device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k, int
             fugId[i]  = S.D(F_::di + i, c) * f.P;
             Y[i]      = S.D(F_::Y + i, c);
             fugSta[i] = S.D(F_::phiS + i, c) * Y[i] * f.P;
-            res[i]    = log(ddiv(fugId[i], fugSta[i] * f.Yt));
+            res[i]    = log(fugId[i] / (fugSta[i] * f.Yt));
         }
         Asta = S.D(F_::Asta, c), Bsta = S.D(F_::Bsta, c), Zsta = S.D(F_::Zsta, c);
         Se   = 0;
@@ -324,7 +324,7 @@ __device__ void sta_nr_body(const FluidConst& F, const PhasedArgs& a, int k, int
             Se = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                res[i] = log(ddiv(fugId[i], fugSta[i] * f.Yt));
+                res[i] = log(fugId[i] / (fugSta[i] * f.Yt));
                 Se += res[i] * res[i];
             }
             Se = sqrt(Se);
@@ -402,7 +402,7 @@ __device__ void s01_ssm_body(const FluidConst& F, const PhasedArgs& a, int k)
                 Y[i] = z[i] * ks[i];
                 Yt += Y[i];
             }
-            const double r = drcp(Yt);
+            const double r = 1 / Yt;
 #pragma unroll
             for (int i = 0; i < NC; i++) Y[i] *= r;
             bool conv = false;
@@ -424,7 +424,7 @@ __device__ void s01_ssm_body(const FluidConst& F, const PhasedArgs& a, int k)
             Sk = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                const double d = ddiv(fid[i], fs[i] * Yt);
+                const double d = fid[i] / (fs[i] * Yt);
                 ks[i] *= d;
                 Se += sq(d - 1);
                 Sk += sq(log(ks[i]));
@@ -580,7 +580,7 @@ __device__ void sp_ssm_body(const FluidConst& F, const PhasedArgs& a, int r)
 #pragma unroll
             for (int i = 0; i < NC; i++) {
                 const double tmp = 1 + f.nu[0] * (f.Ks[i] - 1);
-                f.x[1][i]        = ddiv(f.zi[i], tmp);
+                f.x[1][i]        = f.zi[i] / tmp;
                 f.x[0][i]        = f.Ks[i] * f.x[1][i];
             }
             double fug0[NC], fug1[NC];
@@ -589,8 +589,8 @@ __device__ void sp_ssm_body(const FluidConst& F, const PhasedArgs& a, int r)
             double Se = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                Se = __dadd_rn(Se, sq(ddiv(fug1[i], fug0[i]) - 1));
-                f.Ks[i] = ddiv(f.phi[1][i], f.phi[0][i]);
+                Se = __dadd_rn(Se, sq(fug1[i] / fug0[i] - 1));
+                f.Ks[i] = f.phi[1][i] / f.phi[0][i];
             }
             iter++;
             const bool cap = iter > maxIt;
@@ -757,7 +757,7 @@ __device__ void sp_nrinit_body(const FluidConst& F, const PhasedArgs& a, int r)
         for (int i = 0; i < NC; i++) {
             f.n[0][i] = f.nu[0] * f.x[0][i];
             f.n[1][i] = f.nu[1] * f.x[1][i];
-            const double res = log(ddiv(f.fug[1][i], f.fug[0][i]));
+            const double res = log(f.fug[1][i] / f.fug[0][i]);
             eNR += res * res;
         }
         eNR = sqrt(eNR);
@@ -796,7 +796,7 @@ __device__ void sp_nr_body(const FluidConst& F, const PhasedArgs& a, int r)
         eNR  = eNR0;
         iter = 0;
 #pragma unroll
-        for (int i = 0; i < NC; i++) res[i] = log(ddiv(f.fug[1][i], f.fug[0][i]));
+        for (int i = 0; i < NC; i++) res[i] = log(f.fug[1][i] / f.fug[0][i]);
     };
     if (c >= 0) load();
     while (__any_sync(0xffffffffu, c >= 0)) {
@@ -808,7 +808,7 @@ __device__ void sp_nr_body(const FluidConst& F, const PhasedArgs& a, int r)
                 eNR = 0;
 #pragma unroll
                 for (int i = 0; i < NC; i++) {
-                    res[i] = log(ddiv(f.fug[1][i], f.fug[0][i]));
+                    res[i] = log(f.fug[1][i] / f.fug[0][i]);
                     eNR += res[i] * res[i];
                 }
                 eNR = sqrt(eNR);

@@ -3,8 +3,8 @@
 // successive substitution converges over tens of thousands of iterations).
 //
 // Such a cell is a chain of tens of thousands of dependent iterations, so
-// its time is latency: on one thread an FP64 division costs ~114 cycles (~60
-// as ddiv), a logarithm ~270, acos ~190 and cos ~255, an FP64 add ~8.
+// its time is latency: on one thread an FP64 division costs ~115 cycles and
+// independent divisions do not overlap, a logarithm ~270, acos + cos ~475.
 // Here every lane holds the whole cell state (a CellFlash) and takes the
 // same branches, while the operations of an iteration that are independent
 // of one another run on different lanes and are then broadcast with
@@ -70,7 +70,7 @@ struct WarpSplit {
             if (f.Ks[i] < Kmin) Kmin = f.Ks[i];
             if (f.Ks[i] > Kmax) Kmax = f.Ks[i];
         }
-        const double bound = drcp(1 - (half ? Kmin : Kmax));
+        const double bound = 1 / (1 - (half ? Kmin : Kmax));
         const double numin = __shfl_sync(WARP_ALL, bound, 0);
         const double numax = __shfl_sync(WARP_ALL, bound, 16);
         double       v     = 0.5 * (numin + numax);
@@ -82,7 +82,7 @@ struct WarpSplit {
         int          iter = 0;
         while (true) {
             const double tmp  = 1 + v * km1;
-            const double term = ddiv(num, half ? tmp * tmp : tmp);
+            const double term = num / (half ? tmp * tmp : tmp);
             double       rj = 0, J = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
@@ -90,7 +90,7 @@ struct WarpSplit {
                 J -= __shfl_sync(WARP_ALL, term, 16 + i);
             }
             if (fabs(rj) < f.F.rr_tol || iter > f.F.rr_maxit) break;
-            const double dnuj  = ddiv(-rj, J);
+            const double dnuj  = -rj / J;
             const double tmpnu = v + dnuj;
             if (tmpnu < numax && tmpnu > numin)
                 v = tmpnu;
@@ -109,7 +109,7 @@ struct WarpSplit {
     __device__ __forceinline__ void update_x()
     {
         const double tmp = 1 + f.nu[0] * (pick(f.Ks) - 1);
-        const double x1  = ddiv(pick(f.zi), tmp);
+        const double x1  = pick(f.zi) / tmp;
         const double x0  = pick(f.Ks) * x1;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
@@ -199,7 +199,7 @@ struct WarpSplit {
             fug_phi_all();
             // lane i: component i's squared fugacity-ratio residual; lane
             // 16 + i: its new K (one division on every lane)
-            const double quo = ddiv(half ? pick(f.phi[1]) : pick(f.fug[1]), half ? pick(f.phi[0]) : pick(f.fug[0]));
+            const double quo = (half ? pick(f.phi[1]) : pick(f.fug[1])) / (half ? pick(f.phi[0]) : pick(f.fug[0]));
             const double v   = half ? quo : sq(quo - 1);
             Se               = 0;
 #pragma unroll
@@ -220,7 +220,7 @@ struct WarpSplit {
     // ln(f_1i / f_0i) of every component, one per lane, and their squared sum
     __device__ __forceinline__ double residual(double* res) const
     {
-        const double r   = log(ddiv(pick(f.fug[1]), pick(f.fug[0])));
+        const double r   = log(pick(f.fug[1]) / pick(f.fug[0]));
         double       eNR = 0;
 #pragma unroll
         for (int i = 0; i < NC; i++) {

@@ -60,18 +60,3 @@ def test_div_const_is_the_correctly_rounded_quotient(name):
         if not (got == want and np.signbit(got) == np.signbit(want)):
             bad.append((x, got, want))
     assert not bad, bad[:5]
-
-
-@pytest.mark.gpu
-def test_ddiv_matches_device_division():
-    """The kernels' general FP64 division (ddiv in flash_common.cuh: a
-    reciprocal estimate, Newton-Raphson on reciprocal and quotient together,
-    a remainder correction) gives the bits of the device's '/' on ~1.2e9
-    seeded operand pairs over six distributions: moderate and wide
-    exponents, divisors and dividends next to powers of two, quotients next
-    to one, and operands outside its fast path (which take '/')."""
-    from opencaeporo_b200 import _lib
-    for seed in (1, 2):
-        bad, cycles = _lib.selfcheck_division(600_000_000, seed=seed)
-        assert bad == 0, (seed, bad)
-    assert 0 < cycles < 114, cycles  # shorter than the division routine's chain

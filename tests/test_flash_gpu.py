@@ -196,7 +196,8 @@ def test_batched_equals_plain(case):
     # the counts of the iteration it ends
     event = (_lib.CELL_SSMSTA_CAP | _lib.CELL_NRSTA_FAIL | _lib.CELL_SSMSP_FAIL | _lib.CELL_NRSP_FAIL |
              _lib.CELL_SINGULAR)
-    np.testing.assert_array_equal(a["status"] & ~event, b["status"] & ~event, err_msg="status")
+    keep = np.uint16(0xFFFF & ~event)
+    np.testing.assert_array_equal(a["status"] & keep, b["status"] & keep, err_msg="status")
     same_it = np.all(a["iters"] == b["iters"], axis=1)
     diff = np.nonzero(same_it & (a["status"] != b["status"]))[0]
     assert len(diff) == 0, [(int(c), int(a["status"][c]), int(b["status"][c]), a["iters"][c].tolist())
