@@ -332,16 +332,57 @@ int ocpf_flash_fimn(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_sk
 int ocpf_init_flash_fimn(ocpf_ctx* ctx, int64_t ncell, const ocpf_init_in* in, ocpf_skip* skip, double* Ni,
                          ocpf_fim_out* out, double* res, double* resPc, int form, void* stream);
 
+/* Schedules of ocpf_flash_fim_regions for the batched forms. */
+#define OCPF_SCHED_ONE_LAUNCH 0 /* one launch sequence over every region: each step is one kernel over all
+                                   regions' cells, the persistent kernels' warps drain one region's work
+                                   and move on to the next (at most 4 regions of 3, 6, 9 or 12 components;
+                                   otherwise the streams schedule is used) */
+#define OCPF_SCHED_STREAMS 1    /* one launch sequence per region, overlapped on the regions' own streams */
+
+/* Launch shape of the batched forms of one context, and the schedule of the
+ * ocpf_flash_fim_regions calls it leads (as ctx[0]). Every field changes
+ * only which GPU thread handles which cell, except slow_threads, which
+ * runs the split restarts of the few cells that need them on one thread per
+ * cell instead of one warp per cell (the two paths agree to rounding). No
+ * reference counterpart. */
+typedef struct {
+    int32_t block;        /* threads per block of the thread-per-item kernels: 64 or 128 (default 128) */
+    int32_t persist_pct;  /* resident blocks per SM of the persistent kernels, in percent of what their
+                             registers allow: 1..100 (default 100) */
+    int32_t slow_threads; /* split restarts: 0 one warp per cell (default), 1 one thread per cell */
+    int32_t schedule;     /* OCPF_SCHED_* (default OCPF_SCHED_ONE_LAUNCH) */
+    float   ms;           /* ocpf_autotune: the chosen configuration's time per call; 0 when set by hand */
+    int32_t pad;
+} ocpf_tuning;
+
+int ocpf_get_tuning(const ocpf_ctx* ctx, ocpf_tuning* t);
+int ocpf_set_tuning(ocpf_ctx* ctx, const ocpf_tuning* t);
+
+/* Autotuner: times the batched launch of `form` (OCPF_FORM_BATCHED, _MIXED or
+ * _FAST) over these nreg regions (nreg = 1: one context's ocpf_flash_fim)
+ * for every candidate launch shape -- block 64 / 128, persistent grids at
+ * 50 / 100 % of their resident limit, split restarts on one warp / one
+ * thread per cell and, for several regions, both schedules -- and keeps the
+ * fastest in every context (*best receives it). The runs read the caller's
+ * inputs and skip cache but write only the tuner's own copies: nothing of
+ * the caller's arrays changes. It allocates those copies (about 2.3 KB per
+ * cell for 6 components) for its duration and synchronises `stream`.
+ * `reps` timed runs per candidate (after one untimed), at least 1. */
+int ocpf_autotune(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in, const ocpf_skip* skip,
+                  int form, int reps, void* stream, ocpf_tuning* best);
+
 /* Several PVT regions at once -- the batched counterpart of a Bulk whose
  * cells belong to different regions (flashCal[PVTNUM[n]] in
  * src/OCPFluidMethod.cpp:1108-1120), with the cells grouped by region.
  * Region r flashes ncell[r] cells of in[r] / skip[r] / out[r] through
  * ctx[r] (distinct contexts; fluids of different component counts may be
- * mixed). Each region runs on its context's own stream, forked from and
- * joined back into `stream`, so regions of uneven cost overlap on the GPU;
- * the call is asynchronous on `stream` like ocpf_flash_fim. skip may be null
- * when no region uses the skip cache. Results equal one ocpf_flash_fim per
- * region. */
+ * mixed). The batched forms run as one launch sequence over all regions
+ * (OCPF_SCHED_ONE_LAUNCH, the default, replayed from a CUDA graph while the
+ * arguments stay the same) or as one sequence per region on the regions'
+ * own streams (OCPF_SCHED_STREAMS), as ctx[0]'s tuning says; the plain form
+ * always takes the streams. The call is asynchronous on `stream` like
+ * ocpf_flash_fim. skip may be null when no region uses the skip cache.
+ * Results equal one ocpf_flash_fim per region, bit for bit. */
 int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
                            ocpf_skip* skip, ocpf_fim_out* out, int form, void* stream);
 

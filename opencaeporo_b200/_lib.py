@@ -38,7 +38,10 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_flash_impec", "ocpf_init_flash_fim", "ocpf_init_flash_impec",
            "ocpf_flash_fimn", "ocpf_init_flash_fimn", "ocpf_flash_fim_subset", "ocpf_flash_impec_subset",
            "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count",
-           "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian")
+           "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian",
+           "ocpf_get_tuning", "ocpf_set_tuning", "ocpf_autotune")
+
+SCHED_ONE_LAUNCH, SCHED_STREAMS = 0, 1  # OCPF_SCHED_*
 
 _vp = C.c_void_p
 
@@ -152,6 +155,12 @@ def skip_shapes(nc: int) -> dict:
             "z": (nc, "f64")}
 
 
+class Tuning(C.Structure):
+    """ocpf_tuning"""
+    _fields_ = [("block", C.c_int32), ("persist_pct", C.c_int32), ("slow_threads", C.c_int32),
+                ("schedule", C.c_int32), ("ms", C.c_float), ("pad", C.c_int32)]
+
+
 _LIB = None
 
 
@@ -198,6 +207,13 @@ def lib():
     L.ocpf_flash_fim_regions.argtypes = [C.c_int, C.POINTER(_vp), C.POINTER(C.c_int64), C.POINTER(FimIn),
                                          C.POINTER(Skip), C.POINTER(FimOut), C.c_int, _vp]
     L.ocpf_flash_fim_regions.restype = C.c_int
+    L.ocpf_get_tuning.argtypes = [_vp, C.POINTER(Tuning)]
+    L.ocpf_get_tuning.restype = C.c_int
+    L.ocpf_set_tuning.argtypes = [_vp, C.POINTER(Tuning)]
+    L.ocpf_set_tuning.restype = C.c_int
+    L.ocpf_autotune.argtypes = [C.c_int, C.POINTER(_vp), C.POINTER(C.c_int64), C.POINTER(FimIn), C.POINTER(Skip),
+                                C.c_int, C.c_int, _vp, C.POINTER(Tuning)]
+    L.ocpf_autotune.restype = C.c_int
     L.ocpf_measure_fp64_latency.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.ocpf_measure_fp64_latency.restype = C.c_int
     L.ocpf_flash_impec.argtypes = [_vp, C.c_int64, C.POINTER(ImpecIn), C.POINTER(Skip), C.POINTER(ImpecOut),

@@ -8,7 +8,7 @@
 #include <new>
 #include <vector>
 
-#include "flash_phased.cuh"
+#include "flash_multi.cuh"
 
 namespace ocpf {
 
@@ -28,15 +28,15 @@ using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const
                                       cudaStream_t);
 
 // Batched-form launch sequences (flash_phased_ncN.cu).
-#define OCPF_DECL_PHASED(N)                                                           \
-    cudaError_t launch_phased_nc##N(const FluidConst& F, const PhasedArgs& a, cudaStream_t st); \
+#define OCPF_DECL_PHASED(N)                                                                                 \
+    cudaError_t launch_phased_nc##N(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t, cudaStream_t st); \
     int         phased_state_doubles_nc##N();
 OCPF_DECL_PHASED(3)
 OCPF_DECL_PHASED(6)
 OCPF_DECL_PHASED(9)
 OCPF_DECL_PHASED(12)
 
-using PhasedLauncher = cudaError_t (*)(const FluidConst&, const PhasedArgs&, cudaStream_t);
+using PhasedLauncher = cudaError_t (*)(const FluidConst&, const PhasedArgs&, const LaunchTune&, cudaStream_t);
 
 static PhasedLauncher phased_kernel(int nc, int* ndbl)
 {
@@ -151,7 +151,19 @@ struct ocpf_ctx {
     cudaStream_t    gs;
     cudaGraphExec_t gexec;
     PhasedArgs      gkey;
+    LaunchTune      gtune;
     bool            gvalid;
+    // launch shape of the batched forms (ocpf_set_tuning / ocpf_autotune)
+    // and, for ocpf_flash_fim_regions led by this context, the schedule
+    LaunchTune tune;
+    int32_t    sched;
+    float      tune_ms;
+    // ocpf_flash_fim_regions' one-launch sequence as a CUDA graph, keyed by
+    // its arguments (held by the first region's context)
+    cudaGraphExec_t mgexec;
+    MultiArgs*      mgkey;
+    LaunchTune      mgtune;
+    int32_t         mgkernels;
     int32_t         gkernels;      // kernel nodes of the captured graph
     int32_t         last_kernels;  // kernels the last call launched, -1 unknown
     // subset calls: compact device copies of the listed cells, grown on demand
@@ -212,6 +224,14 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->gs        = nullptr;
     c->gexec     = nullptr;
     c->gvalid    = false;
+    c->gtune     = kDefaultTune;
+    c->tune      = kDefaultTune;
+    c->sched     = OCPF_SCHED_ONE_LAUNCH;
+    c->tune_ms   = 0;
+    c->mgexec    = nullptr;
+    c->mgkey     = nullptr;
+    c->mgtune    = kDefaultTune;
+    c->mgkernels = 0;
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
         delete c;
         cudaSetDevice(prev);
@@ -236,6 +256,8 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     if (c->mlp) cudaFree(c->mlp);
     if (c->rs) cudaStreamDestroy(c->rs);
     if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    if (c->mgexec) cudaGraphExecDestroy(c->mgexec);
+    delete c->mgkey;
     if (c->gs) cudaStreamDestroy(c->gs);
     if (c->evf) cudaEventDestroy(c->evf);
     if (c->evj) cudaEventDestroy(c->evj);
@@ -351,18 +373,22 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusInvalidated;
     c->last_kernels = -1;
-    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, st);
-    if (!(c->gvalid && std::memcmp(&c->gkey, &args, sizeof(args)) == 0)) {
+    const LaunchTune& t = c->tune;
+    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, t, st);
+    if (!(c->gvalid && std::memcmp(&c->gkey, &args, sizeof(args)) == 0 &&
+          std::memcmp(&c->gtune, &t, sizeof(t)) == 0)) {
         c->gvalid = false;
-        if (!c->gs && cudaStreamCreateWithFlags(&c->gs, cudaStreamNonBlocking) != cudaSuccess) return k(c->fc, args, st);
+        if (!c->gs && cudaStreamCreateWithFlags(&c->gs, cudaStreamNonBlocking) != cudaSuccess)
+            return k(c->fc, args, t, st);
         cudaGraph_t g = nullptr;
-        if (cudaStreamBeginCapture(c->gs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return k(c->fc, args, st);
-        const cudaError_t le = k(c->fc, args, c->gs);
+        if (cudaStreamBeginCapture(c->gs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return k(c->fc, args, t, st);
+        const cudaError_t le = k(c->fc, args, t, c->gs);
         const cudaError_t ce = cudaStreamEndCapture(c->gs, &g);
         if (le != cudaSuccess || ce != cudaSuccess || !g) {
             if (g) cudaGraphDestroy(g);
             cudaGetLastError();
-            return k(c->fc, args, st);
+            return k(c->fc, args, t, st);
         }
         size_t nn = 0;
         int    nk = 0;
@@ -390,9 +416,10 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
         if (!ok) {
             c->gexec = nullptr;
             cudaGetLastError();
-            return k(c->fc, args, st);
+            return k(c->fc, args, t, st);
         }
         c->gkey   = args;
+        c->gtune  = t;
         c->gvalid = true;
     }
     c->last_kernels = c->gkernels;
@@ -573,23 +600,114 @@ extern "C" int ocpf_init_flash_fimn(ocpf_ctx* c, int64_t ncell, const ocpf_init_
                        stream);
 }
 
-extern "C" int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
-                                      ocpf_skip* sk, ocpf_fim_out* out, int form, void* stream)
+// The one-launch sequence of ocpf_flash_fim_regions, replayed from a CUDA
+// graph held by the leading context while the arguments and the launch
+// shape stay the same (as launch_phased does for one region).
+static cudaError_t launch_multi(ocpf_ctx* c, const MultiFluid& MF, const MultiArgs& M, cudaStream_t st)
 {
-    if (nreg < 0) return OCPF_EINVAL;
-    if (nreg == 0) return OCPF_OK;
-    if (!ctx || !ncell || !in || !out) return OCPF_EINVAL;
-    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
-    for (int r = 0; r < nreg; r++) {
-        if (!ctx[r] || ncell[r] < 0 || ctx[r]->device != ctx[0]->device) return OCPF_EINVAL;
-        for (int q = 0; q < r; q++)
-            if (ctx[q] == ctx[r]) return OCPF_EINVAL;  // one context owns one scratch and stream
-        if (ncell[r] > 0 && !fim_args_ok(ctx[r], &in[r], sk ? &sk[r] : nullptr, &out[r])) return OCPF_EINVAL;
+    const LaunchTune&       t  = c->tune;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusInvalidated;
+    c->last_kernels = -1;
+    if (cs != cudaStreamCaptureStatusNone) return launch_phased_multi(MF, M, t, st);
+    const bool same = c->mgexec && c->mgkey && std::memcmp(c->mgkey, &M, sizeof(M)) == 0 &&
+                      std::memcmp(&c->mgtune, &t, sizeof(t)) == 0;
+    if (!same) {
+        if (!c->mgkey) {
+            c->mgkey = new (std::nothrow) MultiArgs;
+            if (!c->mgkey) return launch_phased_multi(MF, M, t, st);
+            std::memset(c->mgkey, 0, sizeof(MultiArgs));
+            // the first call launches directly (it also sets up each kernel)
+            std::memcpy(c->mgkey, &M, sizeof(M));
+            c->mgtune = t;
+            return launch_phased_multi(MF, M, t, st);
+        }
+        if (!c->gs && cudaStreamCreateWithFlags(&c->gs, cudaStreamNonBlocking) != cudaSuccess)
+            return launch_phased_multi(MF, M, t, st);
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(c->gs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+            return launch_phased_multi(MF, M, t, st);
+        const cudaError_t le = launch_phased_multi(MF, M, t, c->gs);
+        const cudaError_t ce = cudaStreamEndCapture(c->gs, &g);
+        if (le != cudaSuccess || ce != cudaSuccess || !g) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            return launch_phased_multi(MF, M, t, st);
+        }
+        size_t nn = 0;
+        int    nk = 0;
+        if (cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn > 0) {
+            std::vector<cudaGraphNode_t> nodes(nn);
+            if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+                for (size_t i = 0; i < nn; i++) {
+                    cudaGraphNodeType ty;
+                    if (cudaGraphNodeGetType(nodes[i], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) nk++;
+                }
+        }
+        if (c->mgexec) cudaGraphExecDestroy(c->mgexec);
+        c->mgexec = nullptr;
+        const bool ok = cudaGraphInstantiate(&c->mgexec, g, 0) == cudaSuccess;
+        cudaGraphDestroy(g);
+        if (!ok) {
+            c->mgexec = nullptr;
+            cudaGetLastError();
+            return launch_phased_multi(MF, M, t, st);
+        }
+        std::memcpy(c->mgkey, &M, sizeof(M));
+        c->mgtune    = t;
+        c->mgkernels = nk;
     }
-    int prev = 0;
-    cudaGetDevice(&prev);
-    const int dev = ctx[0]->device;
-    if (prev != dev) cudaSetDevice(dev);
+    c->last_kernels = c->mgkernels;
+    return cudaGraphLaunch(c->mgexec, st);
+}
+
+static bool multi_nc_ok(int nc) { return nc == 3 || nc == 6 || nc == 9 || nc == 12; }
+
+// Every non-empty region in one launch sequence (OCPF_SCHED_ONE_LAUNCH).
+static int regions_one_launch(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
+                              ocpf_skip* sk, ocpf_fim_out* out, int form, cudaStream_t st)
+{
+    MultiFluid* MF = new (std::nothrow) MultiFluid;
+    if (!MF) return OCPF_ENOMEM;
+    MultiArgs M;
+    std::memset(&M, 0, sizeof(M));  // compared bytewise as the graph's key
+    int rc = OCPF_OK, n = 0;
+    for (int r = 0; r < nreg && rc == OCPF_OK; r++) {
+        if (ncell[r] == 0) continue;
+        ocpf_ctx* c = ctx[r];
+        rc          = ensure_scratch(c, ncell[r]);
+        if (rc != OCPF_OK) break;
+        PhasedArgs& a = M.a[n];
+        a.count  = ncell[r];
+        a.stride = ncell[r];
+        a.in     = in[r];
+        a.sk     = sk ? sk[r] : ocpf_skip{};
+        a.out    = out[r];
+        a.opts   = form >= OCPF_FORM_MIXED ? PH_MIXED : 0u;
+        a.mlp    = c->mlp;
+        a.tail   = FlashTail{FM_FIM, nullptr, nullptr, nullptr};
+        if (form == OCPF_FORM_FAST && c->mlp && c->fc.learn_on) a.opts |= PH_LEARN;
+        scratch_view(c, 0, c->eq_cap, a.S, a.L);
+        MF->F[n] = c->fc;
+        M.nc[n]  = c->fc.nc;
+        n++;
+    }
+    if (rc == OCPF_OK && n > 0) {
+        M.n = n;
+        for (int r = 0; r < n; r++) {
+            M.a[r].vpart  = r;
+            M.a[r].vparts = n;
+        }
+        if (launch_multi(ctx[0], *MF, M, st) != cudaSuccess) rc = OCPF_ECUDA;
+    }
+    delete MF;
+    return rc;
+}
+
+// One launch sequence per region on the regions' own streams (OCPF_SCHED_STREAMS).
+static int regions_streams(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
+                           ocpf_skip* sk, ocpf_fim_out* out, int form, cudaStream_t stream)
+{
     int rc = OCPF_OK;
     for (int r = 0; r < nreg && rc == OCPF_OK; r++) {
         ocpf_ctx* c = ctx[r];
@@ -600,7 +718,7 @@ extern "C" int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int6
             rc = OCPF_ECUDA;
     }
     // fork: every region's stream starts after the work already on `stream`
-    if (rc == OCPF_OK && cudaEventRecord(ctx[0]->evf, (cudaStream_t)stream) != cudaSuccess) rc = OCPF_ECUDA;
+    if (rc == OCPF_OK && cudaEventRecord(ctx[0]->evf, stream) != cudaSuccess) rc = OCPF_ECUDA;
     for (int r = 0; r < nreg && rc == OCPF_OK; r++) {
         ocpf_ctx* c = ctx[r];
         if (cudaStreamWaitEvent(c->rs, ctx[0]->evf, 0) != cudaSuccess) {
@@ -613,11 +731,78 @@ extern "C" int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int6
         c->timed = false;
         // join: `stream` continues after every region
         if (rc == OCPF_OK && (cudaEventRecord(c->evj, c->rs) != cudaSuccess ||
-                              cudaStreamWaitEvent((cudaStream_t)stream, c->evj, 0) != cudaSuccess))
+                              cudaStreamWaitEvent(stream, c->evj, 0) != cudaSuccess))
             rc = OCPF_ECUDA;
     }
+    return rc;
+}
+
+static int regions_check(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
+                         const ocpf_skip* sk, const ocpf_fim_out* out, int form)
+{
+    if (nreg < 0) return OCPF_EINVAL;
+    if (nreg == 0) return OCPF_OK;
+    if (!ctx || !ncell || !in || !out) return OCPF_EINVAL;
+    if (form < OCPF_FORM_PLAIN || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    for (int r = 0; r < nreg; r++) {
+        if (!ctx[r] || ncell[r] < 0 || ctx[r]->device != ctx[0]->device) return OCPF_EINVAL;
+        for (int q = 0; q < r; q++)
+            if (ctx[q] == ctx[r]) return OCPF_EINVAL;  // one context owns one scratch and stream
+        if (ncell[r] > 0 && !fim_args_ok(ctx[r], &in[r], sk ? &sk[r] : nullptr, &out[r])) return OCPF_EINVAL;
+    }
+    return OCPF_OK;
+}
+
+static bool one_launch_ok(int nreg, ocpf_ctx* const* ctx, int form)
+{
+    if (form == OCPF_FORM_PLAIN || nreg > MULTI_MAX || ctx[0]->sched != OCPF_SCHED_ONE_LAUNCH) return false;
+    for (int r = 0; r < nreg; r++)
+        if (!multi_nc_ok(ctx[r]->fc.nc)) return false;
+    return true;
+}
+
+extern "C" int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
+                                      ocpf_skip* sk, ocpf_fim_out* out, int form, void* stream)
+{
+    int rc = regions_check(nreg, ctx, ncell, in, sk, out, form);
+    if (rc != OCPF_OK || nreg == 0) return rc;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    const int dev = ctx[0]->device;
+    if (prev != dev) cudaSetDevice(dev);
+    if (one_launch_ok(nreg, ctx, form))
+        rc = regions_one_launch(nreg, ctx, ncell, in, sk, out, form, (cudaStream_t)stream);
+    else
+        rc = regions_streams(nreg, ctx, ncell, in, sk, out, form, (cudaStream_t)stream);
+    for (int r = 0; r < nreg; r++) ctx[r]->timed = false;
     if (prev != dev) cudaSetDevice(prev);
     return rc;
+}
+
+// ------------------------------------------------------------------ tuning
+extern "C" int ocpf_get_tuning(const ocpf_ctx* c, ocpf_tuning* t)
+{
+    if (!c || !t) return OCPF_EINVAL;
+    t->block        = c->tune.block;
+    t->persist_pct  = c->tune.persist_pct;
+    t->slow_threads = c->tune.slow_threads;
+    t->schedule     = c->sched;
+    t->ms           = c->tune_ms;
+    t->pad          = 0;
+    return OCPF_OK;
+}
+
+extern "C" int ocpf_set_tuning(ocpf_ctx* c, const ocpf_tuning* t)
+{
+    if (!c || !t) return OCPF_EINVAL;
+    if ((t->block != 64 && t->block != 128) || t->persist_pct < 1 || t->persist_pct > 100 ||
+        (t->slow_threads != 0 && t->slow_threads != 1) ||
+        (t->schedule != OCPF_SCHED_ONE_LAUNCH && t->schedule != OCPF_SCHED_STREAMS))
+        return OCPF_EINVAL;
+    c->tune    = LaunchTune{t->block, t->persist_pct, t->slow_threads, 0};
+    c->sched   = t->schedule;
+    c->tune_ms = t->ms;
+    return OCPF_OK;
 }
 
 extern "C" int ocpf_last_launch_count(ocpf_ctx* c, int* n)
@@ -1153,3 +1338,131 @@ bool ctx_fim_args_ok(const ocpf_ctx* c, const ocpf_fim_in* in, const ocpf_skip* 
     return fim_args_ok(c, in, sk, o);
 }
 }  // namespace ocpf
+
+extern "C" int ocpf_autotune(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
+                             const ocpf_skip* sk, int form, int reps, void* stream, ocpf_tuning* best)
+{
+    if (nreg < 1 || !best || reps < 1 || form < OCPF_FORM_BATCHED || form > OCPF_FORM_FAST) return OCPF_EINVAL;
+    if (!ctx || !ncell || !in) return OCPF_EINVAL;
+    for (int r = 0; r < nreg; r++) {
+        if (!ctx[r] || ncell[r] < 0 || ctx[r]->device != ctx[0]->device) return OCPF_EINVAL;
+        for (int q = 0; q < r; q++)
+            if (ctx[q] == ctx[r]) return OCPF_EINVAL;
+        const ocpf_fim_in& i = in[r];
+        if (ncell[r] > 0 && (!i.P || !i.T || !i.Ni || !i.S || !i.lastNP || !i.xij)) return OCPF_EINVAL;
+        if (ncell[r] > 0 && !skip_ok(ctx[r], sk ? &sk[r] : nullptr)) return OCPF_EINVAL;
+    }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    const int dev = ctx[0]->device;
+    if (prev != dev) cudaSetDevice(dev);
+    const cudaStream_t st = (cudaStream_t)stream;
+    // the tuner's own copies: inputs, outputs, skip cache and its saved state
+    std::vector<void*>        bufs(nreg, nullptr), skbuf(nreg, nullptr);
+    std::vector<Views>        v(nreg);
+    std::vector<ocpf_fim_in>  vin(nreg);
+    std::vector<ocpf_skip>    vsk(nreg);
+    std::vector<ocpf_fim_out> vout(nreg);
+    int                       rc = OCPF_OK;
+    ocpf_fim_out              all{};
+    all.nj = (double*)1, all.ePEC = (double*)1, all.iters = (int32_t*)1, all.status = (uint16_t*)1,
+    all.ftype = (uint8_t*)1;  // keep every diagnostic output in the views
+    for (int r = 0; r < nreg && rc == OCPF_OK; r++) {
+        if (ncell[r] == 0) continue;
+        const Layout L{ctx[r]->fc.nc, ctx[r]->fc.nc + 1, ctx[r]->fc.nc + 2};
+        const bool   has_sk = sk && sk[r].flag;
+        if (cudaMalloc(&bufs[r], stage_stride(L.bytes_per_cell(), ncell[r])) != cudaSuccess) {
+            rc = OCPF_ENOMEM;
+            break;
+        }
+        v[r] = carve(bufs[r], ncell[r], L, has_sk ? &sk[r] : nullptr, &all);
+        const int64_t n = ncell[r];
+        const ocpf_fim_in& i = in[r];
+        cudaMemcpyAsync((void*)v[r].in.P, i.P, 8 * n, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync((void*)v[r].in.T, i.T, 8 * n, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync((void*)v[r].in.Ni, i.Ni, 8 * n * L.ncom, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync((void*)v[r].in.S, i.S, 8 * n * NPH, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync((void*)v[r].in.lastNP, i.lastNP, 4 * n, cudaMemcpyDeviceToDevice, st);
+        cudaMemcpyAsync((void*)v[r].in.xij, i.xij, 8 * n * NPH * L.ncom, cudaMemcpyDeviceToDevice, st);
+        if (has_sk) {
+            // the caller's cache, kept aside and restored before every run
+            const size_t skb = (size_t)n * (4 + 8 * (3 + L.nc));
+            if (cudaMalloc(&skbuf[r], skb) != cudaSuccess) {
+                rc = OCPF_ENOMEM;
+                break;
+            }
+            char* p = (char*)skbuf[r];
+            cudaMemcpyAsync(p, sk[r].flag, 4 * n, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(p + 4 * n, sk[r].minEig, 8 * n, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(p + 12 * n, sk[r].P, 8 * n, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(p + 20 * n, sk[r].T, 8 * n, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(p + 28 * n, sk[r].z, 8 * n * L.nc, cudaMemcpyDeviceToDevice, st);
+        }
+        vin[r]  = v[r].in;
+        vsk[r]  = v[r].sk;
+        vout[r] = v[r].out;
+    }
+    auto restore_skip = [&]() {
+        for (int r = 0; r < nreg; r++) {
+            if (!skbuf[r]) continue;
+            const int64_t n = ncell[r];
+            const char*   p = (const char*)skbuf[r];
+            cudaMemcpyAsync(vsk[r].flag, p, 4 * n, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(vsk[r].minEig, p + 4 * n, 8 * n, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(vsk[r].P, p + 12 * n, 8 * n, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(vsk[r].T, p + 20 * n, 8 * n, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(vsk[r].z, p + 28 * n, 8 * n * ctx[r]->fc.nc, cudaMemcpyDeviceToDevice, st);
+        }
+    };
+    ocpf_tuning win{};
+    win.ms = -1;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (rc == OCPF_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = OCPF_ECUDA;
+    const int blocks[2] = {128, 64}, pcts[2] = {100, 50}, slows[2] = {0, 1};
+    const int nsched = nreg > 1 ? 2 : 1;
+    for (int sc = 0; sc < nsched && rc == OCPF_OK; sc++)
+        for (int bi = 0; bi < 2 && rc == OCPF_OK; bi++)
+            for (int pi = 0; pi < 2 && rc == OCPF_OK; pi++)
+                for (int si = 0; si < 2 && rc == OCPF_OK; si++) {
+                    ocpf_tuning cand{blocks[bi], pcts[pi], slows[si], sc == 0 ? OCPF_SCHED_ONE_LAUNCH : OCPF_SCHED_STREAMS,
+                                     0.f, 0};
+                    for (int r = 0; r < nreg; r++) ocpf_set_tuning(ctx[r], &cand);
+                    float bestc = 1e30f;
+                    for (int k = 0; k <= reps && rc == OCPF_OK; k++) {
+                        restore_skip();
+                        cudaEventRecord(e0, st);
+                        if (nreg == 1)
+                            rc = launch_form(ctx[0], form, ncell[0], ncell[0], vin[0], vsk[0], vout[0], st, false);
+                        else if (one_launch_ok(nreg, ctx, form))
+                            rc = regions_one_launch(nreg, ctx, ncell, vin.data(), vsk.data(), vout.data(), form, st);
+                        else
+                            rc = regions_streams(nreg, ctx, ncell, vin.data(), vsk.data(), vout.data(), form, st);
+                        cudaEventRecord(e1, st);
+                        if (cudaEventSynchronize(e1) != cudaSuccess) rc = OCPF_ECUDA;
+                        float ms = 0;
+                        cudaEventElapsedTime(&ms, e0, e1);
+                        if (k > 0 && ms < bestc) bestc = ms;
+                    }
+                    if (rc == OCPF_OK && (win.ms < 0 || bestc < win.ms)) {
+                        win    = cand;
+                        win.ms = bestc;
+                    }
+                }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(st);
+    for (int r = 0; r < nreg; r++) {
+        if (bufs[r]) cudaFree(bufs[r]);
+        if (skbuf[r]) cudaFree(skbuf[r]);
+    }
+    if (rc == OCPF_OK) {
+        for (int r = 0; r < nreg; r++) ocpf_set_tuning(ctx[r], &win);
+        *best = win;
+    } else {
+        const ocpf_tuning def{kDefaultTune.block, kDefaultTune.persist_pct, kDefaultTune.slow_threads,
+                              OCPF_SCHED_ONE_LAUNCH, 0.f, 0};
+        for (int r = 0; r < nreg; r++) ocpf_set_tuning(ctx[r], &def);
+    }
+    if (prev != dev) cudaSetDevice(prev);
+    return rc;
+}

@@ -35,7 +35,7 @@ __device__ void learn_body(const FluidConst& F, const PhasedArgs& a, LearnSmem& 
     const uint32_t  n = a.L.len(L_FRESH);
     const int       m0 = 16 * (threadIdx.x >> 5);
     mlp_load_weights(sm.w, a.mlp);
-    for (uint32_t base = blockIdx.x * 64u; base < n; base += gridDim.x * 64u) {
+    for (uint32_t base = vblock(a) * 64u; base < n; base += vgrid(a) * 64u) {
         __syncthreads();  // weights loaded / previous tile's outputs consumed
         if (threadIdx.x < 64) {
             const uint32_t k = base + threadIdx.x;

@@ -122,6 +122,21 @@ struct Lists {
     }
 };
 
+// Launch shape of a batched sequence, chosen per context by the autotuner
+// (ocpf_autotune): threads per block of the thread-per-item kernels (64 or
+// 128; every kernel is built for at most 128), the resident blocks per SM
+// of the persistent kernels as a percentage of what their registers allow,
+// and the restart path: one warp per cell (0) or one thread per cell (1).
+// Block size and persistent grid change only which thread takes which
+// cell, never a cell's arithmetic.
+struct LaunchTune {
+    int32_t block;
+    int32_t persist_pct;
+    int32_t slow_threads;
+    int32_t pad;
+};
+constexpr LaunchTune kDefaultTune{128, 100, 0, 0};
+
 // PhasedArgs::opts bits
 constexpr uint32_t PH_MIXED = 1u;  // FP32 successive substitution (flash_mixed.cuh)
 constexpr uint32_t PH_LEARN = 2u;  // learned initialiser for fresh cells (flash_learned.cuh)
@@ -129,6 +144,11 @@ constexpr uint32_t PH_LEARN = 2u;  // learned initialiser for fresh cells (flash
 struct PhasedArgs {
     int64_t      count, stride;
     uint32_t     opts;
+    // Block partition of a launch shared by several regions (flash_multi):
+    // this region's blocks are those with blockIdx.x % vparts == vpart, and
+    // its grid-stride loops see block blockIdx.x / vparts of a grid of
+    // gridDim.x / vparts. vparts <= 1: the whole launch is this region's.
+    int32_t      vpart, vparts;
     const float* mlp;  // learned initialiser parameters (PH_LEARN)
     FlashTail    tail; // entry point (FlashFIM, FlashIMPEC, InitFlash*) and its extra arrays
     ocpf_fim_in  in;
@@ -137,6 +157,16 @@ struct PhasedArgs {
     StateBuf     S;
     Lists        L;
 };
+
+// The region's block index and block count within its launch (PhasedArgs::vpart).
+__device__ __forceinline__ uint32_t vblock(const PhasedArgs& a)
+{
+    return a.vparts > 1 ? blockIdx.x / (uint32_t)a.vparts : blockIdx.x;
+}
+__device__ __forceinline__ uint32_t vgrid(const PhasedArgs& a)
+{
+    return a.vparts > 1 ? gridDim.x / (uint32_t)a.vparts : gridDim.x;
+}
 
 // z of cell c, bit for bit as FimCell::load_inputs forms it: Ni / Nh
 // (InitPTN), or in the initialisation the given mole fractions (InitPTZ).

@@ -9,9 +9,9 @@ namespace ocpf {
 
 // Thread-per-item kernels walk their list with a grid-stride loop: the grid
 // is fixed at launch (the list length is only known on the device).
-#define OCPF_FOR_ITEMS(A, LIST, c)                                                              \
-    for (uint32_t _k = blockIdx.x * blockDim.x + threadIdx.x, _n = (A).L.len(LIST); _k < _n; \
-         _k += gridDim.x * blockDim.x)                                                          \
+#define OCPF_FOR_ITEMS(A, LIST, c)                                                                   \
+    for (uint32_t _k = vblock(A) * blockDim.x + threadIdx.x, _n = (A).L.len(LIST); _k < _n;        \
+         _k += vgrid(A) * blockDim.x)                                                                \
         if (const int64_t c = (A).L.item(LIST, _k); true)
 
 // ------------------------------------------------------------------ init
@@ -24,8 +24,8 @@ __device__ void init_body(const FluidConst& F, const PhasedArgs& a)
 {
     using F_ = SF<NC>;
     const StateBuf& S = a.S;
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
-         c += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t c = vblock(a) * (int64_t)blockDim.x + threadIdx.x; c < a.count;
+         c += (int64_t)vgrid(a) * blockDim.x) {
         FimCell<NC> f(F);
         f.load_inputs(c, a.stride, a.in, a.sk, a.tail);
         f.cal_ai_bi();
@@ -841,9 +841,9 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
     using F_ = SF<NC>;
     const StateBuf& S    = a.S;
     const uint32_t  n    = a.L.len(L_SLOW);
-    const uint32_t  nw   = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t  nw   = (vgrid(a) * blockDim.x) >> 5;
     const bool      lead = (threadIdx.x & 31) == 0;
-    for (uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < n; k += nw) {
+    for (uint32_t k = (vblock(a) * blockDim.x + threadIdx.x) >> 5; k < n; k += nw) {
         const int64_t c = a.L.item(L_SLOW, k);
         CellFlash<NC> f(F);
         uint32_t      meta;
@@ -881,14 +881,58 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
     }
 }
 
+// The restart loop of slow_body with one thread per cell (CellFlash's own
+// SplitSSM2 / SplitNR, as in the plain form): 32 cells per warp instead of
+// one, each on a longer dependent chain. The autotuner's alternative for
+// batches with many restarting cells.
+template <int NC>
+__device__ void slow_thread_body(const FluidConst& F, const PhasedArgs& a)
+{
+    using F_ = SF<NC>;
+    const StateBuf& S = a.S;
+    OCPF_FOR_ITEMS(a, L_SLOW, c)
+    {
+        CellFlash<NC> f(F);
+        uint32_t      meta;
+        load_split_cell(f, a, c, meta);
+        f.T = a.in.T[c] + CONV5;
+        f.cal_kwilson();
+        int guard = S.I(IF_GUARD, c);
+        while (true) {
+            f.split_ssm2(true);
+            f.split_nr();
+            if (!f.check_split()) break;
+            if (f.ssmsp_conflag || f.nrsp_conflag) break;
+            if (++guard > SPLIT_RESTART_CAP) {
+                f.status |= ST_SPLIT_CAP;
+                break;
+            }
+        }
+        f.check_split();
+        if (!f.ssmsp_conflag) f.status |= ST_SSMSP_FAIL;
+        if (!f.nrsp_conflag) f.status |= ST_NRSP_FAIL;
+        finish_epec(f);
+        S.D(F_::ePEC, c) = f.ePEC;
+        if (f.NP == 1) {
+            S.D(F_::Aj0, c) = f.Aj[0];
+            S.D(F_::Bj0, c) = f.Bj[0];
+            S.D(F_::Zj0, c) = f.Zj[0];
+            store_single_phase(f, S, c, true);
+        } else {
+            store_split(f, S, c);
+        }
+        store_book(f, S, c, meta);
+    }
+}
+
 // --------------------------------------------------------------- finalize
 template <int NC, bool FIMN = false>
 __device__ void phased_finalize_body(const FluidConst& F, const PhasedArgs& a)
 {
     using F_ = SF<NC>;
     const StateBuf& S = a.S;
-    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < a.count;
-         c += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t c = vblock(a) * (int64_t)blockDim.x + threadIdx.x; c < a.count;
+         c += (int64_t)vgrid(a) * blockDim.x) {
         FimCell<NC> f(F);
         f.load_inputs(c, a.stride, a.in, a.sk, a.tail);
         uint32_t meta;

@@ -1,43 +1,4 @@
-// flash_plain_nc12.cu -- the plain FP64 FIM flash kernel for 12 hydrocarbon
-// components (one translation unit per component count keeps builds parallel).
-#include "flash_fim.cuh"
-
-namespace ocpf {
-
-// One thread per cell, 128 cells per block: the hardware block scheduler
-// balances the very uneven per-cell iteration counts across the SMs.
-__global__ void __launch_bounds__(128) k_flash_fim_plain_nc12(const __grid_constant__ FluidConst F,
-                                                             int64_t count, int64_t stride,
-                                                             const ocpf_fim_in in, const ocpf_skip sk,
-                                                             const ocpf_fim_out out, const FlashTail tail)
-{
-    const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (n >= count) return;
-    FimCell<12> c(F);
-    c.run(n, stride, in, sk, out, tail);
-}
-
-// The same for FlashFIMn / InitFlashFIMn (the FIMn tail in a kernel of its own).
-__global__ void __launch_bounds__(128) k_flash_fimn_plain_nc12(const __grid_constant__ FluidConst F,
-                                                              int64_t count, int64_t stride,
-                                                              const ocpf_fim_in in, const ocpf_skip sk,
-                                                              const ocpf_fim_out out, const FlashTail tail)
-{
-    const int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (n >= count) return;
-    FimCell<12> c(F);
-    c.template run<true>(n, stride, in, sk, out, tail);
-}
-
-cudaError_t launch_plain_nc12(const FluidConst& F, int64_t count, int64_t stride, const ocpf_fim_in& in,
-                              const ocpf_skip& sk, const ocpf_fim_out& out, const FlashTail& tail,
-                              unsigned blocks, int bs, cudaStream_t st)
-{
-    if (tail.mode & FM_FIMN)
-        k_flash_fimn_plain_nc12<<<blocks, bs, 0, st>>>(F, count, stride, in, sk, out, tail);
-    else
-        k_flash_fim_plain_nc12<<<blocks, bs, 0, st>>>(F, count, stride, in, sk, out, tail);
-    return cudaGetLastError();
-}
-
-}  // namespace ocpf
+// flash_plain_nc12.cu -- the plain FP64 FIM flash kernels for 12 hydrocarbon
+// components (flash_plain_inst.cuh).
+#define OCPF_NC 12
+#include "flash_plain_inst.cuh"

@@ -92,6 +92,17 @@ class MixtureCompBatch:
         check(lib().ocpf_create(C.byref(self._f), int(device), C.byref(h)), "ocpf_create")
         self._h = h
 
+    def tuning(self) -> dict:
+        """This context's launch shape and regions schedule (ocpf_get_tuning)."""
+        t = _lib.Tuning()
+        check(lib().ocpf_get_tuning(self._h, C.byref(t)), "ocpf_get_tuning")
+        return {k: getattr(t, k) for k in ("block", "persist_pct", "slow_threads", "schedule", "ms")}
+
+    def set_tuning(self, block=128, persist_pct=100, slow_threads=0, schedule=0):
+        """Sets the launch shape by hand (ocpf_set_tuning)."""
+        t = _lib.Tuning(int(block), int(persist_pct), int(slow_threads), int(schedule), 0.0, 0)
+        check(lib().ocpf_set_tuning(self._h, C.byref(t)), "ocpf_set_tuning")
+
     def close(self):
         if getattr(self, "_h", None):
             lib().ocpf_destroy(self._h)
@@ -338,11 +349,23 @@ class MixtureCompBatch:
         check(rc, "ocpf_flash_fim_host")
 
 
+def _region_structs(regions, fresh, diagnostics):
+    n = len(regions)
+    ctx = (C.c_void_p * n)(*[m._h.value for m, _ in regions])
+    cnt = (C.c_int64 * n)(*[st.ncell for _, st in regions])
+    ins, sks, outs = (_lib.FimIn * n)(), (_lib.Skip * n)(), (_lib.FimOut * n)()
+    for r, (m, st) in enumerate(regions):
+        ins[r], sks[r], outs[r] = m._structs(st, optional=diagnostics, fresh=fresh)
+    return ctx, cnt, ins, sks, outs
+
+
 def flash_fim_regions(regions, form: str = "batched", stream=None, fresh: bool = False, diagnostics: bool = True):
     """Flashes several PVT regions in one call (``ocpf_flash_fim_regions``):
     ``regions`` is a list of (MixtureCompBatch, CellState) pairs, one per
     region, on one device; fluids may have different component counts. The
-    regions run concurrently on their contexts' streams, joined back into
+    batched forms run as one launch sequence over all regions, or as one
+    sequence per region on the contexts' streams, as the first region's
+    tuning says (``set_tuning`` / ``autotune``); the call is ordered on
     ``stream`` (default: torch's current stream)."""
     torch = _torch()
     n = len(regions)
@@ -351,10 +374,24 @@ def flash_fim_regions(regions, form: str = "batched", stream=None, fresh: bool =
     dev = regions[0][0].device
     if stream is None:
         stream = torch.cuda.current_stream(dev)
-    ctx = (C.c_void_p * n)(*[m._h.value for m, _ in regions])
-    cnt = (C.c_int64 * n)(*[st.ncell for _, st in regions])
-    ins, sks, outs = (_lib.FimIn * n)(), (_lib.Skip * n)(), (_lib.FimOut * n)()
-    for r, (m, st) in enumerate(regions):
-        ins[r], sks[r], outs[r] = m._structs(st, optional=diagnostics, fresh=fresh)
+    ctx, cnt, ins, sks, outs = _region_structs(regions, fresh, diagnostics)
     rc = lib().ocpf_flash_fim_regions(n, ctx, cnt, ins, sks, outs, FORMS[form], C.c_void_p(stream.cuda_stream))
     check(rc, "ocpf_flash_fim_regions")
+
+
+def autotune(regions, form: str = "fast", reps: int = 2, stream=None, fresh: bool = True) -> dict:
+    """``ocpf_autotune`` over (MixtureCompBatch, CellState) pairs (one pair:
+    that context's own launch shape): times every candidate launch shape on
+    the states' inputs without changing them, keeps the fastest in every
+    context and returns it."""
+    torch = _torch()
+    n = len(regions)
+    dev = regions[0][0].device
+    if stream is None:
+        stream = torch.cuda.current_stream(dev)
+    ctx, cnt, ins, sks, _ = _region_structs(regions, fresh, True)
+    best = _lib.Tuning()
+    rc = lib().ocpf_autotune(n, ctx, cnt, ins, sks, FORMS[form], int(reps), C.c_void_p(stream.cuda_stream),
+                             C.byref(best))
+    check(rc, "ocpf_autotune")
+    return {k: getattr(best, k) for k in ("block", "persist_pct", "slow_threads", "schedule", "ms")}

@@ -19,6 +19,8 @@ bRowSizedSdP[n] rows of ncol, row-major, in [n, 3 * ncol * ncol].
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 
 CONV1 = 5.61458
@@ -241,4 +243,70 @@ def assemble(bk, cn, ncom, dt):
         offEB[c] = -bB
         offBE[c] = bE
         diag[int(cn["eId"][c])] += -bE
+    return diag, offEB, offBE
+
+
+# ------------------------------------------- the reference's own assembly
+REF_JAC_LIB = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref", "libocpjac.so")
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_JAC_LIB)
+
+
+def assemble_reference(bk, cn, ncom, dt):
+    """(diag, offEB, offBE) as the reference's own
+    IsoT_FIM::AssembleMatBulksNew scatters them into its LinearSystem
+    (compiled from the reference sources into oracle/_ref/libocpjac.so,
+    ``make -C oracle jac``), on the same Bulk arrays and connections as
+    ``assemble``."""
+    import ctypes as C
+    lib = C.CDLL(REF_JAC_LIB)
+    dp, ip, lp = C.POINTER(C.c_double), C.POINTER(C.c_int32), C.POINTER(C.c_int64)
+
+    class OrcJac(C.Structure):
+        _fields_ = [("nb", C.c_int64), ("ncom", C.c_int32), ("lend", C.c_int32),
+                    ("v", dp), ("poroP", dp), ("vfP", dp), ("vfi", dp),
+                    ("phaseExist", ip), ("pSderExist", ip), ("pVnumCom", ip),
+                    ("Pj", dp), ("depth", dp), ("xi", dp), ("kr", dp), ("mu", dp), ("muP", dp), ("xiP", dp),
+                    ("rhoP", dp), ("xij", dp), ("rhox", dp), ("xix", dp), ("mux", dp), ("dPcj_dS", dp),
+                    ("dKr_dS", dp), ("dSec_dPri", dp), ("nconn", C.c_int64), ("bId", lp), ("eId", lp),
+                    ("area", dp), ("upblock", lp), ("upblock_Rho", dp), ("dt", C.c_double),
+                    ("diag", dp), ("offEB", dp), ("offBE", dp)]
+
+    nb = len(np.asarray(bk["vfP"]))
+    ncol = ncom + 1
+    nconn = len(cn["bId"])
+    keep = []
+
+    def d(a):
+        a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+        keep.append(a)
+        return a.ctypes.data_as(dp)
+
+    def i32(a):
+        a = np.ascontiguousarray(np.asarray(a).astype(np.int32).reshape(-1))
+        keep.append(a)
+        return a.ctypes.data_as(ip)
+
+    def i64(a):
+        a = np.ascontiguousarray(np.asarray(a).astype(np.int64).reshape(-1))
+        keep.append(a)
+        return a.ctypes.data_as(lp)
+
+    sec = np.asarray(bk["dSec_dPri"], dtype=np.float64).reshape(nb, -1)
+    diag = np.zeros((nb, ncol, ncol))
+    offEB = np.zeros((nconn, ncol, ncol))
+    offBE = np.zeros((nconn, ncol, ncol))
+    j = OrcJac(nb, ncom, sec.shape[1], d(bk["v"]), d(bk["poroP"]), d(bk["vfP"]), d(bk["vfi"]),
+               i32(bk["phaseExist"]), i32(bk["pSderExist"]), i32(bk["pVnumCom"]), d(bk["Pj"]), d(bk["depth"]),
+               d(bk["xi"]), d(bk["kr"]), d(bk["mu"]), d(bk["muP"]), d(bk["xiP"]), d(bk["rhoP"]), d(bk["xij"]),
+               d(bk["rhox"]), d(bk["xix"]), d(bk["mux"]), d(bk["dPcj_dS"]), d(bk["dKr_dS"]), d(sec), nconn,
+               i64(cn["bId"]), i64(cn["eId"]), d(cn["area"]), i64(cn["upblock"]), d(cn["upblock_Rho"]), float(dt),
+               diag.ctypes.data_as(dp), offEB.ctypes.data_as(dp), offBE.ctypes.data_as(dp))
+    lib.orc_assemble_bulks.argtypes = [C.POINTER(OrcJac)]
+    lib.orc_assemble_bulks.restype = C.c_int
+    rc = lib.orc_assemble_bulks(C.byref(j))
+    if rc != 0:
+        raise RuntimeError("reference assembly: unexpected row layout")
     return diag, offEB, offBE

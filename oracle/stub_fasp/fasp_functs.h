@@ -1,0 +1,1 @@
+/* TEST INFRASTRUCTURE ONLY: see fasp.h. */

@@ -237,36 +237,6 @@ def test_batched_host_path_and_reserve():
     m.close()
 
 
-def test_regions_call_equals_one_call_per_region():
-    """Four PVT regions of 3, 6, 9 and 12 components in one
-    ocpf_flash_fim_regions call (each on its own stream) give exactly the
-    outputs of one ocpf_flash_fim per region."""
-    torch = _torch()
-    from opencaeporo_b200 import synth
-    from opencaeporo_b200.flash import MixtureCompBatch, flash_fim_regions
-    from opencaeporo_b200.fluid import synthetic_fluid
-    regs, sts, alone = [], [], []
-    for nc, seed in ((3, 31), (6, 61), (9, 91), (12, 121)):
-        fl = synthetic_fluid(nc, seed)
-        w = synth.uniform_states(fl, 3000 + 500 * nc, seed, p_mpa=(2.0, 60.0), t_k=(300.0, 450.0), alpha=0.5)
-        m = MixtureCompBatch(fl)
-        a = m.new_state(len(w["P"]))
-        b = m.new_state(len(w["P"]))
-        for st in (a, b):
-            st.load(w["P"], w["T"], w["Ni"])
-        m.flash_fim(a, form="batched", fresh=True)
-        regs.append((m, b))
-        alone.append(a)
-    flash_fim_regions(regs, form="batched", fresh=True)
-    torch.cuda.synchronize()
-    for (m, b), a in zip(regs, alone):
-        ha, hb = a.to_host(), b.to_host()
-        for k, v in ha.items():
-            if isinstance(v, np.ndarray):
-                np.testing.assert_array_equal(v, hb[k], err_msg=f"nc={m.nc} {k}")
-        m.close()
-
-
 def test_graph_replay_equals_direct_launch():
     """From the second call on, the batched sequence is replayed from a
     captured CUDA graph; replays (also after the arguments change, which
