@@ -382,7 +382,10 @@ int ocpf_autotune(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const oc
  * own streams (OCPF_SCHED_STREAMS), as ctx[0]'s tuning says; the plain form
  * always takes the streams. The call is asynchronous on `stream` like
  * ocpf_flash_fim. skip may be null when no region uses the skip cache.
- * Results equal one ocpf_flash_fim per region, bit for bit. */
+ * With the streams schedule the results equal one ocpf_flash_fim per region
+ * bit for bit; the one-launch kernels evaluate the same expressions but are
+ * compiled apart (the compiler fuses multiply-adds per kernel), so they
+ * agree to rounding. */
 int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell, const ocpf_fim_in* in,
                            ocpf_skip* skip, ocpf_fim_out* out, int form, void* stream);
 
@@ -398,6 +401,14 @@ int ocpf_flash_fim_host(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocp
 /* Device time (ms) of the last ocpf_flash_fim's flash kernel, measured with
  * CUDA events on its stream; waits for that kernel to finish. */
 int ocpf_last_kernel_ms(ocpf_ctx* ctx, float* ms);
+
+/* The parts of the last ocpf_flash_fim in a batched form (device time, ms,
+ * CUDA events on its stream; waits for the call to finish): ms[0] the
+ * sequence up to the split-restart path (set-up, stability tests, the
+ * split's first try), ms[1] the restart path (the few cells whose split
+ * restarts), ms[2] finalize (properties, derivatives, copy-out). Zeros after
+ * a plain-form call. No reference counterpart (measurement utility). */
+int ocpf_last_phase_ms(ocpf_ctx* ctx, float* ms);
 
 /* Number of kernels the last flash call on this context launched (1 for
  * the plain form; for the batched forms the kernel nodes of the replayed

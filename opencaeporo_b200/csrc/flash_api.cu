@@ -29,14 +29,16 @@ using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const
 
 // Batched-form launch sequences (flash_phased_ncN.cu).
 #define OCPF_DECL_PHASED(N)                                                                                 \
-    cudaError_t launch_phased_nc##N(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t, cudaStream_t st); \
+    cudaError_t launch_phased_nc##N(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t, cudaStream_t st, \
+                                    const cudaEvent_t* marks);                                                       \
     int         phased_state_doubles_nc##N();
 OCPF_DECL_PHASED(3)
 OCPF_DECL_PHASED(6)
 OCPF_DECL_PHASED(9)
 OCPF_DECL_PHASED(12)
 
-using PhasedLauncher = cudaError_t (*)(const FluidConst&, const PhasedArgs&, const LaunchTune&, cudaStream_t);
+using PhasedLauncher = cudaError_t (*)(const FluidConst&, const PhasedArgs&, const LaunchTune&, cudaStream_t,
+                                       const cudaEvent_t*);
 
 static PhasedLauncher phased_kernel(int nc, int* ndbl)
 {
@@ -131,6 +133,10 @@ struct ocpf_ctx {
     int         device;
     FluidConst  fc;
     cudaEvent_t ev0, ev1;
+    // the batched sequence's parts in the last timed call: marks[0] before
+    // and marks[1] after its split-restart kernel
+    cudaEvent_t marks[2];
+    bool        marked;
     bool        timed;
     // host-path staging (device) buffers, grown on demand
     int64_t     stage_cap;
@@ -152,6 +158,7 @@ struct ocpf_ctx {
     cudaGraphExec_t gexec;
     PhasedArgs      gkey;
     LaunchTune      gtune;
+    bool            gmark;   // the captured sequence records the part marks
     bool            gvalid;
     // launch shape of the batched forms (ocpf_set_tuning / ocpf_autotune)
     // and, for ocpf_flash_fim_regions led by this context, the schedule
@@ -225,6 +232,7 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->gexec     = nullptr;
     c->gvalid    = false;
     c->gtune     = kDefaultTune;
+    c->gmark     = false;
     c->tune      = kDefaultTune;
     c->sched     = OCPF_SCHED_ONE_LAUNCH;
     c->tune_ms   = 0;
@@ -232,7 +240,9 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->mgkey     = nullptr;
     c->mgtune    = kDefaultTune;
     c->mgkernels = 0;
-    if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    c->marked = false;
+    if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
+        cudaEventCreate(&c->marks[0]) != cudaSuccess || cudaEventCreate(&c->marks[1]) != cudaSuccess) {
         delete c;
         cudaSetDevice(prev);
         return OCPF_ECUDA;
@@ -250,6 +260,8 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     cudaSetDevice(c->device);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
+    cudaEventDestroy(c->marks[0]);
+    cudaEventDestroy(c->marks[1]);
     if (c->stage) cudaFree(c->stage);
     if (c->sub) cudaFree(c->sub);
     if (c->eq) cudaFree(c->eq);
@@ -368,27 +380,29 @@ static void scratch_view(const ocpf_ctx* c, int part, int64_t cap, StateBuf& S, 
 // differ). Work already captured by the caller's own stream capture, and the
 // host path's alternating parts, launch directly.
 static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs& args, cudaStream_t st,
-                                 bool graph_ok)
+                                 bool graph_ok, bool mark)
 {
+    const cudaEvent_t* mk = mark ? c->marks : nullptr;
+    c->marked             = mark;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusInvalidated;
     c->last_kernels = -1;
     const LaunchTune& t = c->tune;
-    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, t, st);
+    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, t, st, mk);
     if (!(c->gvalid && std::memcmp(&c->gkey, &args, sizeof(args)) == 0 &&
-          std::memcmp(&c->gtune, &t, sizeof(t)) == 0)) {
+          std::memcmp(&c->gtune, &t, sizeof(t)) == 0 && c->gmark == mark)) {
         c->gvalid = false;
         if (!c->gs && cudaStreamCreateWithFlags(&c->gs, cudaStreamNonBlocking) != cudaSuccess)
-            return k(c->fc, args, t, st);
+            return k(c->fc, args, t, st, mk);
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(c->gs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            return k(c->fc, args, t, st);
-        const cudaError_t le = k(c->fc, args, t, c->gs);
+            return k(c->fc, args, t, st, mk);
+        const cudaError_t le = k(c->fc, args, t, c->gs, mk);
         const cudaError_t ce = cudaStreamEndCapture(c->gs, &g);
         if (le != cudaSuccess || ce != cudaSuccess || !g) {
             if (g) cudaGraphDestroy(g);
             cudaGetLastError();
-            return k(c->fc, args, t, st);
+            return k(c->fc, args, t, st, mk);
         }
         size_t nn = 0;
         int    nk = 0;
@@ -416,10 +430,11 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
         if (!ok) {
             c->gexec = nullptr;
             cudaGetLastError();
-            return k(c->fc, args, t, st);
+            return k(c->fc, args, t, st, mk);
         }
         c->gkey   = args;
         c->gtune  = t;
+        c->gmark  = mark;
         c->gvalid = true;
     }
     c->last_kernels = c->gkernels;
@@ -441,6 +456,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         if (timed) cudaEventRecord(c->ev0, st);
         e               = k(c->fc, count, stride, in, sk, out, tail, (unsigned)blocks, bs, st);
         c->last_kernels = 1;
+        c->marked       = false;
         if (timed) cudaEventRecord(c->ev1, st);
     } else {
         int            nd = 0;
@@ -466,7 +482,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
             scratch_view(c, part, stride, args.S, args.L);
         }
         if (timed) cudaEventRecord(c->ev0, st);
-        e = launch_phased(c, k, args, st, part < 0);
+        e = launch_phased(c, k, args, st, part < 0, timed && part < 0);
         if (timed) cudaEventRecord(c->ev1, st);
     }
     return e == cudaSuccess ? OCPF_OK : OCPF_ECUDA;
@@ -809,6 +825,19 @@ extern "C" int ocpf_last_launch_count(ocpf_ctx* c, int* n)
 {
     if (!c || !n) return OCPF_EINVAL;
     *n = c->last_kernels;
+    return OCPF_OK;
+}
+
+extern "C" int ocpf_last_phase_ms(ocpf_ctx* c, float* ms)
+{
+    if (!c || !ms) return OCPF_EINVAL;
+    ms[0] = ms[1] = ms[2] = 0;
+    if (!c->timed || !c->marked) return OCPF_OK;
+    if (cudaEventSynchronize(c->ev1) != cudaSuccess) return OCPF_ECUDA;
+    if (cudaEventElapsedTime(&ms[0], c->ev0, c->marks[0]) != cudaSuccess ||
+        cudaEventElapsedTime(&ms[1], c->marks[0], c->marks[1]) != cudaSuccess ||
+        cudaEventElapsedTime(&ms[2], c->marks[1], c->ev1) != cudaSuccess)
+        return OCPF_ECUDA;
     return OCPF_OK;
 }
 

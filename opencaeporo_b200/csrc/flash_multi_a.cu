@@ -26,9 +26,13 @@ KM kpm_sta_prep(const __grid_constant__ MultiFluid MF, const __grid_constant__ M
 {
     OCPF_MULTI_ITEMS(MF, M, (sta_prep_body<NC_>(F_, A_, k)));
 }
+// Only the regions whose context holds a trained network (PH_LEARN) run it;
+// the others have no parameters to read. The test is block-uniform, as the
+// body's barriers need.
 KM kpm_learn(const __grid_constant__ MultiFluid MF, const __grid_constant__ MultiArgs M)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    if (!(M.a[blockIdx.x % (uint32_t)M.n].opts & PH_LEARN) || !M.a[blockIdx.x % (uint32_t)M.n].mlp) return;
     OCPF_MULTI_ITEMS(MF, M, (learn_body<NC_>(F_, A_, *reinterpret_cast<LearnSmem*>(smem_raw))));
 }
 #undef KM

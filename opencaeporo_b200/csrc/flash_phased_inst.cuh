@@ -82,9 +82,11 @@ void OCPF_CAT(split_round_, OCPF_NC)(const FluidConst& F, const PhasedArgs& a, c
 }  // namespace
 
 // The launch sequence of one batched flash (the schedule of flash_phased.cuh)
-// with the context's launch shape.
+// with the context's launch shape. marks (may be null): two events recorded
+// on the stream just before and just after the split-restart kernel, so that
+// a caller can time the sequence's parts.
 cudaError_t OCPF_CAT(launch_phased_nc, OCPF_NC)(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t,
-                                                cudaStream_t st)
+                                                cudaStream_t st, const cudaEvent_t* marks)
 {
     static int sms = 0, occ_s01 = 0, occ_sta = 0, occ_sp = 0, occ_sta32 = 0, occ_spnr = 0, occ_stnr = 0;
     if (!sms) {
@@ -139,10 +141,12 @@ cudaError_t OCPF_CAT(launch_phased_nc, OCPF_NC)(const FluidConst& F, const Phase
         }
     }
     for (int r = 0; r < SPLIT_ROUNDS; r++) OCPF_CAT(split_round_, OCPF_NC)(F, a, st, r, gp, bp, g_sp, g_spnr);
+    if (marks) cudaEventRecord(marks[0], st);
     if (t.slow_threads)
         KP(slow_thread)<<<gp, bp, 0, st>>>(F, a);
     else
         KP(slow)<<<gp, 128, 0, st>>>(F, a);
+    if (marks) cudaEventRecord(marks[1], st);
     if (a.tail.mode & FM_FIMN)
         KP(finalize_fimn)<<<gcell, bp, 0, st>>>(F, a);
     else

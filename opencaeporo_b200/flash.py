@@ -312,6 +312,13 @@ class MixtureCompBatch:
         check(lib().ocpf_last_launch_count(self._h, C.byref(k)), "ocpf_last_launch_count")
         return int(k.value)
 
+    def last_phase_ms(self) -> tuple:
+        """(up to the restart path, restart path, finalize) device ms of the
+        last batched-form flash_fim (ocpf_last_phase_ms)."""
+        ms = (C.c_float * 3)()
+        check(lib().ocpf_last_phase_ms(self._h, ms), "ocpf_last_phase_ms")
+        return tuple(float(v) for v in ms)
+
     def last_kernel_ms(self) -> float:
         ms = C.c_float(0)
         check(lib().ocpf_last_kernel_ms(self._h, C.byref(ms)), "ocpf_last_kernel_ms")
