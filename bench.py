@@ -277,6 +277,7 @@ def our_arm(args):
     # whose split restarts: one dependent chain each), and finalize
     forms = {}
     if not args.no_plain:
+        m.set_part_timing(True)
         for fm in ("batched", "mixed", "fast"):
             parts, tot = [], []
             for s_ in range(3):
@@ -289,7 +290,9 @@ def our_arm(args):
                     tot.append(m.last_kernel_ms())
             p = np.mean(np.array(parts), axis=0)
             forms[fm] = {"ms": float(np.mean(tot)), "to_restart_path_ms": float(p[0]), "restart_path_ms": float(p[1]),
-                         "finalize_ms": float(p[2]), "excluding_restart_path_ms": float(p[0] + p[2])}
+                         "finalize_ms": float(p[2]), "excluding_restart_path_ms": float(p[0] + p[2]),
+                         "launch": "direct (part marks)"}
+        m.set_part_timing(False)
     ms_total, kern_ms = shards.max_over_ranks([ms_total, kern_ms], dev)
     ms_step = ms_total / args.steps
     value = world * n / (ms_step * 1e-3)
@@ -488,6 +491,10 @@ def regions_arm(args):
     from opencaeporo_b200.flash import MixtureCompBatch, autotune, flash_fim_regions
     from opencaeporo_b200.fluid import synthetic_fluid
     per = args.ncell // 2
+    t_start = time.time()
+
+    def note(what):  # progress on stderr: the arm runs for minutes
+        print(f"[regions4 {time.time() - t_start:7.1f} s] {what}", file=sys.stderr, flush=True)
     regs, wls = [], []
     for nc, seed in ((3, 31), (6, 61), (9, 91), (12, 121)):
         fl = synthetic_fluid(nc, seed)
@@ -515,16 +522,23 @@ def regions_arm(args):
                 ts.append(a.elapsed_time(b))
         return float(np.mean(ts))
 
+    note("states loaded")
     form = args.form
     lead = regs[0][0]
     lead.set_tuning(schedule=0)
     t_one_default = timed(lambda: flash_fim_regions(regs, form=form, fresh=True))
+    note(f"one launch {t_one_default:.1f} ms")
     lead.set_tuning(schedule=1)
     t_streams_default = timed(lambda: flash_fim_regions(regs, form=form, fresh=True))
+    note(f"streams {t_streams_default:.1f} ms")
     best = autotune(regs, form=form, reps=1)
+    note(f"autotuned {best}")
     t_tuned = timed(lambda: flash_fim_regions(regs, form=form, fresh=True))
+    note(f"tuned {t_tuned:.1f} ms")
     t_serial = timed(lambda: [m.flash_fim(st, form=form, fresh=True) for m, st in regs])
+    note(f"one call per region {t_serial:.1f} ms")
     t_plain = timed(lambda: [m.flash_fim(st, form="plain", fresh=True) for m, st in regs], steps=1)
+    note(f"plain {t_plain:.1f} ms")
     # outputs of the tuned call, and each fluid's first states against the reference
     flash_fim_regions(regs, form=form, fresh=True)
     torch.cuda.synchronize()
@@ -537,10 +551,12 @@ def regions_arm(args):
         # leave out the states the reference's unbounded restart loop may not
         # end on: those the bounded restatement needs >= 60,000 split steps
         # for (see reference_arm)
+        note(f"nc={fl.nc}: screening the reference sample")
         scr = O.flash_fim("port", fl, w["P"][:ns], w["T"][:ns], w["Ni"][:ns], nthreads=cores)
         ix = np.nonzero(scr["iters"][:, 2] < 60000)[0]
         wv = {k: w[k][ix] for k in ("P", "T", "Ni")}
         sub = {k: v[ix] for k, v in got.items() if isinstance(v, np.ndarray)}
+        note(f"nc={fl.nc}: reference on {len(ix)} states")
         ref = O.flash_fim("reference" if O.available("reference") else "port", fl, wv["P"], wv["T"], wv["Ni"],
                           nthreads=cores)
         left_out = ns - len(ix)

@@ -402,12 +402,20 @@ int ocpf_flash_fim_host(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocp
  * CUDA events on its stream; waits for that kernel to finish. */
 int ocpf_last_kernel_ms(ocpf_ctx* ctx, float* ms);
 
-/* The parts of the last ocpf_flash_fim in a batched form (device time, ms,
- * CUDA events on its stream; waits for the call to finish): ms[0] the
+/* With on != 0, every later ocpf_flash_fim of a batched form records the
+ * events ocpf_last_phase_ms reads, and launches its kernel sequence directly
+ * instead of replaying it from the context's CUDA graph (events recorded by
+ * a replayed graph cannot be timed against each other). Off by default. No
+ * reference counterpart (measurement utility). */
+int ocpf_set_part_timing(ocpf_ctx* ctx, int on);
+
+/* The parts of the last ocpf_flash_fim in a batched form with part timing
+ * on (device time, ms, CUDA events on its stream; waits for the call to
+ * finish; zeros otherwise): ms[0] the
  * sequence up to the split-restart path (set-up, stability tests, the
  * split's first try), ms[1] the restart path (the few cells whose split
- * restarts), ms[2] finalize (properties, derivatives, copy-out). Zeros after
- * a plain-form call. No reference counterpart (measurement utility). */
+ * restarts), ms[2] finalize (properties, derivatives, copy-out). No
+ * reference counterpart (measurement utility). */
 int ocpf_last_phase_ms(ocpf_ctx* ctx, float* ms);
 
 /* Number of kernels the last flash call on this context launched (1 for

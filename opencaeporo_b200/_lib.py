@@ -39,7 +39,8 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_flash_fimn", "ocpf_init_flash_fimn", "ocpf_flash_fim_subset", "ocpf_flash_impec_subset",
            "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count",
            "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian",
-           "ocpf_get_tuning", "ocpf_set_tuning", "ocpf_autotune", "ocpf_last_phase_ms")
+           "ocpf_get_tuning", "ocpf_set_tuning", "ocpf_autotune", "ocpf_last_phase_ms",
+           "ocpf_set_part_timing")
 
 SCHED_ONE_LAUNCH, SCHED_STREAMS = 0, 1  # OCPF_SCHED_*
 
@@ -207,6 +208,8 @@ def lib():
     L.ocpf_flash_fim_regions.argtypes = [C.c_int, C.POINTER(_vp), C.POINTER(C.c_int64), C.POINTER(FimIn),
                                          C.POINTER(Skip), C.POINTER(FimOut), C.c_int, _vp]
     L.ocpf_flash_fim_regions.restype = C.c_int
+    L.ocpf_set_part_timing.argtypes = [_vp, C.c_int]
+    L.ocpf_set_part_timing.restype = C.c_int
     L.ocpf_last_phase_ms.argtypes = [_vp, C.POINTER(C.c_float)]
     L.ocpf_last_phase_ms.restype = C.c_int
     L.ocpf_get_tuning.argtypes = [_vp, C.POINTER(Tuning)]

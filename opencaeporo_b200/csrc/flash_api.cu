@@ -137,6 +137,7 @@ struct ocpf_ctx {
     // and marks[1] after its split-restart kernel
     cudaEvent_t marks[2];
     bool        marked;
+    bool        part_timing;  // ocpf_set_part_timing: record the marks (launches directly)
     bool        timed;
     // host-path staging (device) buffers, grown on demand
     int64_t     stage_cap;
@@ -240,7 +241,8 @@ extern "C" int ocpf_create(const ocpf_fluid* fluid, int device, ocpf_ctx** ctx)
     c->mgkey     = nullptr;
     c->mgtune    = kDefaultTune;
     c->mgkernels = 0;
-    c->marked = false;
+    c->marked      = false;
+    c->part_timing = false;
     if (cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess ||
         cudaEventCreate(&c->marks[0]) != cudaSuccess || cudaEventCreate(&c->marks[1]) != cudaSuccess) {
         delete c;
@@ -382,8 +384,11 @@ static void scratch_view(const ocpf_ctx* c, int part, int64_t cap, StateBuf& S, 
 static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs& args, cudaStream_t st,
                                  bool graph_ok, bool mark)
 {
+    // the part marks are taken on direct launches: events recorded by a
+    // replayed graph's nodes cannot be timed against each other
     const cudaEvent_t* mk = mark ? c->marks : nullptr;
     c->marked             = mark;
+    if (mark) graph_ok = false;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusInvalidated;
     c->last_kernels = -1;
@@ -482,7 +487,7 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
             scratch_view(c, part, stride, args.S, args.L);
         }
         if (timed) cudaEventRecord(c->ev0, st);
-        e = launch_phased(c, k, args, st, part < 0, timed && part < 0);
+        e = launch_phased(c, k, args, st, part < 0, timed && part < 0 && c->part_timing);
         if (timed) cudaEventRecord(c->ev1, st);
     }
     return e == cudaSuccess ? OCPF_OK : OCPF_ECUDA;
@@ -825,6 +830,13 @@ extern "C" int ocpf_last_launch_count(ocpf_ctx* c, int* n)
 {
     if (!c || !n) return OCPF_EINVAL;
     *n = c->last_kernels;
+    return OCPF_OK;
+}
+
+extern "C" int ocpf_set_part_timing(ocpf_ctx* c, int on)
+{
+    if (!c) return OCPF_EINVAL;
+    c->part_timing = on != 0;
     return OCPF_OK;
 }
 

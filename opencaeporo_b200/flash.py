@@ -312,9 +312,14 @@ class MixtureCompBatch:
         check(lib().ocpf_last_launch_count(self._h, C.byref(k)), "ocpf_last_launch_count")
         return int(k.value)
 
+    def set_part_timing(self, on: bool = True):
+        """Records the batched sequence's part marks on later flash_fim calls
+        (direct launches instead of graph replay; ocpf_set_part_timing)."""
+        check(lib().ocpf_set_part_timing(self._h, 1 if on else 0), "ocpf_set_part_timing")
+
     def last_phase_ms(self) -> tuple:
         """(up to the restart path, restart path, finalize) device ms of the
-        last batched-form flash_fim (ocpf_last_phase_ms)."""
+        last batched-form flash_fim with part timing on (ocpf_last_phase_ms)."""
         ms = (C.c_float * 3)()
         check(lib().ocpf_last_phase_ms(self._h, ms), "ocpf_last_phase_ms")
         return tuple(float(v) for v in ms)
