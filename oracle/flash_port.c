@@ -51,6 +51,7 @@ typedef struct {
     int    ssmsta_conflag, nrsta_conflag, ssmsp_conflag, nrsp_conflag;
     double ssmsta_realTol, nrsta_realTol, ssmsp_realTol, nrsp_realTol;
     int    it_ssmsta, it_nrsta, it_ssmsp, it_nrsp, it_rr; /* per call */
+    int    restarts;                                    /* PhaseSplit restarts, per call */
     double ePEC;
     /* state */
     double P, T, Nh, Nt, vf, vfP;
@@ -958,6 +959,7 @@ static void phase_split(Mix* m)
     while (!m->nrsp_conflag && guard++ < 200) {
         split_ssm2(m, 1);
         split_nr(m);
+        m->restarts++;
         if (!check_split(m)) break;
         if (m->ssmsp_conflag) break;
     }
@@ -1427,6 +1429,7 @@ static void flash_fim(Mix* m, double Pin, double Tin, const double* Niin, const 
 {
     const int NC = m->NC, numCom = m->numCom;
     m->it_ssmsta = m->it_nrsta = m->it_ssmsp = m->it_nrsp = m->it_rr = 0;
+    m->restarts  = 0;
     m->lNP = lastNP > 0 ? lastNP - 1 : 0;
     if (m->lNP == 2)
         for (int i = 0; i < NC; i++) m->lKs[i] = xijin[i] / xijin[i + numCom];
@@ -1617,6 +1620,7 @@ static void* run_job(void* arg)
         b->iters[n * 5 + 2] = m->it_ssmsp;
         b->iters[n * 5 + 3] = m->it_nrsp;
         b->iters[n * 5 + 4] = m->it_rr;
+        if (b->restarts) b->restarts[n] = m->restarts;
         if (f->use_skip) {
             b->skip_flag[n]   = m->sk_flag;
             b->skip_minEig[n] = m->sk_minEig;

@@ -50,7 +50,7 @@ _BATCH_FIELDS = [
     ("vfP", _dp), ("vfi", _dp), ("nj", _dp), ("rho", _dp), ("xi", _dp), ("mu", _dp),
     ("rhoP", _dp), ("xiP", _dp), ("muP", _dp), ("xij", _dp), ("rhox", _dp), ("xix", _dp),
     ("mux", _dp), ("dSec_dPri", _dp), ("bRowSizedSdP", _ip), ("pSderExist", _ip),
-    ("pVnumCom", _ip), ("ePEC", _dp), ("ftype", _ip), ("NPhc", _ip), ("iters", _ip),
+    ("pVnumCom", _ip), ("ePEC", _dp), ("ftype", _ip), ("NPhc", _ip), ("iters", _ip), ("restarts", _ip),
 ]
 
 
@@ -224,7 +224,7 @@ def _prepare(fluid, P, T, Ni, S, lastNP, xij, skip):
         "bRowSizedSdP": np.full(n, -1, np.int32), "pSderExist": np.full((n, NP), -1, np.int32),
         "pVnumCom": np.full((n, NP), -1, np.int32), "ePEC": nan(n),
         "ftype": np.full(n, -1, np.int32), "NPhc": np.full(n, -1, np.int32),
-        "iters": np.full((n, 5), -1, np.int32),
+        "iters": np.full((n, 5), -1, np.int32), "restarts": np.full(n, -1, np.int32),
     }
     b = OrcBatch()
     b.n = n

@@ -103,6 +103,7 @@ typedef struct {
     int32_t* ftype;        /* [n] */
     int32_t* NPhc;         /* [n] hydrocarbon phase count */
     int32_t* iters;        /* [n*5] SSMSTA, NRSTA, SSMSP, NRSP, RR iterations */
+    int32_t* restarts;     /* [n] PhaseSplit restarts (the restatement only; may be NULL) */
 } orc_batch;
 
 /* Runs FlashFIM over the batch with nthreads host threads (each owning its own

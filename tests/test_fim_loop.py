@@ -5,11 +5,17 @@ the plain FP64 form iteration by iteration, every iteration's flash agrees
 with the reference's own FlashFIM given the same warm-start state, and
 KrPc, the upstream choice and the Jacobian's bulk part run after the flash
 on its device arrays."""
+import os
+import sys
+
 import numpy as np
 import pytest
 
-from oracle import compare as CMP
-from oracle import oracle as O
+if __name__ == "__main__":  # run as a script (the full-size check below)
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+from oracle import compare as CMP  # noqa: E402
+from oracle import oracle as O  # noqa: E402
 
 GRID = (24, 40, 12)
 
@@ -38,8 +44,8 @@ def check_against_reference(fl, before, after, kind="reference"):
     converged cells off by more than 1e-8 without the reference itself
     moving by more than 1e-9 under 1-ulp input perturbations, cells beyond
     10x the reference's own sensitivity). States the bounded restatement
-    needs >= 60,000 split steps for are left out (the reference's restart
-    loop has no bound)."""
+    needs >= 60,000 split steps or >= 150 restarts for are left out (the
+    reference's restart loop has no bound)."""
     n = len(before["P"])
     nc = fl.nc
     skip0 = {k: np.ascontiguousarray(v) for k, v in before["skip"].items()}
@@ -55,7 +61,7 @@ def check_against_reference(fl, before, after, kind="reference"):
                            xij=warm["xij"][cells], skip=sk, nthreads=0)
 
     scr = flash("port", np.arange(n))
-    keep = np.nonzero(scr["iters"][:, 2] < 60000)[0]
+    keep = np.nonzero((scr["iters"][:, 2] < 60000) & (scr["restarts"] < 150))[0]
     r = flash(kind, keep)
     got = {k: v[keep] for k, v in after.items()}
     got["xij"] = got["xij"].reshape(len(keep), 3, nc + 1)
@@ -123,9 +129,6 @@ def main():
     """
     import argparse
     import json
-    import os
-    import sys
-    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
     from opencaeporo_b200.fim_loop import run
     from opencaeporo_b200.workload import bench_fluid
     ap = argparse.ArgumentParser()
