@@ -843,9 +843,6 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
     const uint32_t  n    = a.L.len(L_SLOW);
     const uint32_t  nw   = (vgrid(a) * blockDim.x) >> 5;
     const bool      lead = (threadIdx.x & 31) == 0;
-    // the Rachford-Rice terms' exchange rows of each warp (blocks of 128)
-    __shared__ double rr_rows[4][64];
-    double* rows = rr_rows[(threadIdx.x >> 5) & 3];
     for (uint32_t k = (vblock(a) * blockDim.x + threadIdx.x) >> 5; k < n; k += nw) {
         const int64_t c = a.L.item(L_SLOW, k);
         CellFlash<NC> f(F);
@@ -856,7 +853,7 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
         WarpSplit<NC> w(f);
         int           guard = S.I(IF_GUARD, c);
         while (true) {
-            w.split_ssm2(true, rows);
+            w.split_ssm2(true);
             w.split_nr();
             if (!f.check_split()) break;
             if (f.ssmsp_conflag || f.nrsp_conflag) break;

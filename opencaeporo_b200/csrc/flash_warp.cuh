@@ -61,13 +61,9 @@ struct WarpSplit {
 
     // RachfordRice2, src/MixtureComp.cpp:1907-1959 (CellFlash::rachford_rice2):
     // lane i forms component i's residual term, lane 16 + i its Jacobian
-    // term from the lane's own K_i (Kq) and z_i (zq); the terms go through
-    // the warp's shared-memory rows (two rows of 32, used in turn, so one
-    // warp barrier per Newton step suffices) and every lane sums them in the
-    // reference's order.
-    __device__ void rachford_rice2(double Kq, double zq, double* rows)
+    // term; the sums run on every lane in the reference's order.
+    __device__ void rachford_rice2()
     {
-        __syncwarp();  // every lane has read the rows of the previous call
         double Kmin = f.Ks[0], Kmax = f.Ks[0];
 #pragma unroll
         for (int i = 1; i < NC; i++) {
@@ -80,20 +76,18 @@ struct WarpSplit {
         double       v     = 0.5 * (numin + numax);
         // loop-invariant parts of component q's terms, formed as the
         // one-thread form forms them: z km1 / tmp and z km1 km1 / (tmp tmp)
-        const double km1 = Kq - 1;
-        const double zk  = zq * km1;
+        const double km1 = pick(f.Ks) - 1;
+        const double zk  = pick(f.zi) * km1;
         const double num = half ? zk * km1 : zk;
         int          iter = 0;
         while (true) {
-            double* row       = rows + ((iter & 1) << 5);
             const double tmp  = 1 + v * km1;
-            row[lane]         = num / (half ? tmp * tmp : tmp);
-            __syncwarp();
-            double rj = 0, J = 0;
+            const double term = num / (half ? tmp * tmp : tmp);
+            double       rj = 0, J = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
-                rj += row[i];
-                J -= row[16 + i];
+                rj += __shfl_sync(WARP_ALL, term, i);
+                J -= __shfl_sync(WARP_ALL, term, 16 + i);
             }
             if (fabs(rj) < f.F.rr_tol || iter > f.F.rr_maxit) break;
             const double dnuj  = -rj / J;
@@ -183,16 +177,8 @@ struct WarpSplit {
     }
 
     // SplitSSM2 with UpdateXRR, src/MixtureComp.cpp:1847-1903, 2030-2043
-    // (CellFlash::split_ssm2 with the pieces above). During the iterations
-    // lane 16 h + q keeps only component q of phase h -- K_q, z_q, x_hq,
-    // phi_hq, f_hq -- instead of the whole cell: the compositions, the
-    // fugacities and the K update stay on their lanes, and only the phase's
-    // composition (for its mixing rule), the fugacity ratios' partners
-    // across the halves, the residual's terms and the new K travel. Every
-    // value is the one the whole-state form computes (same expressions, same
-    // order of the sums). The cell state is written back once at the end.
-    // `rows`: this warp's 64 doubles of shared memory.
-    __device__ void split_ssm2(bool restart, double* rows)
+    // (CellFlash::split_ssm2 with the pieces above).
+    __device__ void split_ssm2(bool restart)
     {
         f.ssmsp_conflag = true;
         double Se       = 1;
@@ -206,51 +192,27 @@ struct WarpSplit {
             Stol *= 1e-1;
             maxIt *= 2;
         }
-        if (!(Se > Stol)) {  // no iteration at all (a tolerance of 1 or more)
-            f.ssmsp_realTol = sqrt(Se);
-            return;
-        }
-        const double zq = pick(f.zi);
-        double       Kq = pick(f.Ks);
-        double       xq = 0, phq = 0, aj = 0, bj = 0, zj = 0;
-        int          iter = 0;
-        do {
-            rachford_rice2(Kq, zq, rows);
-            // UpdateXRR: x_1q = z_q / (1 + nu (K_q - 1)), x_0q = K_q x_1q
-            const double tmp = 1 + f.nu[0] * (Kq - 1);
-            const double x1  = zq / tmp;
-            xq               = half ? x1 : Kq * x1;
-            // CalFugPhi of phase `half` on its half-warp
-            double xj[NC];
-#pragma unroll
-            for (int k = 0; k < NC; k++) xj[k] = __shfl_sync(WARP_ALL, xq, (lane & 16) + k);
-            phq              = fug_lane(xj, aj, bj, zj);
-            const double fgq = phq * xq * f.P;
-            // lane q: f_1q / f_0q (its residual term); lane 16 + q: phi_1q /
-            // phi_0q (the new K_q): each takes its partner from the other half
-            const double recv = __shfl_xor_sync(WARP_ALL, half ? fgq : phq, 16);
-            const double quo  = (half ? phq : recv) / (half ? recv : fgq);
-            const double v    = half ? quo : sq(quo - 1);
-            Se                = 0;
+        int iter = 0;
+        while (Se > Stol) {
+            rachford_rice2();
+            update_x();
+            fug_phi_all();
+            // lane i: component i's squared fugacity-ratio residual; lane
+            // 16 + i: its new K (one division on every lane)
+            const double quo = (half ? pick(f.phi[1]) : pick(f.fug[1])) / (half ? pick(f.phi[0]) : pick(f.fug[0]));
+            const double v   = half ? quo : sq(quo - 1);
+            Se               = 0;
 #pragma unroll
             for (int i = 0; i < NC; i++) {
                 Se      = __dadd_rn(Se, __shfl_sync(WARP_ALL, v, i));
                 f.Ks[i] = __shfl_sync(WARP_ALL, v, 16 + i);
             }
-            const double other = __shfl_xor_sync(WARP_ALL, v, 16);
-            Kq                 = half ? v : other;
             iter++;
             if (iter > maxIt) {
                 f.ssmsp_conflag = false;
                 break;
             }
-        } while (Se > Stol);
-        // the whole cell on every lane again, for SplitNR and CheckSplit
-#pragma unroll
-        for (int j = 0; j < 2; j++)
-#pragma unroll
-            for (int i = 0; i < NC; i++) f.x[j][i] = __shfl_sync(WARP_ALL, xq, 16 * j + i);
-        share_phases(phq, aj, bj, zj);
+        }
         f.ssmsp_realTol = sqrt(Se);
         f.it_ssmsp += iter;
     }
