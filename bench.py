@@ -814,6 +814,23 @@ def entries_arm(args):
                          "bytes_per_launch": jbytes, "peak_source": peak_src},
             "parity": "bit-identical to the restatement on the 8x8x8 test grid (tests/test_fim_jacobian.py)"}
         g.close()
+    # the last-time-step copies of the flash's arrays and the skip cache
+    # (IsoT_FIM::UpdateLastTimeStep / ResetToLastTimeStep): one copy launch,
+    # HBM-bound (each byte read once and written once)
+    last = m.new_last(st)
+    t_save = timed(lambda: None, lambda: m.update_last_step(st, last, inputs=False))
+    t_reset = timed(lambda: None, lambda: m.reset_to_last_step(st, last, inputs=False))
+    torch.cuda.synchronize()
+    bits = lambda x, y: torch.equal(x.view(torch.uint8), y.view(torch.uint8))  # NaN-safe
+    same = all(bits(st.out[k], last.out[k]) for k in st.out) and all(bits(st.skip[k], last.skip[k]) for k in st.skip)
+    cbytes = sum(t.numel() * t.element_size() for t in list(st.out.values()) + list(st.skip.values()))
+    res["update_last_step"] = {
+        "value": n / (t_save * 1e-3), "unit": "cells/s", "ms_per_step": t_save, "reset_ms": t_reset,
+        "identical_after_copy": bool(same),
+        "roofline": {"bound": "hbm", "achieved": 2 * cbytes / (t_save * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": (2 * cbytes / (t_save * 1e-3) / 1e9 / peak) if peak else None,
+                     "bytes_per_launch": 2 * cbytes, "peak_source": peak_src}}
+    del last
     fu.close()
     m.close()
     print(json.dumps({

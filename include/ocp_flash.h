@@ -398,6 +398,35 @@ int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell,
 int ocpf_flash_fim_host(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
                         ocpf_fim_out* out, int form);
 
+/* ---- Last-time-step copies -------------------------------------------
+ * IsoT_FIM::UpdateLastTimeStep (src/OCPFluidMethod.cpp:2915-2960) keeps a
+ * copy of every Bulk array the flash writes, and ResetToLastTimeStep
+ * (:2859-2897) puts it back when a time step is cut; SkipStaAnaly does the
+ * same for its cache (src/AcceleratePVT.cpp:122-138). Here `last` and
+ * `last_skip` are the caller's arrays in the layouts of ocpf_fim_out and
+ * ocpf_skip for the same ncell and nc (hydrocarbon components):
+ *   ocpf_update_last_step:   last <- cur, last_skip <- skip;
+ *   ocpf_reset_to_last_step: cur <- last, skip <- last_skip.
+ * Every field set in both structs is copied, the optional diagnostics
+ * included, dSec_dPri whole ([3*(numCom+1)^2][ncell]); a field set in only
+ * one of the two is OCPF_EINVAL, as are skip and last_skip not both set or
+ * both null and a source overlapping its destination. One kernel launch
+ * copies all the arrays, asynchronously on `stream`. The Bulk arrays
+ * outside the flash (P, Ni, Pj, Pc, kr and the rock's) are the caller's:
+ * ocpf_copy_arrays copies any of them in one launch as well. */
+#define OCPF_COPY_MAX 64 /* array pairs of one copy launch */
+int ocpf_update_last_step(int nc, int64_t ncell, const ocpf_fim_out* cur, const ocpf_skip* skip,
+                          const ocpf_fim_out* last, const ocpf_skip* last_skip, void* stream);
+int ocpf_reset_to_last_step(int nc, int64_t ncell, const ocpf_fim_out* cur, const ocpf_skip* skip,
+                            const ocpf_fim_out* last, const ocpf_skip* last_skip, void* stream);
+
+/* Copies narr (at most OCPF_COPY_MAX) device arrays, src[i] to dst[i] of
+ * bytes[i] bytes, in one kernel launch on `stream`. Arrays of 0 bytes and
+ * pairs with dst[i] == src[i] are skipped; a null pointer of a non-empty
+ * pair, a negative size or a source overlapping its destination is
+ * OCPF_EINVAL (and nothing is launched). */
+int ocpf_copy_arrays(int narr, void* const* dst, const void* const* src, const int64_t* bytes, void* stream);
+
 /* Device time (ms) of the last ocpf_flash_fim's flash kernel, measured with
  * CUDA events on its stream; waits for that kernel to finish. */
 int ocpf_last_kernel_ms(ocpf_ctx* ctx, float* ms);

@@ -40,7 +40,9 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count",
            "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian",
            "ocpf_get_tuning", "ocpf_set_tuning", "ocpf_autotune", "ocpf_last_phase_ms",
-           "ocpf_set_part_timing")
+           "ocpf_set_part_timing", "ocpf_update_last_step", "ocpf_reset_to_last_step", "ocpf_copy_arrays")
+
+COPY_MAX = 64  # OCPF_COPY_MAX
 
 SCHED_ONE_LAUNCH, SCHED_STREAMS = 0, 1  # OCPF_SCHED_*
 
@@ -212,6 +214,12 @@ def lib():
     L.ocpf_set_part_timing.restype = C.c_int
     L.ocpf_last_phase_ms.argtypes = [_vp, C.POINTER(C.c_float)]
     L.ocpf_last_phase_ms.restype = C.c_int
+    for name in ("ocpf_update_last_step", "ocpf_reset_to_last_step"):
+        getattr(L, name).argtypes = [C.c_int, C.c_int64, C.POINTER(FimOut), C.POINTER(Skip), C.POINTER(FimOut),
+                                     C.POINTER(Skip), _vp]
+        getattr(L, name).restype = C.c_int
+    L.ocpf_copy_arrays.argtypes = [C.c_int, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(C.c_int64), _vp]
+    L.ocpf_copy_arrays.restype = C.c_int
     L.ocpf_get_tuning.argtypes = [_vp, C.POINTER(Tuning)]
     L.ocpf_get_tuning.restype = C.c_int
     L.ocpf_set_tuning.argtypes = [_vp, C.POINTER(Tuning)]

@@ -329,6 +329,39 @@ class MixtureCompBatch:
         check(lib().ocpf_last_kernel_ms(self._h, C.byref(ms)), "ocpf_last_kernel_ms")
         return float(ms.value)
 
+    # ------------------------------------------------------ last time step
+    def new_last(self, st: CellState) -> CellState:
+        """Device arrays for the last-time-step copy of ``st`` (Bulk's ``l*``
+        arrays and SkipStaAnaly's ``l*`` cache), same shapes."""
+        return self.new_state(st.ncell)
+
+    def _step_copy(self, fn: str, st: CellState, last: CellState, inputs: bool, stream):
+        torch = _torch()
+        if last.ncell != st.ncell or last.nc != st.nc:
+            raise ValueError("last-step state of another shape")
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        s = C.c_void_p(stream.cuda_stream)
+        _, sk, out = self._structs(st)
+        _, lsk, lout = self._structs(last)
+        check(getattr(lib(), fn)(self.nc, st.ncell, C.byref(out), C.byref(sk), C.byref(lout), C.byref(lsk), s), fn)
+        if inputs:
+            pairs = [(last.P, st.P), (last.Ni, st.Ni)]
+            copy_arrays(pairs if fn == "ocpf_update_last_step" else [(b, a) for a, b in pairs], stream)
+
+    def update_last_step(self, st: CellState, last: CellState, inputs: bool = True, stream=None):
+        """IsoT_FIM::UpdateLastTimeStep for the flash's arrays
+        (``src/OCPFluidMethod.cpp:2915-2960``) and the skip cache
+        (``src/AcceleratePVT.cpp:131-138``): ``last`` <- ``st``; with
+        ``inputs`` also P and Ni (``lP``, ``lNi``). Asynchronous."""
+        self._step_copy("ocpf_update_last_step", st, last, inputs, stream)
+
+    def reset_to_last_step(self, st: CellState, last: CellState, inputs: bool = True, stream=None):
+        """IsoT_FIM::ResetToLastTimeStep (``src/OCPFluidMethod.cpp:2859-2897``)
+        and SkipStaAnaly::ResetToLastTimeStep (``src/AcceleratePVT.cpp:122-129``):
+        ``st`` <- ``last``. Asynchronous."""
+        self._step_copy("ocpf_reset_to_last_step", st, last, inputs, stream)
+
     # ------------------------------------------------------------- host path
     def new_host_state(self, ncell: int, pinned: bool = True) -> dict:
         """Host SoA buffers for :meth:`flash_fim_host` (pinned if requested)."""
@@ -389,6 +422,29 @@ def flash_fim_regions(regions, form: str = "batched", stream=None, fresh: bool =
     ctx, cnt, ins, sks, outs = _region_structs(regions, fresh, diagnostics)
     rc = lib().ocpf_flash_fim_regions(n, ctx, cnt, ins, sks, outs, FORMS[form], C.c_void_p(stream.cuda_stream))
     check(rc, "ocpf_flash_fim_regions")
+
+
+def copy_arrays(pairs, stream=None):
+    """``ocpf_copy_arrays``: copies each (dst, src) pair of device tensors
+    (same number of bytes) in one kernel launch, asynchronously."""
+    torch = _torch()
+    pairs = list(pairs)
+    if not pairs:
+        return
+    if len(pairs) > _lib.COPY_MAX:
+        raise ValueError(f"at most {_lib.COPY_MAX} pairs per launch")
+    for d, s in pairs:
+        if d.numel() * d.element_size() != s.numel() * s.element_size():
+            raise ValueError("pair of different sizes")
+        if not (d.is_contiguous() and s.is_contiguous()):
+            raise ValueError("contiguous tensors only")
+    if stream is None:
+        stream = torch.cuda.current_stream(pairs[0][0].device)
+    n = len(pairs)
+    dst = (C.c_void_p * n)(*[d.data_ptr() for d, _ in pairs])
+    src = (C.c_void_p * n)(*[s.data_ptr() for _, s in pairs])
+    nb = (C.c_int64 * n)(*[s.numel() * s.element_size() for _, s in pairs])
+    check(lib().ocpf_copy_arrays(n, dst, src, nb, C.c_void_p(stream.cuda_stream)), "ocpf_copy_arrays")
 
 
 def autotune(regions, form: str = "fast", reps: int = 2, stream=None, fresh: bool = True) -> dict:
