@@ -524,6 +524,17 @@ typedef struct {
     const double* sgof;
 } ocpf_satfunc;
 
+/* The SWFN, SGFN and SOF3 tables of one saturation region (3 columns,
+ * row-major, as the keywords list them): Sw, krw, Pcow; Sg, krg, Pcgo;
+ * So, krow, krog. The reference uses this family (FlowUnit_ODGW02) as soon
+ * as SOF3 is given (src/Bulk.cpp:271-279). */
+typedef struct {
+    int32_t       nrow_swfn, nrow_sgfn, nrow_sof3, pad;
+    const double* swfn;
+    const double* sgfn;
+    const double* sof3;
+} ocpf_satfunc3;
+
 typedef struct ocpf_krpc ocpf_krpc;
 
 /* Device inputs: P [ncell], the flash's S [3][ncell] (oil, gas, water), and
@@ -550,6 +561,15 @@ typedef struct {
  * fewer than 2 rows or a decreasing first column, OCPF_EUNSUPPORTED when
  * the tables exceed 48 KB together. */
 int ocpf_krpc_create(const ocpf_satfunc* regions, int nregion, int device, ocpf_krpc** out);
+
+/* The same for FlowUnit_ODGW02 (src/FlowUnit.cpp:522-535): ocpf_cal_krpc on
+ * the handle then evaluates SWFN at S_w, SGFN at S_g and SOF3 at S_o, with
+ * the reference's two oil models kept as they are: with derivative outputs
+ * (CalKrPcDeriv, :569-652) Stone II from kroMax = SOF3's last krow, whose
+ * derivative enters dKr_dS[0] (d kro / d S_o) alone; without (CalKrPc,
+ * :537-567) the default model (Sg krog + (Sw - Swco) krow) / (Sg + Sw - Swco),
+ * kroMax where that denominator is at most 1e-8. Same error codes. */
+int ocpf_krpc_create_sof3(const ocpf_satfunc3* regions, int nregion, int device, ocpf_krpc** out);
 int ocpf_krpc_destroy(ocpf_krpc* k);
 
 /* For every cell: SWOF at S_w and SGOF at S_g (OCPTable::Eval_All, linear

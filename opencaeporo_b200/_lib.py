@@ -40,7 +40,8 @@ EXPORTS = ("ocpf_version", "ocpf_status_string", "ocpf_create", "ocpf_destroy",
            "ocpf_krpc_create", "ocpf_krpc_destroy", "ocpf_cal_krpc", "ocpf_last_launch_count",
            "ocpf_conn_create", "ocpf_conn_destroy", "ocpf_fim_upwind", "ocpf_fim_jacobian",
            "ocpf_get_tuning", "ocpf_set_tuning", "ocpf_autotune", "ocpf_last_phase_ms",
-           "ocpf_set_part_timing", "ocpf_update_last_step", "ocpf_reset_to_last_step", "ocpf_copy_arrays")
+           "ocpf_set_part_timing", "ocpf_update_last_step", "ocpf_reset_to_last_step", "ocpf_copy_arrays",
+           "ocpf_krpc_create_sof3")
 
 COPY_MAX = 64  # OCPF_COPY_MAX
 
@@ -103,6 +104,12 @@ KRPC_OUT_FIELDS = ("kr", "Pc", "Pj", "dKr_dS", "dPcj_dS")
 
 class Satfunc(C.Structure):
     _fields_ = [("nrow_swof", C.c_int32), ("nrow_sgof", C.c_int32), ("swof", _vp), ("sgof", _vp)]
+
+
+class Satfunc3(C.Structure):
+    """ocpf_satfunc3 (SWFN, SGFN, SOF3)"""
+    _fields_ = [("nrow_swfn", C.c_int32), ("nrow_sgfn", C.c_int32), ("nrow_sof3", C.c_int32), ("pad", C.c_int32),
+                ("swfn", _vp), ("sgfn", _vp), ("sof3", _vp)]
 
 
 class KrpcIn(C.Structure):
@@ -261,6 +268,8 @@ def lib():
     L.ocpf_last_launch_count.argtypes = [_vp, C.POINTER(C.c_int)]
     L.ocpf_last_launch_count.restype = C.c_int
     L.ocpf_krpc_create.argtypes = [C.POINTER(Satfunc), C.c_int, C.c_int, C.POINTER(_vp)]
+    L.ocpf_krpc_create_sof3.argtypes = [C.POINTER(Satfunc3), C.c_int, C.c_int, C.POINTER(_vp)]
+    L.ocpf_krpc_create_sof3.restype = C.c_int
     L.ocpf_krpc_create.restype = C.c_int
     L.ocpf_krpc_destroy.argtypes = [_vp]
     L.ocpf_krpc_destroy.restype = C.c_int

@@ -1,13 +1,16 @@
 """Relative permeability and capillary pressure after the flash: the host
 mirror of ``ocpf_cal_krpc``, the batched IsoT_FIM::CalKrPc /
 IsoT_IMPEC::CalKrPc (src/OCPFluidMethod.cpp:1189-1199, 311-319) for the
-compositional model's default flow unit, FlowUnit_ODGW01
-(src/FlowUnit.cpp:183-349).
+compositional model's flow units: the default FlowUnit_ODGW01
+(src/FlowUnit.cpp:183-349) and FlowUnit_ODGW02 (:522-671), which the
+reference selects when SOF3 is given (src/Bulk.cpp:271-279).
 
-Tables are given as the SWOF / SGOF keywords list them: rows of
-(Sw, krw, krow, Pcow) and (Sg, krg, krog, Pcgo), one pair per saturation
-region. Device arrays are field-major like the flash's: P [n], S [3, n]
-(the flash's ``out['S']``), kr / Pc / Pj [3, n], dKr_dS / dPcj_dS [9, n].
+Tables are given as the keywords list them, one tuple per saturation
+region: (SWOF, SGOF) with rows (Sw, krw, krow, Pcow) and (Sg, krg, krog,
+Pcgo), or (SWFN, SGFN, SOF3) with rows (Sw, krw, Pcow), (Sg, krg, Pcgo) and
+(So, krow, krog). Device arrays are field-major like the flash's: P [n],
+S [3, n] (the flash's ``out['S']``), kr / Pc / Pj [3, n], dKr_dS / dPcj_dS
+[9, n].
 """
 from __future__ import annotations
 
@@ -25,19 +28,36 @@ def _torch():
 
 
 class FlowUnitBatch:
-    """The FlowUnit_ODGW01 of every saturation region on one GPU."""
+    """The flow unit of every saturation region on one GPU: FlowUnit_ODGW01
+    for (SWOF, SGOF) regions, FlowUnit_ODGW02 for (SWFN, SGFN, SOF3) ones
+    (one family for all regions, as the reference's SATmode is)."""
 
     def __init__(self, regions, device: int = 0):
         self.device = device
         self._keep = []
-        regs = (_lib.Satfunc * len(regions))()
-        for i, (swof, sgof) in enumerate(regions):
-            w = np.ascontiguousarray(swof, dtype=np.float64).reshape(-1, 4)
-            g = np.ascontiguousarray(sgof, dtype=np.float64).reshape(-1, 4)
-            self._keep += [w, g]
-            regs[i] = _lib.Satfunc(len(w), len(g), w.ctypes.data, g.ctypes.data)
+        kinds = {len(r) for r in regions}
+        if kinds == {2}:
+            self.family = "swof"
+            regs = (_lib.Satfunc * len(regions))()
+            for i, (swof, sgof) in enumerate(regions):
+                w = np.ascontiguousarray(swof, dtype=np.float64).reshape(-1, 4)
+                g = np.ascontiguousarray(sgof, dtype=np.float64).reshape(-1, 4)
+                self._keep += [w, g]
+                regs[i] = _lib.Satfunc(len(w), len(g), w.ctypes.data, g.ctypes.data)
+            create, name = lib().ocpf_krpc_create, "ocpf_krpc_create"
+        elif kinds == {3}:
+            self.family = "sof3"
+            regs = (_lib.Satfunc3 * len(regions))()
+            for i, tabs in enumerate(regions):
+                t = [np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 3) for x in tabs]
+                self._keep += t
+                regs[i] = _lib.Satfunc3(len(t[0]), len(t[1]), len(t[2]), 0, t[0].ctypes.data, t[1].ctypes.data,
+                                        t[2].ctypes.data)
+            create, name = lib().ocpf_krpc_create_sof3, "ocpf_krpc_create_sof3"
+        else:
+            raise ValueError("regions must all be (SWOF, SGOF) or all (SWFN, SGFN, SOF3)")
         h = C.c_void_p()
-        check(lib().ocpf_krpc_create(regs, len(regions), int(device), C.byref(h)), "ocpf_krpc_create")
+        check(create(regs, len(regions), int(device), C.byref(h)), name)
         self._h = h
 
     def close(self):

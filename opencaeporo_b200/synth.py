@@ -153,3 +153,19 @@ def corey_tables(seed, swc=0.15, sorw=0.2, sgc=0.05, sorg=0.1, nrow=12, pc_scale
     pcgo = pc_scale[1] * sg / sg[-1]
     sgof = np.stack([sg, krg, krog, pcgo], axis=1)
     return swof, sgof
+
+
+def corey_fn_tables(seed, swc=0.15, sorw=0.2, sgc=0.05, sorg=0.1, nrow=12, pc_scale=(4.0, 1.5)):
+    """Seeded synthetic SWFN / SGFN / SOF3 rows (the saturation-function
+    family of keywords): (Sw, krw, Pcow), (Sg, krg, Pcgo) and (So, krow,
+    krog), Corey-type curves with random exponents and an oil end point
+    kroMax below one."""
+    swof, sgof = corey_tables(seed, swc, sorw, sgc, sorg, nrow, pc_scale)
+    rng = np.random.default_rng(seed + 7919)
+    now, nog = rng.uniform(1.5, 4.0, 2)
+    kmax = rng.uniform(0.6, 1.0)
+    so = np.linspace(0.0, 1.0 - swc, nrow)
+    krow = kmax * np.clip((so - sorw) / (1 - swc - sorw), 0, 1) ** now
+    krog = kmax * np.clip((so - sorg) / (1 - swc - sorg), 0, 1) ** nog
+    sof3 = np.stack([so, krow, krog], axis=1)
+    return swof[:, [0, 1, 3]].copy(), sgof[:, [0, 1, 3]].copy(), sof3

@@ -175,6 +175,20 @@ typedef struct {
  * relative permeability). The reference oracle only. */
 int orc_krpc(int nreg, const orc_satfunc* reg, const orc_krpc_batch* batch, int nthreads, double* seconds);
 
+/* Saturation functions of one region in the SWFN / SGFN / SOF3 family
+ * (row-major, 3 columns): Sw, krw, Pcow; Sg, krg, Pcgo; So, krow, krog. */
+typedef struct {
+    int32_t       nrow_swfn, nrow_sgfn, nrow_sof3, pad;
+    const double* swfn;
+    const double* sgfn;
+    const double* sof3;
+} orc_satfunc3;
+
+/* The same with FlowUnit_ODGW02 (src/FlowUnit.cpp:522-671), the flow unit
+ * the reference selects when SOF3 is given (src/Bulk.cpp:271-279). The
+ * reference oracle only. */
+int orc_krpc_sof3(int nreg, const orc_satfunc3* reg, const orc_krpc_batch* batch, int nthreads, double* seconds);
+
 /* Identifies the implementation: "reference" or "port". */
 const char* orc_kind(void);
 

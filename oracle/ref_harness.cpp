@@ -447,6 +447,57 @@ extern "C" int orc_krpc(int nreg, const orc_satfunc* reg, const orc_krpc_batch* 
     });
 }
 
+// The same over FlowUnit_ODGW02 units built from SWFN / SGFN / SOF3 tables
+// (src/FlowUnit.cpp:522-535), one per region and thread.
+static void run_chunk_krpc_sof3(int nreg, const orc_satfunc3* reg, const orc_krpc_batch* b, int64_t lo,
+                                int64_t hi, double* secs)
+{
+    ParamReservoir rs;
+    auto cols = [](const double* rows, int nrow) {
+        std::vector<std::vector<OCP_DBL>> c(3, std::vector<OCP_DBL>(nrow));
+        for (int r = 0; r < nrow; r++)
+            for (int k = 0; k < 3; k++) c[k][r] = rows[r * 3 + k];
+        return c;
+    };
+    for (int i = 0; i < nreg; i++) {
+        rs.SWFN_T.data.push_back(cols(reg[i].swfn, reg[i].nrow_swfn));
+        rs.SGFN_T.data.push_back(cols(reg[i].sgfn, reg[i].nrow_sgfn));
+        rs.SOF3_T.data.push_back(cols(reg[i].sof3, reg[i].nrow_sof3));
+    }
+    std::vector<FlowUnit_ODGW02*> fu;
+    for (int i = 0; i < nreg; i++) fu.push_back(new FlowUnit_ODGW02(rs, static_cast<USI>(i)));
+    auto t0 = std::chrono::steady_clock::now();
+    for (int64_t n = lo; n < hi; n++) {
+        const int r = b->satnum ? b->satnum[n] : 0;
+        if (b->deriv)
+            fu[r]->CalKrPcDeriv(b->S + 3 * n, b->kr + 3 * n, b->Pc + 3 * n, b->dKr_dS + 9 * n, b->dPcj_dS + 9 * n,
+                                static_cast<OCP_USI>(n));
+        else
+            fu[r]->CalKrPc(b->S + 3 * n, b->kr + 3 * n, b->Pc + 3 * n, static_cast<OCP_USI>(n));
+        for (int j = 0; j < 3; j++) b->Pj[3 * n + j] = b->P[n] + b->Pc[3 * n + j];
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    *secs   = std::chrono::duration<double>(t1 - t0).count();
+    for (auto* f : fu) delete f;
+}
+
+extern "C" int orc_krpc_sof3(int nreg, const orc_satfunc3* reg, const orc_krpc_batch* b, int nthreads,
+                             double* seconds)
+{
+    if (nreg < 1 || !reg || !b || !b->P || !b->S || !b->kr || !b->Pc || !b->Pj) return 1;
+    if (b->deriv && (!b->dKr_dS || !b->dPcj_dS)) return 1;
+    for (int i = 0; i < nreg; i++)
+        if (!reg[i].swfn || !reg[i].sgfn || !reg[i].sof3 || reg[i].nrow_swfn < 2 || reg[i].nrow_sgfn < 2 ||
+            reg[i].nrow_sof3 < 2)
+            return 1;
+    if (b->satnum)
+        for (int64_t n = 0; n < b->n; n++)
+            if (b->satnum[n] < 0 || b->satnum[n] >= nreg) return 1;
+    return run_threads(b->n, nthreads, seconds, [nreg, reg, b](int64_t lo, int64_t hi, double* s) {
+        run_chunk_krpc_sof3(nreg, reg, b, lo, hi, s);
+    });
+}
+
 // The reference's own dense product of the FIM assembly (DaABpbC,
 // src/DenseMat.cpp:75-94): C = A B + C, row-major, A m x k, B k x n.
 extern "C" void orc_daabpbc(int m, int n, int k, const double* A, const double* B, double* C)

@@ -11,8 +11,8 @@ edge of an iteration cap or a stability threshold; any implementation whose
 rounding differs from the reference's may legitimately land on either side.
 
     python tests/golden/make_golden.py            # writes tests/golden/*.npz
-    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6, krpc, fimn_nc6,
-                                                   # config1_nc6)
+    python tests/golden/make_golden.py restart_nc6   # one case only (also impec_nc6, init_nc6, krpc, krpc_sof3,
+                                                   # fimn_nc6, config1_nc6)
 """
 from __future__ import annotations
 
@@ -398,6 +398,53 @@ def krpc_case():
     print(f"krpc: n={n} size={os.path.getsize(path) / 1e6:.2f} MB")
 
 
+def krpc_sof3_case():
+    """IsoT_FIM::CalKrPc (with derivatives) and IsoT_IMPEC::CalKrPc (without)
+    with FlowUnit_ODGW02 on two saturation regions of synthetic SWFN / SGFN /
+    SOF3 tables (the second with a repeated saturation node), 4096 cells:
+    random saturations, every table node exactly, S_g + S_w at the connate
+    water saturation (the default oil model's small-denominator branch),
+    values outside the tables and NaN. Outputs of the compiled reference."""
+    from oracle import krpc as K
+    r0 = synth.corey_fn_tables(601)
+    w1, g1, o1 = synth.corey_fn_tables(602, swc=0.2, sorw=0.15, nrow=9, pc_scale=(8.0, 3.0))
+    o1 = np.insert(o1, 3, o1[3], axis=0)  # a repeated node
+    regions = [r0, (w1, g1, o1)]
+    rng = np.random.default_rng(603)
+    n = 4096
+    S = np.zeros((n, 3))
+    S[:, 2] = rng.uniform(-0.05, 1.05, n)
+    S[:, 1] = rng.uniform(-0.05, 1.0, n)
+    S[:, 0] = 1 - S[:, 1] - S[:, 2]
+    satnum = rng.integers(0, 2, n).astype(np.int32)
+    k = 0
+    for r, tabs in enumerate(regions):
+        for col, t in zip((2, 1, 0), tabs):
+            for v in t[:, 0]:
+                S[k, col], satnum[k] = v, r
+                k += 1
+        swco = tabs[0][0, 0]
+        for sg in (0.0, 1e-9, 5e-9, 1e-8, 2e-8):
+            S[k], satnum[k] = (1 - swco - sg, sg, swco), r
+            k += 1
+    S[k:k + 4, 1:] = [[np.nan, 0.3], [0.1, np.nan], [np.inf, -np.inf], [-np.inf, np.inf]]
+    S[k + 4, 0] = np.nan
+    P = rng.uniform(500.0, 6000.0, n)
+    out = K.reference_sof3(regions, P, S, satnum, deriv=True, nthreads=8)
+    nod = K.reference_sof3(regions, P, S, satnum, deriv=False, nthreads=8)
+    d = {"note": np.array("CalKrPc, FlowUnit_ODGW02, two synthetic regions"), "in_P": P, "in_S": S,
+         "in_satnum": satnum}
+    for i, (w, g, o) in enumerate(regions):
+        d[f"swfn{i}"], d[f"sgfn{i}"], d[f"sof3{i}"] = w, g, o
+    for key in ("kr", "Pc", "Pj", "dKr_dS", "dPcj_dS"):
+        d[f"out_{key}"] = out[key]
+    for key in ("kr", "Pc", "Pj"):
+        d[f"impec_{key}"] = nod[key]
+    path = os.path.join(HERE, "krpc_sof3.npz")
+    np.savez_compressed(path, **d)
+    print(f"krpc_sof3: n={n} size={os.path.getsize(path) / 1e6:.2f} MB")
+
+
 def config1_case():
     """The CPU-runnable configuration in full: the 6-component fluid and 4096
     independent fresh states, P ~ U(5, 40) MPa, T ~ U(340, 400) K,
@@ -444,7 +491,8 @@ def main(only=()):
     if only:
         for name in only:
             {"restart_nc6": restart_case, "impec_nc6": impec_case, "init_nc6": init_case,
-             "krpc": krpc_case, "fimn_nc6": fimn_case, "config1_nc6": config1_case}[name]()
+             "krpc": krpc_case, "krpc_sof3": krpc_sof3_case, "fimn_nc6": fimn_case,
+             "config1_nc6": config1_case}[name]()
         return
 
     # 1) SPE5 fluid (examples/spe5/EGOIL.in) at 160 degF, the deck's initial composition
@@ -505,6 +553,7 @@ def main(only=()):
 
     # 9) relative permeability and capillary pressure after the flash
     krpc_case()
+    krpc_sof3_case()
 
     # 10) the FIMn formulation's flash and initialisation
     fimn_case()

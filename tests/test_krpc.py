@@ -1,8 +1,9 @@
 """Relative permeability and capillary pressure after the flash
-(IsoT_FIM::CalKrPc with FlowUnit_ODGW01, src/OCPFluidMethod.cpp:1189-1199,
-src/FlowUnit.cpp:183-349): the oracle against the golden fixture made by the
-compiled reference, and ocpf_krpc against both, bit for bit (the kernel
-rounds every operation as the reference does)."""
+(IsoT_FIM::CalKrPc, src/OCPFluidMethod.cpp:1189-1199, with FlowUnit_ODGW01,
+src/FlowUnit.cpp:183-349, and FlowUnit_ODGW02, :522-671): the oracle
+against the golden fixtures made by the compiled reference, and
+ocpf_cal_krpc against both, bit for bit (the kernel rounds every operation
+as the reference does)."""
 import os
 
 import numpy as np
@@ -21,6 +22,15 @@ def _fixture():
     d = np.load(GOLDEN)
     regions = [(d["swof0"], d["sgof0"]), (d["swof1"], d["sgof1"])]
     return regions, d["in_P"], d["in_S"], d["in_satnum"], {k: d[f"out_{k}"] for k in KEYS}
+
+
+def _fixture_sof3():
+    """FlowUnit_ODGW02 (SWFN / SGFN / SOF3) fixture: regions, inputs, the
+    FIM call's outputs and the IMPEC call's (kr, Pc, Pj: another oil model)."""
+    d = np.load(os.path.join(HERE, "golden", "krpc_sof3.npz"))
+    regions = [(d[f"swfn{i}"], d[f"sgfn{i}"], d[f"sof3{i}"]) for i in range(2)]
+    return (regions, d["in_P"], d["in_S"], d["in_satnum"], {k: d[f"out_{k}"] for k in KEYS},
+            {k: d[f"impec_{k}"] for k in ("kr", "Pc", "Pj")})
 
 
 def test_restated_oracle_matches_fixture():
@@ -43,6 +53,36 @@ def test_reference_reproduces_fixture():
     nod = K.reference(regions, P, S, sn, deriv=False, nthreads=4)
     for k in ("kr", "Pc", "Pj"):
         np.testing.assert_array_equal(nod[k], ref[k], err_msg=k)
+
+
+def test_restated_sof3_oracle_matches_fixture():
+    regions, P, S, sn, ref, impec = _fixture_sof3()
+    got = K.restated_sof3(regions, P, S, sn)
+    for k in KEYS:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    nod = K.restated_sof3(regions, P, S, sn, deriv=False)
+    for k in ("kr", "Pc", "Pj"):
+        np.testing.assert_array_equal(nod[k], impec[k], err_msg=k)
+    # the two calls' oil models differ (Stone II vs the default model), the
+    # rest agrees; the default model's small-denominator branch is covered
+    assert not np.array_equal(ref["kr"][:, 0], impec["kr"][:, 0])
+    np.testing.assert_array_equal(ref["kr"][:, 1:], impec["kr"][:, 1:])
+    kmax = {r: regions[r][2][-1, 1] for r in range(2)}
+    assert np.sum(impec["kr"][:, 0] == np.array([kmax[r] for r in sn])) > 10
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SRC), reason="reference sources not present")
+def test_reference_reproduces_sof3_fixture():
+    import subprocess
+    from oracle import oracle as O
+    subprocess.check_call(["make", "-s", "-C", os.path.dirname(O.__file__), "ref"])
+    regions, P, S, sn, ref, impec = _fixture_sof3()
+    got = K.reference_sof3(regions, P, S, sn, nthreads=4)
+    for k in KEYS:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    nod = K.reference_sof3(regions, P, S, sn, deriv=False, nthreads=4)
+    for k in ("kr", "Pc", "Pj"):
+        np.testing.assert_array_equal(nod[k], impec[k], err_msg=k)
 
 
 def test_table_search_is_state_independent():
@@ -86,6 +126,20 @@ def test_krpc_matches_reference_bit_for_bit():
     assert set(nod) == {"kr", "Pc", "Pj"}
     for k in ("kr", "Pc", "Pj"):
         np.testing.assert_array_equal(nod[k], ref[k], err_msg=k)
+
+
+@pytest.mark.gpu
+def test_krpc_sof3_matches_reference_bit_for_bit():
+    """FlowUnit_ODGW02 on the device: the FIM call (Stone II, dKro/dS_o) and
+    the IMPEC call (the default oil model) equal the compiled reference's."""
+    regions, P, S, sn, ref, impec = _fixture_sof3()
+    got = _run_gpu(regions, P, S, sn)
+    for k in KEYS:
+        np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    nod = _run_gpu(regions, P, S, sn, deriv=False)
+    assert set(nod) == {"kr", "Pc", "Pj"}
+    for k in ("kr", "Pc", "Pj"):
+        np.testing.assert_array_equal(nod[k], impec[k], err_msg=k)
 
 
 @pytest.mark.gpu
@@ -144,3 +198,22 @@ def test_krpc_rejects_bad_tables():
     regs[0] = _lib.Satfunc(1, 2, g.ctypes.data, g.ctypes.data)
     assert L.ocpf_krpc_create(regs, 1, 0, C.byref(h)) == 1  # one row
     assert L.ocpf_krpc_create(regs, 0, 0, C.byref(h)) == 1  # no region
+
+
+def test_krpc_sof3_rejects_bad_tables():
+    """The SWFN / SGFN / SOF3 creator refuses a table of one row, a
+    decreasing saturation column or a missing table, before any GPU work."""
+    from opencaeporo_b200 import _lib
+    import ctypes as C
+    L = _lib.lib()
+    regions = _fixture_sof3()[0]
+    w, g, o = (np.ascontiguousarray(t) for t in regions[0])
+    bad = o[::-1].copy()  # decreasing So
+    h = C.c_void_p()
+    regs = (_lib.Satfunc3 * 1)()
+    for args in ((len(w), len(g), len(bad), w, g, bad), (1, len(g), len(o), w, g, o),
+                 (len(w), len(g), len(o), w, None, o)):
+        nw, ng, no, a, b, c = args
+        regs[0] = _lib.Satfunc3(nw, ng, no, 0, a.ctypes.data, None if b is None else b.ctypes.data, c.ctypes.data)
+        assert L.ocpf_krpc_create_sof3(regs, 1, 0, C.byref(h)) == 1
+    assert L.ocpf_krpc_create_sof3(regs, 0, 0, C.byref(h)) == 1
