@@ -71,7 +71,7 @@ cudaError_t launch_phased_multi(const MultiFluid& MF, const MultiArgs& M, const 
     };
     step(MS_INIT, MF, M, gp, bp, 0, st);
     if (learn) {
-        const unsigned gl = (unsigned)(n * std::min<int64_t>((maxc + 63) / 64, (int64_t)sms * 4));
+        const unsigned gl = (unsigned)(n * std::min<int64_t>((maxc + LEARN_TILE - 1) / LEARN_TILE, (int64_t)sms * 4));
         step(MS_LEARN, MF, M, gl, 128, sizeof(LearnSmem), st);
         split_round(LEARN_ROUND);
     }

@@ -114,7 +114,7 @@ cudaError_t OCPF_CAT(launch_phased_nc, OCPF_NC)(const FluidConst& F, const Phase
     KP(init)<<<gcell, bp, 0, st>>>(F, a);
     if (a.opts & PH_LEARN) {
         // learned initialiser: predicted-unstable fresh cells split first
-        const int gl = (int)std::min<int64_t>((a.count + 63) / 64, (int64_t)sms * 4);
+        const int gl = (int)std::min<int64_t>((a.count + LEARN_TILE - 1) / LEARN_TILE, (int64_t)sms * 4);
         KP(learn)<<<gl, 128, sizeof(LearnSmem), st>>>(F, a);
         OCPF_CAT(split_round_, OCPF_NC)(F, a, st, LEARN_ROUND, gp, bp, g_sp, g_spnr);
     }

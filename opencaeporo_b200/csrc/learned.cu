@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "learned.cuh"
+#include "learned_tc.cuh"
 #include "ocp_flash.h"
 
 namespace ocpf {
@@ -157,30 +158,24 @@ __global__ void __launch_bounds__(NTH) k_mlp_grad(int nin, int nout, int64_t n, 
     }
 }
 
-struct FwdSmem {
-    MlpSmemW w;
-    bf16     xs[TS * MLP_IO];
-    bf16     h1[TS * MLP_H], h2[TS * MLP_H];
-    float    out[TS * MLP_IO];
-};
-
-__global__ void __launch_bounds__(NTH) k_mlp_forward(int nin, int nout, int64_t n, const float* __restrict__ p,
-                                                     const float* __restrict__ x, float* __restrict__ y)
+// Forward pass for evaluation on the tcgen05 tensor cores (learned_tc.cuh):
+// 128 samples per CTA tile, grid-stride over the tiles.
+__global__ void __launch_bounds__(MLP_TC_ROWS) k_mlp_forward(int nin, int nout, int64_t n, const float* __restrict__ p,
+                                                             const float* __restrict__ x, float* __restrict__ y)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    FwdSmem&      sm   = *reinterpret_cast<FwdSmem*>(smem_raw);
-    const int64_t base = (int64_t)blockIdx.x * TS;
-    const int     m0   = 16 * (threadIdx.x >> 5);
-    mlp_load_weights(sm.w, p);
-    load_inputs(sm.xs, x, nin, n, base);
-    __syncthreads();
-    mlp_forward_warp(sm.w, sm.xs, m0, sm.h1, sm.h2, nullptr, nullptr, sm.out + m0 * MLP_IO);
-    __syncthreads();
-    for (int i = threadIdx.x; i < TS * nout; i += blockDim.x) {
-        const int     j = i / TS, r = i % TS;
-        const int64_t s = base + r;
-        if (s < n) y[(int64_t)j * n + s] = sm.out[r * MLP_IO + j];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    MlpTc net(*reinterpret_cast<MlpTcSmem*>(smem_raw));
+    net.begin(p);
+    for (int64_t base = (int64_t)blockIdx.x * MLP_TC_ROWS; base < n; base += (int64_t)gridDim.x * MLP_TC_ROWS) {
+        const int64_t s = base + threadIdx.x;
+        float         f[MLP_IO], o[MLP_IO];
+#pragma unroll
+        for (int j = 0; j < MLP_IO; j++) f[j] = (j < nin && s < n) ? x[(int64_t)j * n + s] : 0.f;
+        net.forward(f, o);
+        if (s < n)
+            for (int j = 0; j < nout; j++) y[(int64_t)j * n + s] = o[j];
     }
+    net.end();
 }
 
 // Adam (beta1 0.9, beta2 0.999, eps 1e-8, bias-corrected) on the FP32 master
@@ -213,12 +208,16 @@ extern "C" int ocpf_mlp_forward(int nin, int nout, int64_t n, const float* param
 {
     if (!io_ok(nin, nout) || n < 0 || !params || (n > 0 && (!x || !y))) return OCPF_EINVAL;
     if (n == 0) return OCPF_OK;
-    const int64_t blocks = (n + TS - 1) / TS;
-    if (blocks > 0x7fffffffLL) return OCPF_EINVAL;
-    const size_t sm = sizeof(FwdSmem);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return OCPF_ECUDA;
+    const int64_t tiles  = (n + MLP_TC_ROWS - 1) / MLP_TC_ROWS;
+    const int64_t blocks = tiles < (int64_t)sms * 8 ? tiles : (int64_t)sms * 8;
+    const size_t  sm     = sizeof(MlpTcSmem);
     if (cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
         return OCPF_ECUDA;
-    k_mlp_forward<<<(unsigned)blocks, NTH, sm, (cudaStream_t)stream>>>(nin, nout, n, params, x, y);
+    k_mlp_forward<<<(unsigned)blocks, MLP_TC_ROWS, sm, (cudaStream_t)stream>>>(nin, nout, n, params, x, y);
     return cudaGetLastError() == cudaSuccess ? OCPF_OK : OCPF_ECUDA;
 }
 

@@ -75,6 +75,37 @@ def test_mlp_forward_matches_oracle():
 
 
 @pytest.mark.gpu
+def test_tcgen05_forward_over_many_tiles_and_a_ragged_end():
+    """The evaluation forward pass (tcgen05, 128 samples per tile) on a batch
+    with more tiles than its grid holds CTAs (each CTA loops over several
+    tiles, reusing its tensor memory) and a partial last tile: against the
+    oracle sample by sample, and against the training kernel's mma.sync
+    forward pass through the loss both give for the same outputs."""
+    import torch
+    from opencaeporo_b200 import learn
+    n = 128 * 148 * 8 * 2 + 77
+    p, x, t, w = _problem(n=n, seed=11)
+    dev = torch.device("cuda", 0)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    y = learn.forward(T(p), T(x), 7).cpu().numpy().astype(np.float64)
+    assert np.all(np.isfinite(y))
+    ref, _ = M.forward(p, x, bf16=True)
+    err = np.abs(y - ref[:7])
+    assert np.max(err) < 2e-2 * (1 + np.max(np.abs(ref[:7]))), np.max(err)
+    assert np.mean(err) < 2e-3, np.mean(err)
+    # the same loss from the tcgen05 outputs and from the mma.sync training kernel
+    lam = 0.5
+    g = torch.zeros(M.NPARAM, dtype=torch.float32, device=dev)
+    loss = torch.zeros(2, dtype=torch.float32, device=dev)
+    learn.grad(T(p), T(x), T(t), T(w), lam, g, loss)
+    lk = loss.cpu().numpy().astype(np.float64)
+    z = y[0]
+    bce = np.sum(np.maximum(z, 0) + np.log1p(np.exp(-np.abs(z))) - t[0] * z)
+    mse = np.sum(w * np.sum((y[1:] - t[1:]) ** 2, axis=0) / 6)
+    np.testing.assert_allclose([bce, mse], lk, rtol=1e-3)
+
+
+@pytest.mark.gpu
 def test_mlp_gradient_matches_oracle():
     """Gradient of the BF16 tensor-core kernel against the CPU oracle with
     the same BF16 roundings; and against the exact float64 gradient to
