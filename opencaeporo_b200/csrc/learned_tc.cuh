@@ -65,10 +65,12 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D, M = 128.
-__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n)
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, M = 128; A and
+// B K-major unless a_mn / b_mn (MN-major: bits 15 and 16).
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int n, bool a_mn = false, bool b_mn = false)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(MLP_TC_ROWS >> 4) << 24);
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(MLP_TC_ROWS >> 4) << 24);
 }
 
 __device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc)
@@ -77,6 +79,22 @@ __device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t adesc, uint64_t 
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+// An operand as the MMAs read it: start address, the descriptor's leading
+// and stride byte offsets, and the advance of the start per K = 16 step.
+struct TcOperand {
+    uint32_t start, lbo, sbo, kstep;
+};
+
+// D (at TMEM address dtmem) = A B^T over `ksteps` K = 16 steps; issued by
+// the calling thread.
+__device__ __forceinline__ void tc_gemm(uint32_t dtmem, const TcOperand& A, const TcOperand& B, int ksteps,
+                                        uint32_t idesc)
+{
+    for (int k = 0; k < ksteps; k++)
+        tc_mma(dtmem, umma_desc(A.start + A.kstep * k, A.lbo, A.sbo), umma_desc(B.start + B.kstep * k, B.lbo, B.sbo),
+               idesc, k > 0 ? 1u : 0u);
 }
 
 __device__ __forceinline__ void tc_commit(uint64_t* bar)

@@ -79,7 +79,7 @@ def test_tcgen05_forward_over_many_tiles_and_a_ragged_end():
     """The evaluation forward pass (tcgen05, 128 samples per tile) on a batch
     with more tiles than its grid holds CTAs (each CTA loops over several
     tiles, reusing its tensor memory) and a partial last tile: against the
-    oracle sample by sample, and against the training kernel's mma.sync
+    oracle sample by sample, and against the training kernel's own
     forward pass through the loss both give for the same outputs."""
     import torch
     from opencaeporo_b200 import learn
@@ -93,7 +93,7 @@ def test_tcgen05_forward_over_many_tiles_and_a_ragged_end():
     err = np.abs(y - ref[:7])
     assert np.max(err) < 2e-2 * (1 + np.max(np.abs(ref[:7]))), np.max(err)
     assert np.mean(err) < 2e-3, np.mean(err)
-    # the same loss from the tcgen05 outputs and from the mma.sync training kernel
+    # the same loss from the tcgen05 outputs and from the training kernel's forward pass
     lam = 0.5
     g = torch.zeros(M.NPARAM, dtype=torch.float32, device=dev)
     loss = torch.zeros(2, dtype=torch.float32, device=dev)
