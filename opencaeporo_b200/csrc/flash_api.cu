@@ -30,7 +30,7 @@ using PlainLauncher = cudaError_t (*)(const FluidConst&, int64_t, int64_t, const
 // Batched-form launch sequences (flash_phased_ncN.cu).
 #define OCPF_DECL_PHASED(N)                                                                                 \
     cudaError_t launch_phased_nc##N(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t, cudaStream_t st, \
-                                    const cudaEvent_t* marks);                                                       \
+                                    const cudaEvent_t* marks, const SideStreams* side);                              \
     int         phased_state_doubles_nc##N();
 OCPF_DECL_PHASED(3)
 OCPF_DECL_PHASED(6)
@@ -38,7 +38,7 @@ OCPF_DECL_PHASED(9)
 OCPF_DECL_PHASED(12)
 
 using PhasedLauncher = cudaError_t (*)(const FluidConst&, const PhasedArgs&, const LaunchTune&, cudaStream_t,
-                                       const cudaEvent_t*);
+                                       const cudaEvent_t*, const SideStreams*);
 
 static PhasedLauncher phased_kernel(int nc, int* ndbl)
 {
@@ -177,6 +177,10 @@ struct ocpf_ctx {
     // subset calls: compact device copies of the listed cells, grown on demand
     int64_t sub_cap;
     void*   sub;
+    // the PH_EARLY schedule's side streams and fork/join events, created on
+    // the first batched call
+    SideStreams side;
+    bool        side_ok;
 };
 
 static const char* kVersion = "opencaeporo-b200 flash 0.1 (sm_100a)";
@@ -277,6 +281,11 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     if (c->evj) cudaEventDestroy(c->evj);
     for (auto& s : c->hs)
         if (s) cudaStreamDestroy(s);
+    for (int k = 0; k < 4; k++) {
+        if (c->side.s[k]) cudaStreamDestroy(c->side.s[k]);
+        if (c->side.fork[k]) cudaEventDestroy(c->side.fork[k]);
+        if (c->side.join[k]) cudaEventDestroy(c->side.join[k]);
+    }
     cudaSetDevice(prev);
     delete c;
     return OCPF_OK;
@@ -381,9 +390,34 @@ static void scratch_view(const ocpf_ctx* c, int part, int64_t cap, StateBuf& S, 
 // re-captures (cudaGraphExecUpdate keeps the executable when only parameters
 // differ). Work already captured by the caller's own stream capture, and the
 // host path's alternating parts, launch directly.
+// The side streams of the PH_EARLY schedule, created once per context.
+static bool ensure_side(ocpf_ctx* c)
+{
+    if (c->side_ok) return true;
+    // The side streams of trials 1-3 carry few cells, among them the ones
+    // whose stability was hardest to decide and whose restart chains are
+    // the call's critical path: their blocks are dispatched ahead of the
+    // rest. (Stream 0 is not used: trial 0's cells split on the call's
+    // stream.)
+    int lo = 0, hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess) lo = hi = 0;
+    for (int k = 0; k < 4; k++) {
+        if (!c->side.s[k] &&
+            cudaStreamCreateWithPriority(&c->side.s[k], cudaStreamNonBlocking, k == 0 ? lo : hi) != cudaSuccess)
+            return false;
+        if (!c->side.fork[k] && cudaEventCreateWithFlags(&c->side.fork[k], cudaEventDisableTiming) != cudaSuccess)
+            return false;
+        if (!c->side.join[k] && cudaEventCreateWithFlags(&c->side.join[k], cudaEventDisableTiming) != cudaSuccess)
+            return false;
+    }
+    c->side_ok = true;
+    return true;
+}
+
 static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs& args, cudaStream_t st,
                                  bool graph_ok, bool mark)
 {
+    const SideStreams* sd = (args.opts & PH_EARLY) ? &c->side : nullptr;
     // the part marks are taken on direct launches: events recorded by a
     // replayed graph's nodes cannot be timed against each other
     const cudaEvent_t* mk = mark ? c->marks : nullptr;
@@ -393,21 +427,21 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
     if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusInvalidated;
     c->last_kernels = -1;
     const LaunchTune& t = c->tune;
-    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, t, st, mk);
+    if (!graph_ok || cs != cudaStreamCaptureStatusNone || c->launches++ == 0) return k(c->fc, args, t, st, mk, sd);
     if (!(c->gvalid && std::memcmp(&c->gkey, &args, sizeof(args)) == 0 &&
           std::memcmp(&c->gtune, &t, sizeof(t)) == 0 && c->gmark == mark)) {
         c->gvalid = false;
         if (!c->gs && cudaStreamCreateWithFlags(&c->gs, cudaStreamNonBlocking) != cudaSuccess)
-            return k(c->fc, args, t, st, mk);
+            return k(c->fc, args, t, st, mk, sd);
         cudaGraph_t g = nullptr;
         if (cudaStreamBeginCapture(c->gs, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-            return k(c->fc, args, t, st, mk);
-        const cudaError_t le = k(c->fc, args, t, c->gs, mk);
+            return k(c->fc, args, t, st, mk, sd);
+        const cudaError_t le = k(c->fc, args, t, c->gs, mk, sd);
         const cudaError_t ce = cudaStreamEndCapture(c->gs, &g);
         if (le != cudaSuccess || ce != cudaSuccess || !g) {
             if (g) cudaGraphDestroy(g);
             cudaGetLastError();
-            return k(c->fc, args, t, st, mk);
+            return k(c->fc, args, t, st, mk, sd);
         }
         size_t nn = 0;
         int    nk = 0;
@@ -430,12 +464,12 @@ static cudaError_t launch_phased(ocpf_ctx* c, PhasedLauncher k, const PhasedArgs
                 c->gexec = nullptr;
             }
         }
-        if (!ok) ok = cudaGraphInstantiate(&c->gexec, g, 0) == cudaSuccess;
+        if (!ok) ok = cudaGraphInstantiate(&c->gexec, g, cudaGraphInstantiateFlagUseNodePriority) == cudaSuccess;
         cudaGraphDestroy(g);
         if (!ok) {
             c->gexec = nullptr;
             cudaGetLastError();
-            return k(c->fc, args, t, st, mk);
+            return k(c->fc, args, t, st, mk, sd);
         }
         c->gkey   = args;
         c->gtune  = t;
@@ -478,6 +512,9 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         args.mlp    = c->mlp;
         args.tail   = tail;
         if (form == OCPF_FORM_FAST && c->mlp && c->fc.learn_on) args.opts |= PH_LEARN;
+        // the per-trial split schedule on the device path; the host path's
+        // parts, and calls that record the part marks, keep one stream
+        if (part < 0 && !c->part_timing && ensure_side(c)) args.opts |= PH_EARLY;
         if (part < 0) {
             const int rc = ensure_scratch(c, count);
             if (rc != OCPF_OK) return rc;

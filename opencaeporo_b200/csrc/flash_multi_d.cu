@@ -7,11 +7,11 @@ namespace ocpf {
 #define KM __global__ void __launch_bounds__(128)
 KM kpm_slow(const __grid_constant__ MultiFluid MF, const __grid_constant__ MultiArgs M)
 {
-    OCPF_MULTI_ITEMS(MF, M, (slow_body<NC_>(F_, A_)));
+    OCPF_MULTI_ITEMS(MF, M, (slow_body<NC_>(F_, A_, L_SLOW)));
 }
 KM kpm_slow_thread(const __grid_constant__ MultiFluid MF, const __grid_constant__ MultiArgs M)
 {
-    OCPF_MULTI_ITEMS(MF, M, (slow_thread_body<NC_>(F_, A_)));
+    OCPF_MULTI_ITEMS(MF, M, (slow_thread_body<NC_>(F_, A_, L_SLOW)));
 }
 KM kpm_finalize(const __grid_constant__ MultiFluid MF, const __grid_constant__ MultiArgs M)
 {

@@ -9,13 +9,13 @@
 namespace ocpf {
 // launch sequences of the batched form (flash_phased_ncN.cu)
 cudaError_t launch_phased_nc3(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t, cudaStream_t st,
-                              const cudaEvent_t* marks);
+                              const cudaEvent_t* marks, const SideStreams* side);
 cudaError_t launch_phased_nc6(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t, cudaStream_t st,
-                              const cudaEvent_t* marks);
+                              const cudaEvent_t* marks, const SideStreams* side);
 cudaError_t launch_phased_nc9(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t, cudaStream_t st,
-                              const cudaEvent_t* marks);
+                              const cudaEvent_t* marks, const SideStreams* side);
 cudaError_t launch_phased_nc12(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t, cudaStream_t st,
-                              const cudaEvent_t* marks);
+                              const cudaEvent_t* marks, const SideStreams* side);
 // context accessors (flash_api.cu)
 const FluidConst* ctx_fluid_const(const ocpf_ctx* c);
 int               ctx_device(const ocpf_ctx* c);
@@ -51,7 +51,8 @@ extern "C" int ocpf_flash_fim_noalloc(ocpf_ctx* ctx, int64_t ncell, const ocpf_f
     if (!ctx_fim_args_ok(ctx, in, sk, out)) return OCPF_EINVAL;
     const FluidConst& F = *ctx_fluid_const(ctx);
     int               nd;
-    cudaError_t (*launch)(const FluidConst&, const PhasedArgs&, const LaunchTune&, cudaStream_t, const cudaEvent_t*);
+    cudaError_t (*launch)(const FluidConst&, const PhasedArgs&, const LaunchTune&, cudaStream_t, const cudaEvent_t*,
+                          const SideStreams*);
     switch (F.nc) {
         case 3: launch = launch_phased_nc3, nd = SF<3>::COUNT; break;
         case 6: launch = launch_phased_nc6, nd = SF<6>::COUNT; break;
@@ -100,7 +101,7 @@ extern "C" int ocpf_flash_fim_noalloc(ocpf_ctx* ctx, int64_t ncell, const ocpf_f
         // the launch sequence zeroes the list counters on the stream first;
         // every other scratch field a cell reads is written for it earlier in
         // the same call
-        if (launch(F, a, kDefaultTune, (cudaStream_t)stream, nullptr) != cudaSuccess) rc = OCPF_ECUDA;
+        if (launch(F, a, kDefaultTune, (cudaStream_t)stream, nullptr, nullptr) != cudaSuccess) rc = OCPF_ECUDA;
     }
     if (prev != dev) cudaSetDevice(prev);
     return rc;

@@ -86,9 +86,9 @@ enum ListId : int {
     L_S01_0 = 0, L_S01_1,
     L_STA_0, L_STA_1, L_STA_2, L_STA_3,
     L_NRSTA_0, L_NRSTA_1, L_NRSTA_2, L_NRSTA_3,
-    L_SP_0, L_SP_LEARN,
-    L_SPNR_0, L_SPNR_LEARN,
-    L_SLOW,
+    L_SP_0, L_SP_LEARN, L_SP_T0, L_SP_T1, L_SP_T2, L_SP_T3,
+    L_SPNR_0, L_SPNR_LEARN, L_SPNR_T0, L_SPNR_T1, L_SPNR_T2, L_SPNR_T3,
+    L_SLOW, L_SLOW_T0, L_SLOW_T1, L_SLOW_T2, L_SLOW_T3,
     L_FRESH,  // fresh cells awaiting the learned initialiser
     // mixed form: stability trials whose Newton polish failed from the FP32
     // end point, continued by FP64 substitution, and their Newton step
@@ -101,7 +101,17 @@ enum ListId : int {
 // restart takes the warp-per-cell path.
 constexpr int SPLIT_ROUNDS = 1;
 constexpr int LEARN_ROUND  = SPLIT_ROUNDS;
+// With PH_EARLY, the fresh cells that strict stability trial k >= 1 finds
+// unstable split in round TRIAL_ROUND0 + k (lists L_SP_Tk, L_SPNR_Tk) and
+// restart from L_SLOW_Tk, on a side stream forked after trial k, while the
+// later trials and round 0 run: these few cells, whose stability was the
+// hardest to decide and whose restart chains are the longest, start their
+// split as soon as their own trial has decided. The work of each cell, and
+// its arithmetic, are the same in either schedule.
+constexpr int TRIAL_ROUND0 = LEARN_ROUND + 1;
 static_assert(L_SP_0 + LEARN_ROUND == L_SP_LEARN && L_SPNR_0 + LEARN_ROUND == L_SPNR_LEARN, "list order");
+static_assert(L_SP_0 + TRIAL_ROUND0 == L_SP_T0 && L_SPNR_0 + TRIAL_ROUND0 == L_SPNR_T0 && L_SLOW + 1 == L_SLOW_T0,
+              "list order");
 
 struct Lists {
     int32_t*  items;  // [L_COUNT][cap]
@@ -140,6 +150,15 @@ constexpr LaunchTune kDefaultTune{128, 100, 0, 0};
 // PhasedArgs::opts bits
 constexpr uint32_t PH_MIXED = 1u;  // FP32 successive substitution (flash_mixed.cuh)
 constexpr uint32_t PH_LEARN = 2u;  // learned initialiser for fresh cells (flash_learned.cuh)
+constexpr uint32_t PH_EARLY = 4u;  // split each strict trial's unstable cells on its own side stream
+
+// The side streams of the PH_EARLY schedule: trial k's split round and
+// restarts run on s[k], after fork[k] is recorded on the call's stream; the
+// call's stream waits for join[k] before the finalize.
+struct SideStreams {
+    cudaStream_t s[4];
+    cudaEvent_t  fork[4], join[4];
+};
 
 struct PhasedArgs {
     int64_t      count, stride;

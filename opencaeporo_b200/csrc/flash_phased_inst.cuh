@@ -42,8 +42,11 @@ K128 KP(sp_prep)(const __grid_constant__ FluidConst F, const PhasedArgs a, int r
 K128 KP(sp_ssm)(const __grid_constant__ FluidConst F, const PhasedArgs a, int r) { sp_ssm_body<kNC>(F, a, r); }
 K128 KP(sp_nrinit)(const __grid_constant__ FluidConst F, const PhasedArgs a, int r) { sp_nrinit_body<kNC>(F, a, r); }
 K128 KP(sp_nr)(const __grid_constant__ FluidConst F, const PhasedArgs a, int r) { sp_nr_body<kNC>(F, a, r); }
-K128 KP(slow)(const __grid_constant__ FluidConst F, const PhasedArgs a) { slow_body<kNC>(F, a); }
-K128 KP(slow_thread)(const __grid_constant__ FluidConst F, const PhasedArgs a) { slow_thread_body<kNC>(F, a); }
+K128 KP(slow)(const __grid_constant__ FluidConst F, const PhasedArgs a, int list) { slow_body<kNC>(F, a, list); }
+K128 KP(slow_thread)(const __grid_constant__ FluidConst F, const PhasedArgs a, int list)
+{
+    slow_thread_body<kNC>(F, a, list);
+}
 K128 KP(learn)(const __grid_constant__ FluidConst F, const PhasedArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -84,9 +87,14 @@ void OCPF_CAT(split_round_, OCPF_NC)(const FluidConst& F, const PhasedArgs& a, c
 // The launch sequence of one batched flash (the schedule of flash_phased.cuh)
 // with the context's launch shape. marks (may be null): two events recorded
 // on the stream just before and just after the split-restart kernel, so that
-// a caller can time the sequence's parts.
+// a caller can time the sequence's parts. With PH_EARLY in a.opts, the
+// split round and restarts of the cells that strict trial k >= 1 finds
+// unstable run on side->s[k] (on `st` itself when side is null), forked
+// after trial k and joined before the finalize; trial 0's (most of the
+// split work) stay in round 0 on `st` after the last trial, so that its
+// persistent kernels do not hold the SMs while trials 1-3 run.
 cudaError_t OCPF_CAT(launch_phased_nc, OCPF_NC)(const FluidConst& F, const PhasedArgs& a, const LaunchTune& t,
-                                                cudaStream_t st, const cudaEvent_t* marks)
+                                                cudaStream_t st, const cudaEvent_t* marks, const SideStreams* side)
 {
     static int sms = 0, occ_s01 = 0, occ_sta = 0, occ_sp = 0, occ_sta32 = 0, occ_spnr = 0, occ_stnr = 0;
     if (!sms) {
@@ -139,14 +147,31 @@ cudaError_t OCPF_CAT(launch_phased_nc, OCPF_NC)(const FluidConst& F, const Phase
             KP(sta_verdict)<<<gp, bp, 0, st>>>(F, a, k, L_STA_0 + k, L_NRSTA_0 + k, false);
             KP(sta_nr)<<<g_stnr, 128, 0, st>>>(F, a, k, L_NRSTA_0 + k, -1);
         }
+        if ((a.opts & PH_EARLY) && k > 0) {
+            // trial k's unstable cells: split and restarts beside the later trials
+            cudaStream_t ss = st;
+            if (side) {
+                ss = side->s[k];
+                cudaEventRecord(side->fork[k], st);
+                cudaStreamWaitEvent(ss, side->fork[k], 0);
+            }
+            OCPF_CAT(split_round_, OCPF_NC)(F, a, ss, TRIAL_ROUND0 + k, gp, bp, g_sp, g_spnr);
+            if (t.slow_threads)
+                KP(slow_thread)<<<gp, bp, 0, ss>>>(F, a, L_SLOW_T0 + k);
+            else
+                KP(slow)<<<gp, 128, 0, ss>>>(F, a, L_SLOW_T0 + k);
+            if (side) cudaEventRecord(side->join[k], ss);
+        }
     }
     for (int r = 0; r < SPLIT_ROUNDS; r++) OCPF_CAT(split_round_, OCPF_NC)(F, a, st, r, gp, bp, g_sp, g_spnr);
     if (marks) cudaEventRecord(marks[0], st);
     if (t.slow_threads)
-        KP(slow_thread)<<<gp, bp, 0, st>>>(F, a);
+        KP(slow_thread)<<<gp, bp, 0, st>>>(F, a, L_SLOW);
     else
-        KP(slow)<<<gp, 128, 0, st>>>(F, a);
+        KP(slow)<<<gp, 128, 0, st>>>(F, a, L_SLOW);
     if (marks) cudaEventRecord(marks[1], st);
+    if ((a.opts & PH_EARLY) && side)
+        for (int k = 1; k < 4; k++) cudaStreamWaitEvent(st, side->join[k], 0);
     if (a.tail.mode & FM_FIMN)
         KP(finalize_fimn)<<<gcell, bp, 0, st>>>(F, a);
     else

@@ -190,7 +190,7 @@ __device__ __forceinline__ void sta_decide(CellFlash<NC>& f, const PhasedArgs& a
         f.ssmsta_realTol = sqrt(Se);
         f.NP             = 2;
         store_book(f, S, c, meta & ~(M_RESTART | M_SPPHASE));
-        a.L.push(L_SP_0, (int32_t)c);
+        a.L.push((a.opts & PH_EARLY) && k > 0 ? L_SP_T0 + k : L_SP_0, (int32_t)c);
     } else if (k < 3) {
         store_book(f, S, c, meta);
         a.L.push(L_STA_0 + k + 1, (int32_t)c);
@@ -702,7 +702,8 @@ __device__ __forceinline__ void sp_after_nr(CellFlash<NC>& f, const PhasedArgs& 
     if (restart) {
         store_split(f, S, c);
         store_book(f, S, c, meta);
-        a.L.push(r + 1 < SPLIT_ROUNDS ? L_SP_0 + r + 1 : L_SLOW, (int32_t)c);
+        const int slow = r >= TRIAL_ROUND0 ? L_SLOW_T0 + (r - TRIAL_ROUND0) : L_SLOW;
+        a.L.push(r + 1 < SPLIT_ROUNDS ? L_SP_0 + r + 1 : slow, (int32_t)c);
         return;
     }
     f.check_split();
@@ -836,15 +837,15 @@ __device__ void sp_nr_body(const FluidConst& F, const PhasedArgs& a, int r)
 // states, some needing tens of thousands of steps), one warp per cell
 // (flash_warp.cuh); lane 0 stores the result.
 template <int NC>
-__device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
+__device__ void slow_body(const FluidConst& F, const PhasedArgs& a, int list = L_SLOW)
 {
     using F_ = SF<NC>;
     const StateBuf& S    = a.S;
-    const uint32_t  n    = a.L.len(L_SLOW);
+    const uint32_t  n    = a.L.len(list);
     const uint32_t  nw   = (vgrid(a) * blockDim.x) >> 5;
     const bool      lead = (threadIdx.x & 31) == 0;
     for (uint32_t k = (vblock(a) * blockDim.x + threadIdx.x) >> 5; k < n; k += nw) {
-        const int64_t c = a.L.item(L_SLOW, k);
+        const int64_t c = a.L.item(list, k);
         CellFlash<NC> f(F);
         uint32_t      meta;
         load_split_cell(f, a, c, meta);
@@ -886,11 +887,11 @@ __device__ void slow_body(const FluidConst& F, const PhasedArgs& a)
 // one, each on a longer dependent chain. The autotuner's alternative for
 // batches with many restarting cells.
 template <int NC>
-__device__ void slow_thread_body(const FluidConst& F, const PhasedArgs& a)
+__device__ void slow_thread_body(const FluidConst& F, const PhasedArgs& a, int list = L_SLOW)
 {
     using F_ = SF<NC>;
     const StateBuf& S = a.S;
-    OCPF_FOR_ITEMS(a, L_SLOW, c)
+    OCPF_FOR_ITEMS(a, list, c)
     {
         CellFlash<NC> f(F);
         uint32_t      meta;
