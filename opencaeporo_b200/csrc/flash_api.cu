@@ -4,8 +4,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <chrono>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "flash_multi.cuh"
@@ -143,6 +145,7 @@ struct ocpf_ctx {
     int64_t     stage_cap;
     void*       stage;
     cudaStream_t hs[HOST_PARTS];
+    cudaEvent_t  hdone[HOST_PARTS];  // recorded after each part's last copy-out
     // batched-form scratch: per-cell phase state, cell lists and list
     // counters, in parts of part_cap cells (the host path uses HOST_PARTS parts)
     int64_t     eq_cap;    // total cells the scratch holds
@@ -281,6 +284,8 @@ extern "C" int ocpf_destroy(ocpf_ctx* c)
     if (c->evj) cudaEventDestroy(c->evj);
     for (auto& s : c->hs)
         if (s) cudaStreamDestroy(s);
+    for (auto& ev : c->hdone)
+        if (ev) cudaEventDestroy(ev);
     for (int k = 0; k < 4; k++) {
         if (c->side.s[k]) cudaStreamDestroy(c->side.s[k]);
         if (c->side.fork[k]) cudaEventDestroy(c->side.fork[k]);
@@ -1031,6 +1036,8 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
     }
     for (auto& s : c->hs)
         if (!s) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    for (auto& ev : c->hdone)
+        if (!ev) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     const int64_t cap = c->stage_cap;
     if (form != OCPF_FORM_PLAIN) {
         const int r2 = ensure_scratch(c, cap, HOST_PARTS);
@@ -1042,8 +1049,28 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
     Views V[HOST_PARTS];
     for (int b = 0; b < HOST_PARTS; b++) V[b] = carve((char*)c->stage + b * stage_stride(per, cap), cap, L, sk, out);
     const bool use_sk = c->fc.use_skip != 0;
-    int        bidx   = 0;
-    for (int64_t c0 = 0; c0 < ncell && rc == OCPF_OK; c0 += cap, bidx = (bidx + 1) % HOST_PARTS) {
+    // Each chunk goes to a part whose previous chunk has been copied out
+    // (first every part once, then whichever finishes first), so a chunk
+    // that holds a long restart chain keeps only its own part busy instead
+    // of also holding back the chunks dealt to the same stream after it.
+    int nused = 0;
+    auto next_part = [&]() -> int {
+        if (nused < HOST_PARTS) return nused++;
+        for (;;) {
+            for (int b = 0; b < HOST_PARTS; b++) {
+                const cudaError_t q = cudaEventQuery(c->hdone[b]);
+                if (q == cudaSuccess) return b;
+                if (q != cudaErrorNotReady) return -1;
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    };
+    for (int64_t c0 = 0; c0 < ncell && rc == OCPF_OK; c0 += cap) {
+        const int bidx = next_part();
+        if (bidx < 0) {
+            rc = OCPF_ECUDA;
+            break;
+        }
         const int64_t cnt = std::min<int64_t>(cap, ncell - c0);
         cudaStream_t  st  = c->hs[bidx];
         const Views&  v   = V[bidx];
@@ -1118,6 +1145,7 @@ extern "C" int ocpf_flash_fim_host(ocpf_ctx* c, int64_t ncell, const ocpf_fim_in
             D(sk->T, v.sk.T, 1, 8);
             D(sk->z, v.sk.z, L.nc, 8);
         }
+        if (e == cudaSuccess) e = cudaEventRecord(c->hdone[bidx], st);
         if (e != cudaSuccess) rc = OCPF_ECUDA;
     }
     for (auto& s : c->hs)
