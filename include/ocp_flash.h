@@ -391,8 +391,10 @@ int ocpf_flash_fim_regions(int nreg, ocpf_ctx* const* ctx, const int64_t* ncell,
 
 /* Same call with every array in HOST memory (pinned memory is faster). The
  * cells are streamed through device staging buffers owned by the context in
- * chunks, copies overlapping the flash on two streams; returns after the
- * results are back in host memory. The staging buffers are allocated on the
+ * chunks of 131,072 cells, copies overlapping the flash on four streams.
+ * Each chunk goes to the first stream whose previous chunk is back, so a
+ * chunk with a long restart chain holds back no other. The call returns
+ * after the results are back in host memory. The staging buffers are allocated on the
  * first call (and grown if a larger chunk is requested) and kept until
  * ocpf_destroy. */
 int ocpf_flash_fim_host(ocpf_ctx* ctx, int64_t ncell, const ocpf_fim_in* in, ocpf_skip* skip,
