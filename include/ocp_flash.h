@@ -237,9 +237,9 @@ int ocpf_reserve(ocpf_ctx* ctx, int64_t ncell);
  * device memory: applications that own all of the GPU's memory through their
  * own pool or arena, run under a fixed device-memory budget, or must not let
  * a flash call synchronise the device (cudaMalloc and cudaFree may). Its
- * scratch -- per-cell phase state and cell lists, ~1.8 KB per cell for up to
+ * scratch -- per-cell phase state and cell lists, ~1.9 KB per cell for up to
  * 12 components -- lives in one array compiled into the library, of
- * OCPF_NOALLOC_MAX_CELLS cells (about 7.4 MB, held on every GPU that loads
+ * OCPF_NOALLOC_MAX_CELLS cells (about 7.6 MB, held on every GPU that loads
  * the library until the process exits). The caller passes inputs and outputs
  * as for ocpf_flash_fim; the call allocates nothing and is asynchronous on
  * `stream`. Returns OCPF_ERANGE, without touching the GPU, when ncell exceeds

@@ -519,7 +519,11 @@ static int launch_form(ocpf_ctx* c, int form, int64_t count, int64_t stride, con
         if (form == OCPF_FORM_FAST && c->mlp && c->fc.learn_on) args.opts |= PH_LEARN;
         // the per-trial split schedule on the device path; the host path's
         // parts, and calls that record the part marks, keep one stream
-        if (part < 0 && !c->part_timing && ensure_side(c)) args.opts |= PH_EARLY;
+        if (part < 0 && !c->part_timing && ensure_side(c)) {
+            args.opts |= PH_EARLY;
+            // and the learned round beside trials 2-3 instead of before trial 0
+            if (args.opts & PH_LEARN) args.opts |= PH_DEFER;
+        }
         if (part < 0) {
             const int rc = ensure_scratch(c, count);
             if (rc != OCPF_OK) return rc;

@@ -128,7 +128,7 @@ __device__ void sta_ssm32_body(const FluidConst& F, const PhasedArgs& a, int k)
 {
     using F_ = SF<NC>;
     const StateBuf& S    = a.S;
-    const int       list = L_STA_0 + k;
+    const int       list = stab_list(L_STA_0 + k, a.sdup != 0);
     const uint32_t  n    = a.L.len(list);
     const float     tol2 = fmaxf(SSM32_TOL2, (float)F.ssmsta_tol2);
     float           lnY[NC], lndi[NC], sA[NC], Bi[NC];

@@ -94,6 +94,10 @@ enum ListId : int {
     // end point, continued by FP64 substitution, and their Newton step
     L_STC_0, L_STC_1, L_STC_2, L_STC_3,
     L_NRSTC_0, L_NRSTC_1, L_NRSTC_2, L_NRSTC_3,
+    // with PH_DEFER: the strict test of the cells whose learned split was
+    // not kept runs as a pass of its own, on a duplicate of the 16
+    // stability lists above (stab_list)
+    L_SDUP_0, L_SDUP_LAST = L_SDUP_0 + 15,
     L_COUNT
 };
 // A restart runs 200 or 400 substitution steps on one cell: on the
@@ -151,6 +155,15 @@ constexpr LaunchTune kDefaultTune{128, 100, 0, 0};
 constexpr uint32_t PH_MIXED = 1u;  // FP32 successive substitution (flash_mixed.cuh)
 constexpr uint32_t PH_LEARN = 2u;  // learned initialiser for fresh cells (flash_learned.cuh)
 constexpr uint32_t PH_EARLY = 4u;  // split each strict trial's unstable cells on its own side stream
+constexpr uint32_t PH_DEFER = 8u;  // learned round after trial 1, beside the main sequence (PH_EARLY)
+
+// Stability list `id` (L_STA_k, L_NRSTA_k, L_STC_k or L_NRSTC_k) of the main
+// pass, or with `dup` of the deferred learned round's fallback pass.
+__host__ __device__ constexpr int stab_list(int id, bool dup)
+{
+    return !dup ? id : (id < L_STC_0 ? L_SDUP_0 + (id - L_STA_0) : L_SDUP_0 + 8 + (id - L_STC_0));
+}
+static_assert(L_NRSTA_3 == L_STA_0 + 7 && L_NRSTC_3 == L_STC_0 + 7, "stability lists in two runs of eight");
 
 // The side streams of the PH_EARLY schedule: trial k's split round and
 // restarts run on s[k], after fork[k] is recorded on the call's stream; the
@@ -168,6 +181,9 @@ struct PhasedArgs {
     // its grid-stride loops see block blockIdx.x / vparts of a grid of
     // gridDim.x / vparts. vparts <= 1: the whole launch is this region's.
     int32_t      vpart, vparts;
+    // the pass's stability lists: 0 the main set, 1 the duplicate set of the
+    // deferred learned round's fallback pass (stab_list)
+    int32_t      sdup, pad_sdup;
     const float* mlp;  // learned initialiser parameters (PH_LEARN)
     FlashTail    tail; // entry point (FlashFIM, FlashIMPEC, InitFlash*) and its extra arrays
     ocpf_fim_in  in;

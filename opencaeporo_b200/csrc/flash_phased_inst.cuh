@@ -120,33 +120,43 @@ cudaError_t OCPF_CAT(launch_phased_nc, OCPF_NC)(const FluidConst& F, const Phase
     const bool    mixed = (a.opts & PH_MIXED) != 0;
     cudaMemsetAsync(a.L.ctr, 0, sizeof(uint32_t) * 2 * L_COUNT, st);
     KP(init)<<<gcell, bp, 0, st>>>(F, a);
+    const bool defer = (a.opts & PH_DEFER) != 0;
     if (a.opts & PH_LEARN) {
         // learned initialiser: predicted-unstable fresh cells split first
+        // (with PH_DEFER their split waits until trial 1 has run, below)
         const int gl = (int)std::min<int64_t>((a.count + LEARN_TILE - 1) / LEARN_TILE, (int64_t)sms * 4);
         KP(learn)<<<gl, 128, sizeof(LearnSmem), st>>>(F, a);
-        OCPF_CAT(split_round_, OCPF_NC)(F, a, st, LEARN_ROUND, gp, bp, g_sp, g_spnr);
+        if (!defer) OCPF_CAT(split_round_, OCPF_NC)(F, a, st, LEARN_ROUND, gp, bp, g_sp, g_spnr);
     }
     for (int k = 0; k < 2; k++) {
         KP(s01_prep)<<<gp, bp, 0, st>>>(F, a, k);
         KP(s01_ssm)<<<g_s01, 128, 0, st>>>(F, a, k);
         KP(s01_end)<<<gp, bp, 0, st>>>(F, a, k);
     }
-    for (int k = 0; k < 4; k++) {
-        KP(sta_prep)<<<gp, bp, 0, st>>>(F, a, k);
+    // strict stability trial k of the pass whose arguments are A (its lists:
+    // the main set, or with A.sdup the deferred fallback pass's own set)
+    auto trial = [&](const PhasedArgs& A, cudaStream_t s, int k) {
+        const bool d  = A.sdup != 0;
+        const int  sa = stab_list(L_STA_0 + k, d), na = stab_list(L_NRSTA_0 + k, d);
+        const int  sc = stab_list(L_STC_0 + k, d), nc = stab_list(L_NRSTC_0 + k, d);
+        KP(sta_prep)<<<gp, bp, 0, s>>>(F, A, k);
         if (mixed) {
             // FP32 substitution, FP64 end point and Newton; trials whose
             // Newton fails continue in FP64, then Newton again
-            KP(sta_ssm32)<<<g_sta32, 128, 0, st>>>(F, a, k);
-            KP(sta_verdict)<<<gp, bp, 0, st>>>(F, a, k, L_STA_0 + k, L_NRSTA_0 + k, true);
-            KP(sta_nr)<<<g_stnr, 128, 0, st>>>(F, a, k, L_NRSTA_0 + k, L_STC_0 + k);
-            KP(sta_ssm)<<<g_sta, 128, 0, st>>>(F, a, L_STC_0 + k);
-            KP(sta_verdict)<<<gp, bp, 0, st>>>(F, a, k, L_STC_0 + k, L_NRSTC_0 + k, false);
-            KP(sta_nr)<<<g_stnr, 128, 0, st>>>(F, a, k, L_NRSTC_0 + k, -1);
+            KP(sta_ssm32)<<<g_sta32, 128, 0, s>>>(F, A, k);
+            KP(sta_verdict)<<<gp, bp, 0, s>>>(F, A, k, sa, na, true);
+            KP(sta_nr)<<<g_stnr, 128, 0, s>>>(F, A, k, na, sc);
+            KP(sta_ssm)<<<g_sta, 128, 0, s>>>(F, A, sc);
+            KP(sta_verdict)<<<gp, bp, 0, s>>>(F, A, k, sc, nc, false);
+            KP(sta_nr)<<<g_stnr, 128, 0, s>>>(F, A, k, nc, -1);
         } else {
-            KP(sta_ssm)<<<g_sta, 128, 0, st>>>(F, a, L_STA_0 + k);
-            KP(sta_verdict)<<<gp, bp, 0, st>>>(F, a, k, L_STA_0 + k, L_NRSTA_0 + k, false);
-            KP(sta_nr)<<<g_stnr, 128, 0, st>>>(F, a, k, L_NRSTA_0 + k, -1);
+            KP(sta_ssm)<<<g_sta, 128, 0, s>>>(F, A, sa);
+            KP(sta_verdict)<<<gp, bp, 0, s>>>(F, A, k, sa, na, false);
+            KP(sta_nr)<<<g_stnr, 128, 0, s>>>(F, A, k, na, -1);
         }
+    };
+    for (int k = 0; k < 4; k++) {
+        trial(a, st, k);
         if ((a.opts & PH_EARLY) && k > 0) {
             // trial k's unstable cells: split and restarts beside the later trials
             cudaStream_t ss = st;
@@ -162,7 +172,27 @@ cudaError_t OCPF_CAT(launch_phased_nc, OCPF_NC)(const FluidConst& F, const Phase
                 KP(slow)<<<gp, 128, 0, ss>>>(F, a, L_SLOW_T0 + k);
             if (side) cudaEventRecord(side->join[k], ss);
         }
+        if (defer && k == 1) {
+            // the learned round, off the path of trials 0 and 1 (whose
+            // restart chains are the call's longest), on side stream 0 at the
+            // default priority; then the strict test of the cells whose
+            // learned split it did not keep, on lists of their own, all four
+            // trials; their unstable cells join split round 0
+            cudaStream_t ss = st;
+            if (side) {
+                ss = side->s[0];
+                cudaEventRecord(side->fork[0], st);
+                cudaStreamWaitEvent(ss, side->fork[0], 0);
+            }
+            OCPF_CAT(split_round_, OCPF_NC)(F, a, ss, LEARN_ROUND, gp, bp, g_sp, g_spnr);
+            PhasedArgs b = a;
+            b.sdup       = 1;
+            b.opts &= ~(PH_EARLY | PH_DEFER);
+            for (int kk = 0; kk < 4; kk++) trial(b, ss, kk);
+            if (side) cudaEventRecord(side->join[0], ss);
+        }
     }
+    if (defer && side) cudaStreamWaitEvent(st, side->join[0], 0);
     for (int r = 0; r < SPLIT_ROUNDS; r++) OCPF_CAT(split_round_, OCPF_NC)(F, a, st, r, gp, bp, g_sp, g_spnr);
     if (marks) cudaEventRecord(marks[0], st);
     if (t.slow_threads)

@@ -72,7 +72,7 @@ __device__ void sta_prep_body(const FluidConst& F, const PhasedArgs& a, int k)
 {
     using F_ = SF<NC>;
     const StateBuf& S = a.S;
-    OCPF_FOR_ITEMS(a, L_STA_0 + k, c)
+    OCPF_FOR_ITEMS(a, stab_list(L_STA_0 + k, a.sdup != 0), c)
     {
         CellFlash<NC> f(F);
         load_ptz(f, a, c);
@@ -193,7 +193,7 @@ __device__ __forceinline__ void sta_decide(CellFlash<NC>& f, const PhasedArgs& a
         a.L.push((a.opts & PH_EARLY) && k > 0 ? L_SP_T0 + k : L_SP_0, (int32_t)c);
     } else if (k < 3) {
         store_book(f, S, c, meta);
-        a.L.push(L_STA_0 + k + 1, (int32_t)c);
+        a.L.push(stab_list(L_STA_0 + k + 1, a.sdup != 0), (int32_t)c);
     } else {
         f.ssmsta_realTol = sqrt(Se);
         finish_epec(f);
@@ -662,7 +662,7 @@ __device__ __forceinline__ void learned_after_nr(CellFlash<NC>& f, const PhasedA
     S.I(IF_GUARD, c) = 0;
     store_single_phase(f, S, c, true);
     store_book(f, S, c, meta & ~(M_LEARNED | M_RESTART | M_SPPHASE));
-    a.L.push(L_STA_0, (int32_t)c);
+    a.L.push(stab_list(L_STA_0, (a.opts & PH_DEFER) != 0), (int32_t)c);
 }
 
 // End of PhaseSplit once SplitNR is done (src/MixtureComp.cpp:1750-1758,
