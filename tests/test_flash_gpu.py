@@ -237,6 +237,42 @@ def test_batched_host_path_and_reserve():
     m.close()
 
 
+@pytest.mark.parametrize("case", ["restart_nc6", "config1_nc6"])
+@pytest.mark.parametrize("form", ["batched", "fast"])
+def test_side_stream_schedule_changes_no_output(case, form):
+    """The default schedule of a device-buffer call runs some of the work on
+    side streams:
+    * the split and restarts of the cells that stability trials 1-3 find
+      unstable;
+    * in the fast form, the learned round and the strict test of its
+      fallback cells.
+    With the part marks on, the call keeps everything on its own stream in
+    the plain order. Both give the same outputs bit for bit. The
+    restart-heavy cells include trial-1 cells and long chains. The config-1
+    states include learned splits that are kept and ones that fall back."""
+    torch = _torch()
+    from opencaeporo_b200.flash import MixtureCompBatch
+    from opencaeporo_b200.learn import DEFAULT_MODEL, Initializer
+    fl, inp, ref, _ = load_golden(case)
+    outs = []
+    for one_stream in (False, True):
+        m = MixtureCompBatch(fl)
+        if form == "fast":
+            Initializer.load(DEFAULT_MODEL).attach(m)
+        m.set_part_timing(one_stream)
+        st = m.new_state(len(inp["P"]))
+        st.load(inp["P"], inp["T"], inp["Ni"])
+        for _ in range(2):  # the second call replays the captured sequence
+            st.skip["flag"].zero_()
+            m.flash_fim(st, form=form, fresh=True)
+        torch.cuda.synchronize()
+        outs.append(st.to_host())
+        m.close()
+    for k, v in outs[0].items():
+        if isinstance(v, np.ndarray):
+            np.testing.assert_array_equal(v, outs[1][k], err_msg=k)
+
+
 def test_caller_stream_capture_equals_direct_call():
     """A caller captures its own stream around a batched call. The side
     streams of the per-trial split schedule join that capture through their
