@@ -300,7 +300,7 @@ def our_arm(args):
             p = np.mean(np.array(parts), axis=0)
             forms[fm] = {"ms": float(np.mean(tot)), "to_restart_path_ms": float(p[0]), "restart_path_ms": float(p[1]),
                          "finalize_ms": float(p[2]), "excluding_restart_path_ms": float(p[0] + p[2]),
-                         "launch": "direct (part marks)"}
+                         "launch": "direct launches on one stream (part marks); the headline call forks trials 1-3 splits and the learned round onto side streams"}
         m.set_part_timing(False)
     ms_total, kern_ms = shards.max_over_ranks([ms_total, kern_ms], dev)
     ms_step = ms_total / args.steps
